@@ -1,0 +1,483 @@
+/*
+ * CPU restatement of the reference's FP64 PCG + geometric-multigrid solve path.
+ *
+ * TEST INFRASTRUCTURE ONLY: this file is the oracle of the parity tests and the "port" CPU
+ * baseline.  The product never links, loads or calls it.
+ *
+ * Every routine restates the reference's generic (CPU) code path in the same operation order,
+ * without FP contraction (built with -ffp-contract=off), so that its results are bitwise equal to
+ * the reference build of the same inputs:
+ *   oc_csr_apply        kernel/lafem/arch/apply_generic.hpp:25-69      (Apply::csr_generic)
+ *   oc_axpy             kernel/lafem/arch/axpy_generic.hpp:25-49       (Axpy::value_generic)
+ *   oc_dot              kernel/lafem/arch/dot_product_generic.hpp:21-41
+ *   oc_norm2            kernel/lafem/arch/norm_generic.hpp:24-33
+ *   oc_filter_*         kernel/lafem/arch/unit_filter_generic.hpp:22-37
+ *   inverse diagonal    kernel/solver/jacobi_precond.hpp:136-143 + sparse_matrix_csr.hpp:2277-2291
+ *                       + component_invert_generic.hpp:21-40
+ *   richardson_apply    kernel/solver/richardson.hpp:160-228 with the stopping logic of
+ *                       kernel/solver/iterative.hpp:492-507,748-879 (min_iter = max_iter = steps)
+ *   oc_mg_vcycle        kernel/solver/multigrid.hpp:1270-1350 (apply, V-cycle),
+ *                       :1526-1587 (_apply_coarse), :1713-1838 (_apply_rest),
+ *                       :1845-2000 (_apply_prol, fixed coarse-grid correction omega = 1)
+ *   oc_pcg_solve        kernel/solver/pcg.hpp:159-286 (correct + _apply_intern) with the stopping
+ *                       logic of kernel/solver/iterative.hpp (defaults: tol_abs = 1/eps^2,
+ *                       div_rel = 1/eps, div_abs = 1/eps^2, no stagnation check)
+ * The coarse-grid solve is an exact inverse of the matrix restricted to the free DOFs, formed by
+ * Gauss-Jordan elimination with partial pivoting and applied in ascending column order (the same
+ * coarse solver the reference-side driver oracle/feat_ref_driver.cpp plugs into the reference).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define OC_EPS 2.220446049250313080847e-16
+
+typedef struct
+{
+  uint64_t rows, cols;
+  const uint64_t* row_ptr;
+  const uint64_t* col_ind;
+  const double* val;
+} oc_csr;
+
+/* r = a * op(A) * x + b * y; |b| < eps means y is ignored (apply_generic.hpp:25-69) */
+void oc_csr_apply(double* r, double a, const double* x, double b, const double* y, const oc_csr* A,
+  int transposed)
+{
+  const uint64_t nout = transposed ? A->cols : A->rows;
+  if(fabs(b) < OC_EPS)
+    memset(r, 0, sizeof(double) * nout);
+  else if(r != y)
+    memcpy(r, y, sizeof(double) * nout);
+  if(transposed)
+  {
+    const double ba = b / a;
+    for(uint64_t c = 0; c < A->cols; ++c)
+      r[c] = ba * r[c];
+    for(uint64_t row = 0; row < A->rows; ++row)
+      for(uint64_t i = A->row_ptr[row]; i < A->row_ptr[row + 1]; ++i)
+        r[A->col_ind[i]] += A->val[i] * x[row];
+    for(uint64_t c = 0; c < A->cols; ++c)
+      r[c] = a * r[c];
+  }
+  else
+  {
+    for(uint64_t row = 0; row < A->rows; ++row)
+    {
+      double sum = 0.0;
+      const uint64_t end = A->row_ptr[row + 1];
+      for(uint64_t i = A->row_ptr[row]; i < end; ++i)
+        sum += A->val[i] * x[A->col_ind[i]];
+      r[row] = (sum * a) + (b * r[row]);
+    }
+  }
+}
+
+/* r = a * x + y (axpy_generic.hpp:25-49; every alias branch rounds as fl(fl(a*x) + y)) */
+void oc_axpy(double* r, double a, const double* x, const double* y, uint64_t n)
+{
+  if(r == y)
+    for(uint64_t i = 0; i < n; ++i)
+      r[i] += a * x[i];
+  else if(r == x)
+    for(uint64_t i = 0; i < n; ++i)
+    {
+      r[i] *= a;
+      r[i] += y[i];
+    }
+  else
+    for(uint64_t i = 0; i < n; ++i)
+      r[i] = (a * x[i]) + y[i];
+}
+
+double oc_dot(const double* x, const double* y, uint64_t n)
+{
+  double r = 0.0;
+  for(uint64_t i = 0; i < n; ++i)
+    r += x[i] * y[i];
+  return r;
+}
+
+double oc_norm2(const double* x, uint64_t n)
+{
+  double r = 0.0;
+  for(uint64_t i = 0; i < n; ++i)
+    r += x[i] * x[i];
+  return sqrt(r);
+}
+
+void oc_filter_rhs(double* v, const double* vals, const uint64_t* idx, uint64_t ue)
+{
+  for(uint64_t i = 0; i < ue; ++i)
+    v[idx[i]] = vals[i];
+}
+
+void oc_filter_def(double* v, const uint64_t* idx, uint64_t ue)
+{
+  for(uint64_t i = 0; i < ue; ++i)
+    v[idx[i]] = 0.0;
+}
+
+/* inv_diag_i = omega / a_ii, 0 diagonal when the row has no diagonal entry */
+void oc_inv_diag(double* d, const oc_csr* A, double omega)
+{
+  for(uint64_t row = 0; row < A->rows; ++row)
+  {
+    double a = 0.0;
+    for(uint64_t i = A->row_ptr[row]; i < A->row_ptr[row + 1]; ++i)
+      if(A->col_ind[i] == row)
+      {
+        a = A->val[i];
+        break;
+      }
+    d[row] = omega / a;
+  }
+}
+
+typedef struct
+{
+  oc_csr A, P, R;        /* P: this level <- next coarser level; R: next coarser <- this */
+  const uint64_t* fidx;  /* Dirichlet DOFs */
+  const double* fval;
+  uint64_t nf;
+} oc_level_in;
+
+typedef struct
+{
+  oc_level_in in;
+  uint64_t n;
+  double *rhs, *sol, *def, *cor, *tmp;
+  double *inv_diag, *sm_def, *sm_cor;
+} oc_level;
+
+typedef struct
+{
+  int nlevels;
+  oc_level* lv;
+  double omega;
+  int steps;
+  uint64_t nfree;
+  uint64_t* free_dofs;
+  double* cinv;
+  /* PCG vectors on the finest level */
+  double *r, *p, *t;
+} oc_mg;
+
+static int coarse_factor(oc_mg* mg)
+{
+  oc_level* c = &mg->lv[mg->nlevels - 1];
+  const uint64_t n = c->n;
+  char* dir = (char*)calloc(n, 1);
+  for(uint64_t k = 0; k < c->in.nf; ++k)
+    dir[c->in.fidx[k]] = 1;
+  uint64_t m = 0;
+  for(uint64_t i = 0; i < n; ++i)
+    m += dir[i] ? 0 : 1;
+  mg->nfree = m;
+  mg->free_dofs = (uint64_t*)malloc(sizeof(uint64_t) * (m ? m : 1));
+  uint64_t* pos = (uint64_t*)malloc(sizeof(uint64_t) * n);
+  m = 0;
+  for(uint64_t i = 0; i < n; ++i)
+  {
+    pos[i] = UINT64_MAX;
+    if(!dir[i])
+    {
+      pos[i] = m;
+      mg->free_dofs[m++] = i;
+    }
+  }
+  double* a = (double*)calloc(m * m + 1, sizeof(double));
+  double* inv = (double*)calloc(m * m + 1, sizeof(double));
+  for(uint64_t i = 0; i < m; ++i)
+  {
+    const uint64_t r = mg->free_dofs[i];
+    for(uint64_t k = c->in.A.row_ptr[r]; k < c->in.A.row_ptr[r + 1]; ++k)
+    {
+      const uint64_t cc = c->in.A.col_ind[k];
+      if(pos[cc] != UINT64_MAX)
+        a[i * m + pos[cc]] = c->in.A.val[k];
+    }
+    inv[i * m + i] = 1.0;
+  }
+  for(uint64_t col = 0; col < m; ++col)
+  {
+    uint64_t p = col;
+    for(uint64_t r = col + 1; r < m; ++r)
+      if(fabs(a[r * m + col]) > fabs(a[p * m + col]))
+        p = r;
+    if(p != col)
+      for(uint64_t j = 0; j < m; ++j)
+      {
+        double t = a[p * m + j];
+        a[p * m + j] = a[col * m + j];
+        a[col * m + j] = t;
+        t = inv[p * m + j];
+        inv[p * m + j] = inv[col * m + j];
+        inv[col * m + j] = t;
+      }
+    const double d = a[col * m + col];
+    for(uint64_t j = 0; j < m; ++j)
+    {
+      a[col * m + j] /= d;
+      inv[col * m + j] /= d;
+    }
+    for(uint64_t r = 0; r < m; ++r)
+    {
+      if(r == col)
+        continue;
+      const double f = a[r * m + col];
+      if(f == 0.0)
+        continue;
+      for(uint64_t j = 0; j < m; ++j)
+      {
+        a[r * m + j] -= f * a[col * m + j];
+        inv[r * m + j] -= f * inv[col * m + j];
+      }
+    }
+  }
+  mg->cinv = inv;
+  free(a);
+  free(pos);
+  free(dir);
+  return 0;
+}
+
+oc_mg* oc_mg_create(int nlevels, const oc_level_in* levels, double omega, int steps)
+{
+  oc_mg* mg = (oc_mg*)calloc(1, sizeof(oc_mg));
+  mg->nlevels = nlevels;
+  mg->omega = omega;
+  mg->steps = steps;
+  mg->lv = (oc_level*)calloc((size_t)nlevels, sizeof(oc_level));
+  for(int l = 0; l < nlevels; ++l)
+  {
+    oc_level* v = &mg->lv[l];
+    v->in = levels[l];
+    v->n = levels[l].A.rows;
+    v->rhs = (double*)calloc(v->n, sizeof(double));
+    v->sol = (double*)calloc(v->n, sizeof(double));
+    v->def = (double*)calloc(v->n, sizeof(double));
+    v->cor = (double*)calloc(v->n, sizeof(double));
+    v->tmp = (double*)calloc(v->n, sizeof(double));
+    v->inv_diag = (double*)calloc(v->n, sizeof(double));
+    v->sm_def = (double*)calloc(v->n, sizeof(double));
+    v->sm_cor = (double*)calloc(v->n, sizeof(double));
+    oc_inv_diag(v->inv_diag, &v->in.A, omega);
+  }
+  coarse_factor(mg);
+  const uint64_t n = mg->lv[0].n;
+  mg->r = (double*)calloc(n, sizeof(double));
+  mg->p = (double*)calloc(n, sizeof(double));
+  mg->t = (double*)calloc(n, sizeof(double));
+  return mg;
+}
+
+void oc_mg_destroy(oc_mg* mg)
+{
+  if(!mg)
+    return;
+  for(int l = 0; l < mg->nlevels; ++l)
+  {
+    oc_level* v = &mg->lv[l];
+    free(v->rhs); free(v->sol); free(v->def); free(v->cor); free(v->tmp);
+    free(v->inv_diag); free(v->sm_def); free(v->sm_cor);
+  }
+  free(mg->lv);
+  free(mg->free_dofs);
+  free(mg->cinv);
+  free(mg->r); free(mg->p); free(mg->t);
+  free(mg);
+}
+
+/* Richardson(omega = 1) with Jacobi preconditioner, min_iter = max_iter = steps:
+ * out = smoother(in), out starts at zero (richardson.hpp:160-228). */
+static void richardson_apply(const oc_mg* mg, const oc_level* v, double* out, const double* in)
+{
+  const uint64_t n = v->n;
+  memcpy(v->sm_def, in, sizeof(double) * n);
+  memset(out, 0, sizeof(double) * n);
+  const double def_init = oc_norm2(v->sm_def, n);
+  if(!isfinite(def_init))
+    return;                                   /* Status::aborted */
+  if(def_init <= OC_EPS * OC_EPS)
+    return;                                   /* Status::success */
+  for(int it = 1;; ++it)
+  {
+    /* JacobiPrecond::apply: cor = inv_diag .* def, filter_cor */
+    for(uint64_t i = 0; i < n; ++i)
+      v->sm_cor[i] = v->inv_diag[i] * v->sm_def[i];
+    oc_filter_def(v->sm_cor, v->in.fidx, v->in.nf);
+    oc_axpy(out, 1.0, v->sm_cor, out, n);
+    oc_csr_apply(v->sm_def, -1.0, out, 1.0, in, &v->in.A, 0);
+    oc_filter_def(v->sm_def, v->in.fidx, v->in.nf);
+    /* _set_new_defect without a norm (min_iter == max_iter): the stored defect stays def_init */
+    if(def_init > 1.0 / (OC_EPS * OC_EPS) || def_init > (1.0 / OC_EPS) * def_init)
+      return;                                 /* Status::diverged */
+    if(it < mg->steps)
+      continue;
+    return;                                   /* converged test is false; Status::max_iter */
+  }
+}
+
+static void coarse_apply(const oc_mg* mg, double* x, const double* b)
+{
+  const oc_level* c = &mg->lv[mg->nlevels - 1];
+  memset(x, 0, sizeof(double) * c->n);
+  const uint64_t m = mg->nfree;
+  for(uint64_t i = 0; i < m; ++i)
+  {
+    double s = 0.0;
+    for(uint64_t j = 0; j < m; ++j)
+      s += mg->cinv[i * m + j] * b[mg->free_dofs[j]];
+    x[mg->free_dofs[i]] = s;
+  }
+}
+
+/* cor = MG_V(def) (multigrid.hpp:1270-1350) */
+int oc_mg_vcycle(oc_mg* mg, double* cor, const double* def)
+{
+  const int L = mg->nlevels;
+  memcpy(mg->lv[0].rhs, def, sizeof(double) * mg->lv[0].n);
+  /* _apply_rest(top, true) */
+  for(int i = 0; i + 1 < L; ++i)
+  {
+    oc_level* f = &mg->lv[i];
+    oc_level* c = &mg->lv[i + 1];
+    richardson_apply(mg, f, f->sol, f->rhs);
+    oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+    oc_filter_def(f->def, f->in.fidx, f->in.nf);
+    oc_csr_apply(c->rhs, 1.0, f->def, 0.0, c->rhs, &f->in.R, 0);
+    oc_filter_def(c->rhs, c->in.fidx, c->in.nf);
+  }
+  /* _apply_coarse */
+  if(L > 0)
+    coarse_apply(mg, mg->lv[L - 1].sol, mg->lv[L - 1].rhs);
+  /* _apply_prol(top, true) */
+  for(int i = L - 2; i >= 0; --i)
+  {
+    oc_level* f = &mg->lv[i];
+    oc_level* c = &mg->lv[i + 1];
+    oc_csr_apply(f->cor, 1.0, c->sol, 0.0, f->cor, &f->in.P, 0);
+    oc_filter_def(f->cor, f->in.fidx, f->in.nf);
+    oc_axpy(f->sol, 1.0, f->cor, f->sol, f->n);
+    oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+    oc_filter_def(f->def, f->in.fidx, f->in.nf);
+    richardson_apply(mg, f, f->cor, f->def);
+    oc_axpy(f->sol, 1.0, f->cor, f->sol, f->n);
+  }
+  memcpy(cor, mg->lv[0].sol, sizeof(double) * mg->lv[0].n);
+  return 0;
+}
+
+enum { OC_PROGRESS = 0, OC_SUCCESS = 1, OC_ABORTED = 2, OC_DIVERGED = 3, OC_MAX_ITER = 4 };
+
+/* PCG::correct(sol, rhs) preconditioned by one V-cycle (pcg.hpp:159-286).  sol holds the initial
+ * guess on entry.  defects[0..iters] receives the defect norms (defects[0] = initial). */
+int oc_pcg_solve(oc_mg* mg, double* sol, const double* rhs, double tol_rel, int max_iter,
+  double* defects, int* iters_out)
+{
+  const oc_level* top = &mg->lv[0];
+  const uint64_t n = top->n;
+  const oc_csr* A = &top->in.A;
+  double *r = mg->r, *p = mg->p, *t = mg->t;
+  const double tol_abs = 1.0 / (OC_EPS * OC_EPS), div_abs = 1.0 / (OC_EPS * OC_EPS);
+  const double div_rel = 1.0 / OC_EPS;
+
+  oc_csr_apply(r, -1.0, sol, 1.0, rhs, A, 0);
+  oc_filter_def(r, top->in.fidx, top->in.nf);
+  const double def_init = oc_norm2(r, n);
+  double def_cur = def_init;
+  int it = 0;
+  if(defects)
+    defects[0] = def_init;
+  *iters_out = 0;
+  if(!isfinite(def_init))
+    return OC_ABORTED;
+  if(def_init <= OC_EPS * OC_EPS)
+    return OC_SUCCESS;
+  oc_mg_vcycle(mg, p, r);
+  double gamma = oc_dot(r, p, n);
+  for(;;)
+  {
+    oc_csr_apply(t, 1.0, p, 0.0, t, A, 0);
+    oc_filter_def(t, top->in.fidx, top->in.nf);
+    const double alpha = gamma / oc_dot(t, p, n);
+    oc_axpy(sol, alpha, p, sol, n);
+    oc_axpy(r, -alpha, t, r, n);
+    ++it;
+    def_cur = oc_norm2(r, n);
+    if(defects)
+      defects[it] = def_cur;
+    *iters_out = it;
+    if(!isfinite(def_cur))
+      return OC_ABORTED;
+    if(def_cur > div_abs || def_cur > div_rel * def_init)
+      return OC_DIVERGED;
+    if(def_cur <= tol_abs && (def_cur <= tol_rel * def_init || def_cur <= 0.0))
+      return OC_SUCCESS;
+    if(it >= max_iter)
+      return OC_MAX_ITER;
+    oc_mg_vcycle(mg, t, r);
+    const double gamma2 = gamma;
+    gamma = oc_dot(r, t, n);
+    const double beta = gamma / gamma2;
+    oc_axpy(p, beta, p, t, n);
+  }
+}
+
+/* Plain PCG with a Jacobi preconditioner (or none when omega == 0), on one matrix, for the
+ * reference's known-answer iteration counts (kernel/solver/basic_solver-test.cpp:98-140). */
+int oc_pcg_jacobi(const oc_csr* A, const uint64_t* fidx, uint64_t nf, double omega, double* sol,
+  const double* rhs, double tol_rel, int max_iter, int* iters_out)
+{
+  const uint64_t n = A->rows;
+  double* r = (double*)calloc(n, sizeof(double));
+  double* p = (double*)calloc(n, sizeof(double));
+  double* t = (double*)calloc(n, sizeof(double));
+  double* d = (double*)calloc(n, sizeof(double));
+  if(omega > 0.0)
+    oc_inv_diag(d, A, omega);
+  int status = OC_PROGRESS;
+  const double tol_abs = 1.0 / (OC_EPS * OC_EPS);
+  oc_csr_apply(r, -1.0, sol, 1.0, rhs, A, 0);
+  oc_filter_def(r, fidx, nf);
+  const double def_init = oc_norm2(r, n);
+  int it = 0;
+#define OC_PRECOND(z, v)                                            \
+  do {                                                              \
+    if(omega > 0.0) for(uint64_t i_ = 0; i_ < n; ++i_) z[i_] = d[i_] * v[i_]; \
+    else memcpy(z, v, sizeof(double) * n);                          \
+    oc_filter_def(z, fidx, nf);                                     \
+  } while(0)
+  if(!isfinite(def_init))
+    status = OC_ABORTED;
+  else if(def_init <= OC_EPS * OC_EPS)
+    status = OC_SUCCESS;
+  else
+  {
+    OC_PRECOND(p, r);
+    double gamma = oc_dot(r, p, n);
+    for(;;)
+    {
+      oc_csr_apply(t, 1.0, p, 0.0, t, A, 0);
+      oc_filter_def(t, fidx, nf);
+      const double alpha = gamma / oc_dot(t, p, n);
+      oc_axpy(sol, alpha, p, sol, n);
+      oc_axpy(r, -alpha, t, r, n);
+      ++it;
+      const double def_cur = oc_norm2(r, n);
+      if(!isfinite(def_cur)) { status = OC_ABORTED; break; }
+      if(def_cur <= tol_abs && def_cur <= tol_rel * def_init) { status = OC_SUCCESS; break; }
+      if(it >= max_iter) { status = OC_MAX_ITER; break; }
+      OC_PRECOND(t, r);
+      const double gamma2 = gamma;
+      gamma = oc_dot(r, t, n);
+      oc_axpy(p, gamma / gamma2, p, t, n);
+    }
+  }
+#undef OC_PRECOND
+  *iters_out = it;
+  free(r); free(p); free(t); free(d);
+  return status;
+}

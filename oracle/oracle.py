@@ -1,0 +1,221 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/_ref/libmgoracle.so`` (the C restatement in ``oracle/mg_oracle.c``) and runs the
+reference-side driver ``oracle/_ref/feat_oracle`` (the reference's own CPU solver, built by
+``oracle/Makefile``).  Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module; the product never does.
+
+Hierarchies are passed finest level first, as in the reference's ``MultiGridHierarchy``
+(kernel/solver/multigrid.hpp:419-957): level i holds A_i, the unit-filter indices of level i, and
+P_i (level i <- level i+1), R_i (level i+1 <- level i) for every level but the coarsest.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+LIB_PATH = os.path.join(REF_DIR, "libmgoracle.so")
+FEAT_BIN = os.path.join(REF_DIR, "feat_oracle")
+
+STATUS = {0: "progress", 1: "success", 2: "aborted", 3: "diverged", 4: "max_iter"}
+
+
+class _Csr(C.Structure):
+    _fields_ = [("rows", C.c_uint64), ("cols", C.c_uint64), ("row_ptr", C.c_void_p),
+                ("col_ind", C.c_void_p), ("val", C.c_void_p)]
+
+
+class _LevelIn(C.Structure):
+    _fields_ = [("A", _Csr), ("P", _Csr), ("R", _Csr), ("fidx", C.c_void_p), ("fval", C.c_void_p),
+                ("nf", C.c_uint64)]
+
+
+def build():
+    """Compile the C restatement (and the reference driver when the reference tree exists)."""
+    targets = ["port"]
+    if os.path.isdir("/root/reference"):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.oc_csr_apply.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_double, C.c_void_p,
+                                   C.POINTER(_Csr), C.c_int]
+        L.oc_axpy.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_uint64]
+        L.oc_dot.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64]
+        L.oc_dot.restype = C.c_double
+        L.oc_norm2.argtypes = [C.c_void_p, C.c_uint64]
+        L.oc_norm2.restype = C.c_double
+        L.oc_mg_create.argtypes = [C.c_int, C.POINTER(_LevelIn), C.c_double, C.c_int]
+        L.oc_mg_create.restype = C.c_void_p
+        L.oc_mg_destroy.argtypes = [C.c_void_p]
+        L.oc_mg_vcycle.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_pcg_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                                   C.c_void_p, C.POINTER(C.c_int)]
+        L.oc_pcg_jacobi.argtypes = [C.POINTER(_Csr), C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
+                                    C.c_void_p, C.c_double, C.c_int, C.POINTER(C.c_int)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None and a.size else None
+
+
+@dataclass
+class Csr:
+    """A CSR matrix with the reference's default index type (u64) and FP64 values."""
+    row_ptr: np.ndarray
+    col_ind: np.ndarray
+    val: np.ndarray
+    shape: tuple
+
+    @staticmethod
+    def of(row_ptr, col_ind, val, shape):
+        return Csr(np.ascontiguousarray(row_ptr, dtype=np.uint64),
+                   np.ascontiguousarray(col_ind, dtype=np.uint64),
+                   np.ascontiguousarray(val, dtype=np.float64), (int(shape[0]), int(shape[1])))
+
+    def c(self):
+        return _Csr(self.shape[0], self.shape[1], _ptr(self.row_ptr), _ptr(self.col_ind), _ptr(self.val))
+
+
+def csr_apply(A: Csr, x, a=1.0, b=0.0, y=None, transposed=False):
+    """r = a * op(A) x + b * y, restated from Apply::csr_generic."""
+    nout = A.shape[1] if transposed else A.shape[0]
+    r = np.zeros(nout) if y is None else np.array(y, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    yy = r if y is not None else None
+    cs = A.c()
+    lib().oc_csr_apply(_ptr(r), a, _ptr(x), b, _ptr(yy) if yy is not None else _ptr(r), C.byref(cs),
+                       1 if transposed else 0)
+    return r
+
+
+def dot(x, y):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    return lib().oc_dot(_ptr(x), _ptr(y), x.size)
+
+
+def norm2(x):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return lib().oc_norm2(_ptr(x), x.size)
+
+
+class MultigridPCG:
+    """The FP64 PCG + V(steps, steps) multigrid of the reference, restated in C."""
+
+    def __init__(self, levels, omega=0.7, steps=2):
+        self._keep = []
+        arr = (_LevelIn * len(levels))()
+        for i, lv in enumerate(levels):
+            A = lv["A"]
+            fidx = np.ascontiguousarray(lv["filter_idx"], dtype=np.uint64)
+            fval = np.ascontiguousarray(lv.get("filter_val", np.zeros(fidx.size)), dtype=np.float64)
+            self._keep += [A, fidx, fval]
+            arr[i].A = A.c()
+            if "P" in lv and lv["P"] is not None:
+                self._keep += [lv["P"], lv["R"]]
+                arr[i].P = lv["P"].c()
+                arr[i].R = lv["R"].c()
+            arr[i].fidx = _ptr(fidx)
+            arr[i].fval = _ptr(fval)
+            arr[i].nf = fidx.size
+        self._arr = arr
+        self.n = levels[0]["A"].shape[0]
+        self._h = lib().oc_mg_create(len(levels), arr, omega, steps)
+
+    def vcycle(self, d):
+        d = np.ascontiguousarray(d, dtype=np.float64)
+        z = np.zeros(self.n)
+        lib().oc_mg_vcycle(self._h, _ptr(z), _ptr(d))
+        return z
+
+    def solve(self, rhs, x0=None, tol_rel=1e-8, max_iter=100):
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        defects = np.zeros(max_iter + 1)
+        it = C.c_int(0)
+        st = lib().oc_pcg_solve(self._h, _ptr(x), _ptr(rhs), tol_rel, max_iter, _ptr(defects),
+                                C.byref(it))
+        return x, {"status": STATUS[st], "iters": it.value, "defects": defects[: it.value + 1]}
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oc_mg_destroy(self._h)
+            self._h = None
+
+
+def pcg_jacobi(A: Csr, rhs, filter_idx, omega=1.0, tol_rel=1e-8, max_iter=1000):
+    """Plain PCG (omega = 0: no preconditioner; else Jacobi(omega)) from a zero guess."""
+    fidx = np.ascontiguousarray(filter_idx, dtype=np.uint64)
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    x = np.zeros(A.shape[0])
+    it = C.c_int(0)
+    cs = A.c()
+    st = lib().oc_pcg_jacobi(C.byref(cs), _ptr(fidx), fidx.size, omega, _ptr(x), _ptr(rhs), tol_rel,
+                             max_iter, C.byref(it))
+    return x, STATUS[st], it.value
+
+
+# ------------------------------------------------------------------ reference-side driver
+def feat_available():
+    return os.path.exists(FEAT_BIN)
+
+
+def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, omega=0.7, steps=2,
+               tol=1e-8, iterates=0, vcycle=False, dump_levels=False, time_reps=0, dump=True,
+               level_min=1, timeout=3600):
+    """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary."""
+    cmd = [FEAT_BIN, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
+           "--out", out_dir, "--rhs", rhs, "--omega", repr(omega), "--steps", str(steps), "--tol",
+           repr(tol), "--iterates", str(iterates), "--time", str(time_reps)]
+    if params:
+        cmd += ["--params", params]
+    if kappa:
+        cmd += ["--kappa", kappa]
+    if vcycle:
+        cmd.append("--vcycle")
+    if dump_levels:
+        cmd.append("--dump-levels")
+    if not dump:
+        cmd.append("--no-dump")
+    os.makedirs(out_dir, exist_ok=True)
+    res = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def load_dump(out_dir, level, level_min=1):
+    """Read a feat_oracle dump (written with --dump-levels) into a finest-first level list."""
+    def ld(name):
+        return np.load(os.path.join(out_dir, name + ".npy"))
+
+    def csr(prefix):
+        return Csr.of(ld(prefix + "_row_ptr"), ld(prefix + "_col_ind"), ld(prefix + "_val"),
+                      ld(prefix + "_shape"))
+
+    levels = []
+    for lv in range(level, level_min - 1, -1):
+        d = {"A": csr(f"L{lv}_A"), "filter_idx": ld(f"L{lv}_filter_idx"),
+             "filter_val": ld(f"L{lv}_filter_val"), "coords": ld(f"L{lv}_coords")}
+        if lv > level_min:
+            d["P"] = csr(f"L{lv}_P")
+            d["R"] = csr(f"L{lv}_R")
+        levels.append(d)
+    return levels
