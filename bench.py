@@ -1,0 +1,323 @@
+"""Benchmark of the geometric-multigrid Poisson solve path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Default workload (the configuration the headline metric is quoted on): 2D Poisson, Q1 on the unit
+square, level 10 (1,050,625 DOFs, 9,443,329 nnz), right-hand side a sum of 8 seeded Gaussians,
+PCG preconditioned by one V(2,2) cycle (Richardson + Jacobi omega 0.7, exact coarse solve on level
+1) run in FP32 inside FP64 PCG (iterative refinement), relative residual 1e-8.
+
+One step = one complete solve from a zero initial guess with the matrices resident in HBM.  Each
+step is timed with CUDA events on the stream of the call; the L2 is overwritten between steps
+(outside the timed interval).  `value` is milliseconds per solve for the whole job (max over ranks
+of the per-rank time / solves of all ranks); every GPU solves its own replica ("replicas only":
+a single solve does not shard).  rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "feat3.doxytest_b200"))
+
+METRIC = "solve ms to 1e-8 residual vs plain FP64 GPU multigrid; SpMV HBM GB/s"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    # name: (dim, level, rhs, precision, description)
+    "poisson2d_l10_mixed": (2, 10, "gauss", "f32",
+                            "2D Poisson Q1 unit square L10 (1,050,625 DOFs), 8-Gaussian RHS seed 1, "
+                            "PCG + FP32 V(2,2) Jacobi(0.7) multigrid in FP64 refinement, tol_rel 1e-8"),
+    "poisson2d_l10_bf16": (2, 10, "gauss", "f32_bf16",
+                           "as poisson2d_l10_mixed with BF16 matrix values in the V-cycle"),
+    "poisson2d_l10_fp64": (2, 10, "gauss", "f64", "plain FP64 PCG + V(2,2) multigrid, L10, 8-Gaussian RHS"),
+    "poisson2d_l7_fp64": (2, 7, "sine", "f64", "2D Poisson Q1 L7 (16,641 DOFs), sine-bubble RHS, plain FP64"),
+}
+DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(dim, level, rhs_kind):
+    from featb200 import assembly as AS
+    gauss = AS.gauss_params(1, dim, width=(0.02, 0.1) if dim == 2 else (0.03, 0.12)) if rhs_kind == "gauss" else None
+    levels, b = AS.poisson_hierarchy(level, dim, rhs=rhs_kind, gauss=gauss)
+    return levels, b, gauss
+
+
+def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900):
+    """The reference's own CPU solver (oracle/_ref/feat_oracle, built from the reference's sources)
+    on the same problem; returns its JSON summary with per-solve times (1 warm-up + reps)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.feat_available():
+        return None
+    from featb200 import assembly as AS
+    with tempfile.TemporaryDirectory() as d:
+        params = None
+        if gauss is not None:
+            params = os.path.join(d, "gauss.txt")
+            AS.write_params(params, gauss=gauss)
+        return O.feat_solve(d, dim=dim, level=level, rhs=rhs_kind, params=params, dump=False, time_reps=reps,
+                            timeout=timeout)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    from featb200 import assembly as AS
+    gauss = AS.gauss_params(1, dim) if rhs_kind == "gauss" else None
+    res = cpu_reference_times(dim, level, rhs_kind, gauss, args.warmup + args.steps)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/feat_oracle (the reference built from "
+                          "its sources) is missing; build it with `make -C oracle ref`"}))
+        return 0
+    times = res["times_ms"][args.warmup:] if len(res["times_ms"]) > args.warmup else res["times_ms"]
+    ms = float(np.mean(times))
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": len(times),
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload + ": " + desc + " (the reference's CPU path is FP64 only)",
+                       "dofs": res["dofs"], "nnz": res["nnz"], "iterations": res["iters"]},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference",
+                             "sample": f"{len(times)} FP64 solves of the workload by the reference's generic "
+                                       "(single-threaded) backend, solve only"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+    import featb200 as fb
+
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    levels, b, gauss = build_problem(dim, level, rhs_kind)
+    n = b.size
+    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm")
+    info_lv = solver.level_info()
+
+    stream = torch.cuda.current_stream()
+    rhs_d = torch.tensor(b, device="cuda")
+    sol_d = torch.zeros_like(rhs_d)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def one_step():
+        sol_d.zero_()
+        st = solver.correct_device(sol_d, rhs_d, stream)
+        return st
+
+    for _ in range(args.warmup):
+        st = one_step()
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = fb.launch_count()
+    times = []
+    iters = []
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.fill_(1)                                   # cold L2 for every solve (not timed)
+        ev0.record(stream)
+        st = one_step()
+        ev1.record(stream)
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+        iters.append(solver.get_num_iter())
+        if st != fb.Status.success:
+            raise SystemExit(f"solve failed: {st}")
+    torch.cuda.synchronize()
+    launches = fb.launch_count() - launches0
+    clk = clocks.stop()
+    total_ms = float(np.sum(times))
+    if pg:
+        t = torch.tensor([total_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+        pg.barrier()
+    ms_per_step = total_ms / args.steps
+    value = ms_per_step / world
+
+    # accuracy against the residual and the FP64 solution
+    x = sol_d.cpu().numpy()
+    A = levels[0]["matrix"].to_scipy()
+    r = b - A @ x
+    r[levels[0]["filter"].indices.astype(np.int64)] = 0.0
+    rel_res = float(np.linalg.norm(r) / np.linalg.norm(b))
+
+    extra = {}
+    if not args.no_plain and precision != "f64":
+        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering="rcm")
+        pt = []
+        for k in range(args.warmup + max(3, args.steps // 2)):
+            flush.fill_(1)
+            sol2 = torch.zeros_like(rhs_d)
+            ev0.record(stream)
+            plain.correct_device(sol2, rhs_d, stream)
+            ev1.record(stream)
+            ev1.synchronize()
+            if k >= args.warmup:
+                pt.append(ev0.elapsed_time(ev1))
+        x64 = sol2.cpu().numpy()
+        extra["plain_fp64_ms"] = float(np.mean(pt))
+        extra["plain_fp64_iterations"] = plain.get_num_iter()
+        extra["speedup_vs_plain_fp64"] = extra["plain_fp64_ms"] / ms_per_step
+        extra["error_vs_fp64"] = float(np.abs(x - x64).max() / np.abs(x64).max())
+        plain.done()
+
+    # roofline of the dominant kernel, timed alone on the solver's stream with a cold L2
+    peak, peak_kind = read_peaks()
+    kern = "pcg_spmv"
+    ms_k, by_k = solver.time_kernel(kern, reps=20, flush_l2=True)
+    ms_d, by_d = solver.time_kernel("mg_defect", reps=20, flush_l2=True)
+    achieved = by_k / (ms_k * 1e-3) / 1e9
+    spmv_gbs = {"pcg_spmv_f64": achieved, "mg_defect_" + precision: by_d / (ms_d * 1e-3) / 1e9}
+
+    # end to end through the C ABI with host buffers (copies inside the timed region)
+    pin_rhs = torch.tensor(b).pin_memory()
+    pin_sol = torch.zeros(n, dtype=torch.float64).pin_memory()
+    e2e_t = []
+    for k in range(args.warmup + args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        pin_sol.zero_()
+        t0 = time.perf_counter()
+        xs = fb.DenseVector(pin_sol.numpy())
+        solver.correct(xs, fb.DenseVector(pin_rhs.numpy()))
+        t1 = time.perf_counter()
+        if k >= args.warmup:
+            e2e_t.append((t1 - t0) * 1e3)
+    e2e_ms = float(np.mean(e2e_t))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res = cpu_reference_times(dim, level, rhs_kind, gauss, 5)
+        if res is not None:
+            cpu = {"value": float(np.median(res["times_ms"][1:] or res["times_ms"])), "unit": "ms", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"{len(res['times_ms']) - 1} FP64 solves (after 1 warm-up) of the same problem by the "
+                             f"reference's generic backend, single-threaded, solve only; {res['iters']} iterations"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if precision != "f64" else "f64", "data": "synthetic",
+                "config": {"workload": args.workload + ": " + desc, "dofs": int(n), "nnz": int(info_lv[0][1]),
+                           "levels": int(info_lv.shape[0]), "ordering": "rcm", "precision": precision,
+                           "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed solve",
+                           "iterations": int(np.median(iters))},
+                "spmv_gbs": spmv_gbs, "rel_residual": rel_res,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "kernel": "k_pcg_q (FP64 CSR SpMV + q.p)",
+                             "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": by_k,
+                             "launch_ms": ms_k},
+                "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(2 * 8 * n),
+                        "d2h_bytes_per_step": int(8 * n)},
+                "gpu_launches": int(launches), "clocks": clk}
+        line.update(extra)
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    solver.done()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1521 @@
+// Solver level: PCG preconditioned by a geometric-multigrid V-cycle, fully device resident.
+//
+// The V(s,s) cycle with Richardson(1)+Jacobi(omega) smoothing of the reference
+// (kernel/solver/multigrid.hpp:1270-2000, kernel/solver/richardson.hpp:160-228,
+// kernel/solver/jacobi_precond.hpp:136-165) is executed as a fixed sequence of fused passes, each
+// one CSR sweep over one level with its element-wise work folded in (one thread per row, the
+// block's slice of the matrix staged in shared memory with 16-byte loads):
+//
+//   down, level l (rhs b given, sol1 = F(D.*b) written by the producer of b):
+//     SMOOTH   (s-1 times)  x' = x + F(D .* F(b - A x))          Richardson steps 2..s
+//     DEFECT               d  = F(b - A x)                       MultiGrid defect (equals the
+//                                                                 smoother's own last defect)
+//     RESTRICT (coarse rows) b_c = F_c(R d), sol1_c = F_c(D_c .* b_c), ||b_c||
+//   coarsest: COARSE       x_c = exact inverse on the free DOFs
+//   up, level l:
+//     PROLONG              x  = x + F(P x_c)
+//     POST1                d  = F(b - A x), c = F(D .* d), ||d||  Richardson step 1
+//     POST2    (s-1 times) c' = c + F(D .* F(d - A c)); last: x = x + c'
+//
+// F zeroes Dirichlet rows (UnitFilter::filter_def/filter_cor).  Richardson's trailing defect of the
+// post-smoother is never read by the reference and is not computed.  Every product and sum is
+// rounded separately (no FMA), and rows are summed in stored entry order, so for FP64 each pass
+// reproduces the reference's generic backend bit for bit; only the global dot products and norms
+// are summed in a different (tree) order.
+//
+// PCG (kernel/solver/pcg.hpp:159-286) adds three passes per iteration: Q (q = F(A p), q.p ->
+// alpha), X (x += alpha p, r -= alpha q, ||r||, convergence test, next V-cycle input) and P
+// (p = z + beta p; r.z and beta come out of the top level's last POST2).  All scalars stay on the
+// device; with use_graph the whole solve is one CUDA graph whose loop is a device-side WHILE node.
+#include "fb_common.cuh"
+#include "fb_setup.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace fb
+{
+  constexpr int NT = 256;   // rows (threads) per block of every pass
+
+  // ------------------------------------------------------------------ device views
+  template<typename V>
+  struct DCsr
+  {
+    const uint32_t* rp;
+    const uint32_t* col;
+    const V* val;
+    uint32_t rows;
+    uint32_t cap;     // staging capacity in entries (multiple of 8); 0 = read rows directly
+  };
+
+  struct Scalars
+  {
+    double gamma, gamma_prev, alpha, beta;
+    double def_init, def_cur;
+    double tol_rel, tol_abs, div_rel, div_abs;
+    double mg_scale, mg_inv_scale;   // V-cycle input scaling (power of two; 1 in FP64 mode)
+    int iter, status, min_iter, max_iter;
+  };
+
+  template<typename V>
+  struct Staged
+  {
+    const V* sv;
+    const uint32_t* sc;
+    uint32_t offv, offc;
+    bool staged;
+  };
+
+  __device__ __forceinline__ uint4 ld_nc(const uint4* p)
+  {
+    uint4 v;
+    asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+    return v;
+  }
+
+  // Stage the block's entries [rp[r0], rp[r0+NT]) of col/val into shared memory.  The copy starts
+  // at the 16-byte boundary below the first entry and ends at the one above the last; device
+  // arrays are allocated with >= 16 bytes of padding, so the over-read stays inside them.
+  template<typename V>
+  __device__ __forceinline__ Staged<V> stage_rows(const DCsr<V>& M, uint32_t r0, unsigned char* smem)
+  {
+    Staged<V> s;
+    constexpr uint32_t EV = 16u / sizeof(V);
+    const uint32_t rend = min(r0 + uint32_t(NT), M.rows);
+    const uint32_t s0 = M.rp[r0], s1 = M.rp[rend];
+    const uint32_t a0v = s0 & ~(EV - 1u), a0c = s0 & ~3u;
+    const uint32_t nv4 = (s1 - a0v + EV - 1u) / EV, nc4 = (s1 - a0c + 3u) / 4u;
+    s.staged = (nv4 * EV <= M.cap) && (nc4 * 4u <= M.cap);
+    V* sv = reinterpret_cast<V*>(smem);
+    uint32_t* sc = reinterpret_cast<uint32_t*>(smem + size_t(M.cap) * sizeof(V));
+    if(s.staged)
+    {
+      const uint4* gv = reinterpret_cast<const uint4*>(M.val + a0v);
+      const uint4* gc = reinterpret_cast<const uint4*>(M.col + a0c);
+      uint4* dv = reinterpret_cast<uint4*>(sv);
+      uint4* dc = reinterpret_cast<uint4*>(sc);
+      for(uint32_t k = threadIdx.x; k < nv4; k += NT)
+        dv[k] = ld_nc(gv + k);
+      for(uint32_t k = threadIdx.x; k < nc4; k += NT)
+        dc[k] = ld_nc(gc + k);
+    }
+    __syncthreads();
+    s.sv = sv;
+    s.sc = sc;
+    s.offv = a0v;
+    s.offc = a0c;
+    return s;
+  }
+
+  template<typename V, typename S>
+  __device__ __forceinline__ typename ValueTraits<V>::acc row_sum(const Staged<V>& st, const DCsr<V>& M, uint32_t row,
+    const S* __restrict__ x)
+  {
+    typedef typename ValueTraits<V>::acc A;
+    const uint32_t j0 = M.rp[row], j1 = M.rp[row + 1];
+    A sum = A(0);
+    if(st.staged)
+    {
+      for(uint32_t j = j0; j < j1; ++j)
+        sum = add(sum, mul(to_acc(st.sv[j - st.offv]), A(x[st.sc[j - st.offc]])));
+    }
+    else
+    {
+      for(uint32_t j = j0; j < j1; ++j)
+        sum = add(sum, mul(to_acc(M.val[j]), A(x[M.col[j]])));
+    }
+    return sum;
+  }
+
+  __device__ __forceinline__ bool gate_closed(const Scalars* sc)
+  {
+    return sc->status != FB_SOLVER_PROGRESS;
+  }
+
+  template<typename S> __device__ __forceinline__ S eps_sq();
+  template<> __device__ __forceinline__ double eps_sq<double>() { return EPS64 * EPS64; }
+  template<> __device__ __forceinline__ float eps_sq<float>() { return EPS32 * EPS32; }
+
+  // Richardson's initial-defect test (iterative.hpp:748-771): smooth only if the norm is finite
+  // and above eps^2 of the smoother's precision.
+  template<typename S>
+  __device__ __forceinline__ int skip_from_norm(double nrm)
+  {
+    return (!isfinite(nrm) || nrm <= double(eps_sq<S>())) ? 1 : 0;
+  }
+
+  // ------------------------------------------------------------------ V-cycle passes
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_smooth(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+    S* __restrict__ xo, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip,
+    const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    if(i >= A.rows)
+      return;
+    S out = S(0);
+    if(!*skip)
+    {
+      const Ac sum = row_sum<V, S>(st, A, i, x);
+      const bool d = dm[i] != 0;
+      const Ac d1 = d ? Ac(0) : sub(Ac(b[i]), sum);
+      const Ac c = d ? Ac(0) : mul(Ac(dinv[i]), d1);
+      out = S(add(Ac(x[i]), c));
+    }
+    xo[i] = out;
+  }
+
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_defect(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+    S* __restrict__ d, const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    if(i >= A.rows)
+      return;
+    const Ac sum = row_sum<V, S>(st, A, i, x);
+    d[i] = dm[i] ? S(0) : S(sub(Ac(b[i]), sum));
+  }
+
+  // coarse rows: b_c = F_c(R d); with_sol: sol1_c = F_c(D_c .* b_c) and ||b_c|| -> skip flag
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_restrict(DCsr<V> R, const S* __restrict__ d, S* __restrict__ bc,
+    S* __restrict__ xc, const S* __restrict__ dinvc, const uint8_t* __restrict__ dmc, int* __restrict__ skipc,
+    RedSlot slot, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(R, r0, smem);
+    const uint32_t j = r0 + threadIdx.x;
+    double sq = 0.0;
+    if(j < R.rows)
+    {
+      const bool dc = dmc[j] != 0;
+      const Ac sum = row_sum<V, S>(st, R, j, d);
+      const Ac v = dc ? Ac(0) : add(sum, Ac(0));
+      bc[j] = S(v);
+      if(xc)
+      {
+        const Ac c = dc ? Ac(0) : mul(Ac(dinvc[j]), v);
+        xc[j] = S(add(Ac(0), c));
+      }
+      sq = double(v) * double(v);
+    }
+    if(!xc)
+      return;
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+      *skipc = skip_from_norm<S>(sqrt(total));
+  }
+
+  // exact coarse solve on the free DOFs (FP64 arithmetic whatever S is)
+  template<typename S>
+  __global__ void __launch_bounds__(NT) k_coarse(const S* __restrict__ b, S* __restrict__ x, uint32_t n,
+    const uint32_t* __restrict__ free_dofs, const double* __restrict__ inv, uint32_t m, const Scalars* __restrict__ sc)
+  {
+    if(gate_closed(sc))
+      return;
+    for(uint32_t i = threadIdx.x; i < n; i += NT)
+      x[i] = S(0);
+    __syncthreads();
+    for(uint32_t i = threadIdx.x; i < m; i += NT)
+    {
+      double s = 0.0;
+      for(uint32_t j = 0; j < m; ++j)
+        s = add(s, mul(inv[size_t(i) * m + j], double(b[free_dofs[j]])));
+      x[free_dofs[i]] = S(s);
+    }
+  }
+
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ x,
+    const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(P, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    if(i >= P.rows)
+      return;
+    const Ac sum = row_sum<V, S>(st, P, i, xc);
+    const Ac c = dm[i] ? Ac(0) : add(sum, Ac(0));
+    x[i] = S(add(Ac(x[i]), c));
+  }
+
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_post1(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+    S* __restrict__ d, S* __restrict__ c, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
+    int* __restrict__ skip, RedSlot slot, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    double sq = 0.0;
+    if(i < A.rows)
+    {
+      const bool dd = dm[i] != 0;
+      const Ac sum = row_sum<V, S>(st, A, i, x);
+      const Ac dv = dd ? Ac(0) : sub(Ac(b[i]), sum);
+      d[i] = S(dv);
+      const Ac cv = dd ? Ac(0) : mul(Ac(dinv[i]), dv);
+      c[i] = S(add(Ac(0), cv));
+      sq = double(dv) * double(dv);
+    }
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+      *skip = skip_from_norm<S>(sqrt(total));
+  }
+
+  // post-smoothing step k >= 2.  LAST: x += c'.  TOP (with LAST): z = x * inv_scale (FP64), and
+  // r.z -> gamma, beta (PCG).
+  template<typename V, typename S, bool LAST, bool TOP>
+  __global__ void __launch_bounds__(NT) k_post2(DCsr<V> A, const S* __restrict__ d, const S* __restrict__ c,
+    S* __restrict__ co, S* __restrict__ x, double* __restrict__ z, const double* __restrict__ r,
+    const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip, RedSlot slot,
+    Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<V> st = stage_rows<V>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    const bool skipped = *skip != 0;
+    double rz = 0.0;
+    if(i < A.rows)
+    {
+      Ac cn = Ac(0);
+      if(!skipped)
+      {
+        const bool dd = dm[i] != 0;
+        const Ac sum = row_sum<V, S>(st, A, i, c);
+        const Ac dk = dd ? Ac(0) : sub(Ac(d[i]), sum);
+        const Ac ck = dd ? Ac(0) : mul(Ac(dinv[i]), dk);
+        cn = add(Ac(c[i]), ck);
+      }
+      if(!LAST)
+        co[i] = S(cn);
+      else
+      {
+        const S xn = S(add(Ac(x[i]), cn));
+        if(TOP)
+        {
+          const double zi = mul(double(xn), sc->mg_inv_scale);
+          z[i] = zi;
+          rz = mul(r[i], zi);
+        }
+        else
+          x[i] = xn;
+      }
+    }
+    if(!(LAST && TOP))
+      return;
+    double total;
+    if(grid_sum_last<NT>(rz, slot, sh, total))
+    {
+      sc->gamma_prev = sc->gamma;
+      sc->gamma = total;
+      sc->beta = total / sc->gamma_prev;
+    }
+  }
+
+  // post-smoothing with a single step: x += c (skip -> x += 0).  TOP as above.
+  template<typename S, bool TOP>
+  __global__ void __launch_bounds__(NT) k_post_final(const S* __restrict__ c, S* __restrict__ x, double* __restrict__ z,
+    const double* __restrict__ r, const int* __restrict__ skip, uint32_t n, RedSlot slot, Scalars* __restrict__ sc)
+  {
+    typedef S Ac;
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    double rz = 0.0;
+    if(i < n)
+    {
+      const Ac cn = *skip ? Ac(0) : c[i];
+      const S xn = S(add(Ac(x[i]), cn));
+      if(TOP)
+      {
+        const double zi = mul(double(xn), sc->mg_inv_scale);
+        z[i] = zi;
+        rz = mul(r[i], zi);
+      }
+      else
+        x[i] = xn;
+    }
+    if(!TOP)
+      return;
+    double total;
+    if(grid_sum_last<NT>(rz, slot, sh, total))
+    {
+      sc->gamma_prev = sc->gamma;
+      sc->gamma = total;
+      sc->beta = total / sc->gamma_prev;
+    }
+  }
+
+  // ------------------------------------------------------------------ PCG passes (FP64)
+  // writes the V-cycle input of the top level: b = S(r * scale) (FP32 modes) and
+  // sol1 = F(D .* b); returns the scale used.
+  template<typename S>
+  __device__ __forceinline__ void mg_input(uint32_t i, double ri, bool dd, double scale, S* __restrict__ bt,
+    S* __restrict__ x1, const S* __restrict__ dinv)
+  {
+    const S b = S(mul(ri, scale));
+    if(bt)
+      bt[i] = b;
+    const S c = dd ? S(0) : mul(dinv[i], b);
+    x1[i] = add(S(0), c);
+  }
+
+  __device__ __forceinline__ double pow2_near_inverse(double v)
+  {
+    if(!(v > 0.0) || !isfinite(v))
+      return 1.0;
+    int e;
+    frexp(v, &e);
+    return ldexp(1.0, -e);
+  }
+
+  // r = F(rhs - A x), ||r|| -> def_init and the status (iterative.hpp:748-771).
+  // FP64 mode also writes the V-cycle input (sol1 = F(D .* r), b aliases r).
+  template<typename S>
+  __global__ void __launch_bounds__(NT) k_pcg_init(DCsr<double> A, const double* __restrict__ rhs,
+    const double* __restrict__ x, double* __restrict__ r, const uint8_t* __restrict__ dm, S* __restrict__ x1,
+    const S* __restrict__ dinv, int* __restrict__ skip_top, double* __restrict__ hist, RedSlot slot,
+    Scalars* __restrict__ sc, cudaGraphConditionalHandle cond)
+  {
+    __shared__ double sh[32];
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<double> st = stage_rows<double>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    double sq = 0.0;
+    if(i < A.rows)
+    {
+      const bool dd = dm[i] != 0;
+      const double sum = row_sum<double, double>(st, A, i, x);
+      const double rv = dd ? 0.0 : sub(rhs[i], sum);
+      r[i] = rv;
+      if(x1)
+        mg_input<S>(i, rv, dd, 1.0, (S*)nullptr, x1, dinv);
+      sq = mul(rv, rv);
+    }
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+    {
+      const double d0 = sqrt(total);
+      sc->def_init = d0;
+      sc->def_cur = d0;
+      sc->iter = 0;
+      sc->gamma = 0.0;
+      hist[0] = d0;
+      int status = FB_SOLVER_PROGRESS;
+      if(!isfinite(d0))
+        status = FB_SOLVER_ABORTED;
+      else if(d0 <= EPS64 * EPS64)
+        status = FB_SOLVER_SUCCESS;
+      sc->status = status;
+      sc->mg_scale = 1.0;
+      sc->mg_inv_scale = 1.0;
+      *skip_top = skip_from_norm<double>(d0);
+      (void)cond;
+    }
+  }
+
+  // V-cycle input of the top level from a FP64 vector v, scaled by a power of two near 1/||v||
+  // (scale_from_def) or 1.  Computes ||b|| -> skip flag of the top pre-smoother.
+  template<typename S>
+  __global__ void __launch_bounds__(NT) k_mg_prep(const double* __restrict__ v, S* __restrict__ bt,
+    S* __restrict__ x1, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, int* __restrict__ skip_top,
+    uint32_t n, int scale_from_def, RedSlot slot, Scalars* __restrict__ sc)
+  {
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    const double scale = scale_from_def ? pow2_near_inverse(sc->def_cur) : 1.0;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    double sq = 0.0;
+    if(i < n)
+    {
+      const double vi = v[i];
+      mg_input<S>(i, vi, dm[i] != 0, scale, bt, x1, dinv);
+      const double b = double(S(mul(vi, scale)));
+      sq = b * b;
+    }
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+    {
+      sc->mg_scale = scale;
+      sc->mg_inv_scale = 1.0 / scale;
+      *skip_top = skip_from_norm<S>(sqrt(total));
+    }
+  }
+
+  // q = F(A p), q.p -> alpha = gamma / (q.p)
+  __global__ void __launch_bounds__(NT) k_pcg_q(DCsr<double> A, const double* __restrict__ p, double* __restrict__ q,
+    const uint8_t* __restrict__ dm, RedSlot slot, Scalars* __restrict__ sc)
+  {
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t r0 = blockIdx.x * NT;
+    Staged<double> st = stage_rows<double>(A, r0, smem);
+    const uint32_t i = r0 + threadIdx.x;
+    double qp = 0.0;
+    if(i < A.rows)
+    {
+      const double sum = row_sum<double, double>(st, A, i, p);
+      const double qv = dm[i] ? 0.0 : add(sum, 0.0);
+      q[i] = qv;
+      qp = mul(qv, p[i]);
+    }
+    double total;
+    if(grid_sum_last<NT>(qp, slot, sh, total))
+      sc->alpha = sc->gamma / total;
+  }
+
+  // x += alpha p; r -= alpha q; ||r||, stopping test (iterative.hpp:492-507,795-879); the next
+  // V-cycle input (FP64: sol1 = F(D .* r); FP32: b = S(r * scale), sol1 = F(D .* b)).
+  template<typename S, bool CONVERT>
+  __global__ void __launch_bounds__(NT) k_pcg_x(double* __restrict__ x, double* __restrict__ r,
+    const double* __restrict__ p, const double* __restrict__ q, const uint8_t* __restrict__ dm, S* __restrict__ bt,
+    S* __restrict__ x1, const S* __restrict__ dinv, int* __restrict__ skip_top, double* __restrict__ hist, uint32_t n,
+    RedSlot slot, Scalars* __restrict__ sc, cudaGraphConditionalHandle cond)
+  {
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+    {
+      if(cond && blockIdx.x == 0 && threadIdx.x == 0)
+        cudaGraphSetConditional(cond, 0u);
+      return;
+    }
+    const double alpha = sc->alpha;
+    const double scale = CONVERT ? pow2_near_inverse(sc->def_cur) : 1.0;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    double sq = 0.0;
+    if(i < n)
+    {
+      x[i] = add(x[i], mul(alpha, p[i]));
+      const double rv = add(r[i], mul(-alpha, q[i]));
+      r[i] = rv;
+      mg_input<S>(i, rv, dm[i] != 0, scale, CONVERT ? bt : (S*)nullptr, x1, dinv);
+      sq = mul(rv, rv);
+    }
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+    {
+      const int it = sc->iter + 1;
+      const double dc = sqrt(total);
+      sc->iter = it;
+      sc->def_cur = dc;
+      hist[it] = dc;
+      int status = FB_SOLVER_PROGRESS;
+      if(!isfinite(dc))
+        status = FB_SOLVER_ABORTED;
+      else if(dc > sc->div_abs || dc > sc->div_rel * sc->def_init)
+        status = FB_SOLVER_DIVERGED;
+      else if(it < sc->min_iter)
+        status = FB_SOLVER_PROGRESS;
+      else if(dc <= sc->tol_abs && (dc <= sc->tol_rel * sc->def_init || dc <= 0.0))
+        status = FB_SOLVER_SUCCESS;
+      else if(it >= sc->max_iter)
+        status = FB_SOLVER_MAX_ITER;
+      sc->status = status;
+      sc->mg_scale = scale;
+      sc->mg_inv_scale = 1.0 / scale;
+      *skip_top = skip_from_norm<S>(dc * scale);
+      if(cond)
+        cudaGraphSetConditional(cond, status == FB_SOLVER_PROGRESS ? 1u : 0u);
+    }
+  }
+
+  // p = z (first) or p = beta p + z (axpy_generic.hpp:34-39 rounding: fl(fl(p*beta) + z))
+  __global__ void __launch_bounds__(NT) k_pcg_p(double* __restrict__ p, const double* __restrict__ z, uint32_t n,
+    int first, const Scalars* __restrict__ sc)
+  {
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    if(i >= n)
+      return;
+    p[i] = first ? z[i] : add(mul(p[i], sc->beta), z[i]);
+  }
+
+  // permutation gathers for the caller <-> device numbering
+  __global__ void k_gather(double* __restrict__ out, const double* __restrict__ in, const uint32_t* __restrict__ perm, uint32_t n)
+  {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n)
+      out[i] = in[perm[i]];
+  }
+  __global__ void k_scatter(double* __restrict__ out, const double* __restrict__ in, const uint32_t* __restrict__ perm, uint32_t n)
+  {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i < n)
+      out[perm[i]] = in[i];
+  }
+  __global__ void k_set_status(Scalars* sc, int status)
+  {
+    sc->status = status;
+  }
+} // namespace fb
+
+// ==================================================================== host side
+struct fb_hierarchy
+{
+  std::vector<fb::HostLevel> levels;
+};
+
+namespace fb
+{
+  struct DevBuf
+  {
+    void* p = nullptr;
+    ~DevBuf() { if(p) cudaFree(p); }
+  };
+
+  struct DevMat
+  {
+    uint32_t rows = 0, cols = 0, nnz = 0, cap = 0;
+    uint32_t *rp = nullptr, *col = nullptr;
+    void* val = nullptr;   // value array in the level's storage type
+    size_t smem = 0;
+  };
+
+  template<typename V> DCsr<V> view(const DevMat& m)
+  {
+    return DCsr<V>{m.rp, m.col, static_cast<const V*>(m.val), m.rows, m.cap};
+  }
+
+  struct DevLevel
+  {
+    uint32_t n = 0;
+    DevMat A, P, R;          // MG storage precision
+    DevMat A64;              // FP64 top-level matrix for PCG (FP32 modes, level 0 only)
+    uint8_t* dm = nullptr;
+    void* dinv = nullptr;    // S
+    void *b = nullptr, *x = nullptr, *x2 = nullptr, *d = nullptr, *c = nullptr, *c2 = nullptr;
+    int* skip_pre = nullptr;
+    int* skip_post = nullptr;
+  };
+} // namespace fb
+
+struct fb_solver
+{
+  fb_solver_config cfg;
+  fb_hierarchy* h = nullptr;
+  int nlev = 0;
+  int vsize = 8;   // bytes per MG vector entry
+  std::vector<fb::DevLevel> lv;
+  std::vector<void*> allocs;
+  std::vector<std::vector<uint32_t>> perms;   // per level; empty = identity
+  // coarse
+  uint32_t* free_dofs = nullptr;
+  double* cinv = nullptr;
+  uint32_t nfree = 0;
+  // PCG
+  double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *z = nullptr, *rhs = nullptr;
+  double *tmp_in = nullptr, *tmp_out = nullptr;
+  void* flush = nullptr;   // L2 flush buffer of fb_solver_time_kernel (allocated on first use)
+  uint32_t* perm0 = nullptr;
+  double* hist = nullptr;
+  fb::Scalars* sc = nullptr;
+  fb::RedSlot slot{nullptr, nullptr};
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaGraph_t vgraph = nullptr;
+  cudaGraphExec_t vexec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint64_t launches_init = 0, launches_body = 0, launches_vcycle = 0;
+  double bytes_init = 0, bytes_body = 0;
+  uint64_t counting = 0;
+  double counting_bytes = 0;
+};
+
+namespace fb
+{
+  static fb_status dalloc(fb_solver* s, void** p, size_t bytes)
+  {
+    cudaError_t e = cudaMalloc(p, bytes + 64);
+    if(e != cudaSuccess)
+    {
+      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      return FB_ERR_NOMEM;
+    }
+    s->allocs.push_back(*p);
+    e = cudaMemset(*p, 0, bytes + 64);
+    if(e != cudaSuccess)
+      return cuda_fail(e, "cudaMemset");
+    return FB_OK;
+  }
+
+#define FB_TRY(x)                     \
+  do {                                \
+    fb_status fb_t_ = (x);            \
+    if(fb_t_ != FB_OK) return fb_t_;  \
+  } while(0)
+
+  static size_t vsize_of(int prec) { return prec == FB_PREC_F64 ? 8 : 4; }
+  static size_t valsize_of(int prec) { return prec == FB_PREC_F64 ? 8 : (prec == FB_PREC_F32 ? 4 : 2); }
+
+  // staging capacity: max over blocks of the aligned slice length, if it fits 96 KB of shared memory
+  static uint32_t staging_cap(const HostCsr& M, size_t vbytes)
+  {
+    uint32_t cap = 0;
+    for(uint32_t r0 = 0; r0 < M.rows; r0 += NT)
+    {
+      const uint32_t re = std::min<uint32_t>(r0 + NT, M.rows);
+      const uint32_t len = M.rp[re] - M.rp[r0] + 16u;
+      cap = std::max(cap, len);
+    }
+    cap = (cap + 7u) & ~7u;
+    const size_t limit = 96 * 1024;
+    if(size_t(cap) * (vbytes + 4) > limit)
+      cap = uint32_t(limit / (vbytes + 4)) & ~7u;
+    return cap;
+  }
+
+  static uint16_t to_bf16_rne(float f)
+  {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if((u & 0x7f800000u) == 0x7f800000u)
+      return uint16_t(u >> 16) | ((u & 0xffffu) ? 0x40u : 0u);
+    const uint32_t lsb = (u >> 16) & 1u;
+    u += 0x7fffu + lsb;
+    return uint16_t(u >> 16);
+  }
+
+  static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec)
+  {
+    d.rows = M.rows;
+    d.cols = M.cols;
+    d.nnz = uint32_t(M.nnz());
+    const size_t vb = valsize_of(prec);
+    d.cap = staging_cap(M, vb);
+    d.smem = size_t(d.cap) * (vb + 4);
+    FB_TRY(dalloc(s, (void**)&d.rp, sizeof(uint32_t) * (size_t(M.rows) + 1)));
+    FB_TRY(dalloc(s, (void**)&d.col, sizeof(uint32_t) * std::max<size_t>(1, M.nnz())));
+    FB_TRY(dalloc(s, &d.val, vb * std::max<size_t>(1, M.nnz())));
+    FB_CUDA(cudaMemcpy(d.rp, M.rp.data(), sizeof(uint32_t) * (size_t(M.rows) + 1), cudaMemcpyHostToDevice));
+    if(M.nnz())
+    {
+      FB_CUDA(cudaMemcpy(d.col, M.col.data(), sizeof(uint32_t) * M.nnz(), cudaMemcpyHostToDevice));
+      if(prec == FB_PREC_F64)
+        FB_CUDA(cudaMemcpy(d.val, M.val.data(), 8 * M.nnz(), cudaMemcpyHostToDevice));
+      else if(prec == FB_PREC_F32)
+      {
+        std::vector<float> f(M.nnz());
+        for(size_t k = 0; k < f.size(); ++k)
+          f[k] = float(M.val[k]);
+        FB_CUDA(cudaMemcpy(d.val, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
+      }
+      else
+      {
+        std::vector<uint16_t> h(M.nnz());
+        for(size_t k = 0; k < h.size(); ++k)
+          h[k] = to_bf16_rne(float(M.val[k]));
+        FB_CUDA(cudaMemcpy(d.val, h.data(), 2 * h.size(), cudaMemcpyHostToDevice));
+      }
+    }
+    return FB_OK;
+  }
+
+  template<typename S>
+  static fb_status upload_vec(fb_solver* s, void** dst, const std::vector<double>& v)
+  {
+    FB_TRY(dalloc(s, dst, sizeof(S) * std::max<size_t>(1, v.size())));
+    std::vector<S> t(v.begin(), v.end());
+    FB_CUDA(cudaMemcpy(*dst, t.data(), sizeof(S) * t.size(), cudaMemcpyHostToDevice));
+    return FB_OK;
+  }
+
+  static unsigned int blocks(uint32_t n) { return std::max(1u, (n + NT - 1) / NT); }
+
+  // ---------------------------------------------------------------- launch sequences
+  template<typename V, typename S>
+  struct Launcher
+  {
+    fb_solver* s;
+    cudaStream_t st;
+    bool dry = false;          // count launches and bytes only
+    uint64_t launches = 0;
+    double bytes = 0;
+
+    DevLevel& L(int i) { return s->lv[size_t(i)]; }
+
+    // algorithmic bytes of one CSR sweep: nnz*(val+idx) + (rows+1)*idx + reads of x + rows*out
+    double csr_bytes(const DevMat& m, double vec_in, double vec_out)
+    {
+      return double(m.nnz) * (double(valsize_of(s->cfg.precision)) + 4.0) + double(m.rows + 1) * 4.0 +
+             double(m.cols) * sizeof(S) + double(m.rows) * sizeof(S) * (vec_in + vec_out);
+    }
+
+    // V-cycle from the top level; the top level's b and sol1 and skip_pre are in place.
+    // Returns the buffer holding the top level's solution (for non-PCG use).
+    void vcycle(bool pcg_top)
+    {
+      const int nl = s->nlev;
+      const int steps = std::max(1, s->cfg.smooth_steps);
+      std::vector<void*> xcur(static_cast<size_t>(nl));
+      for(int l = 0; l + 1 < nl; ++l)
+      {
+        DevLevel& f = L(l);
+        DevLevel& c = L(l + 1);
+        void* xa = f.x;
+        void* xb = f.x2;
+        for(int k = 1; k < steps; ++k)
+        {
+          if(!dry) k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+            (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
+          ++launches;
+          bytes += csr_bytes(f.A, 3, 1) + f.n;
+          std::swap(xa, xb);
+        }
+        xcur[size_t(l)] = xa;
+        if(!dry) k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.A, 1, 1) + f.n;
+        const bool coarsest = (l + 2 == nl);
+        if(!dry) k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
+          coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
+      }
+      {
+        DevLevel& c = L(nl - 1);
+        if(!dry) k_coarse<S><<<1, NT, 0, st>>>((const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
+        ++launches;
+        bytes += double(s->nfree) * s->nfree * 8.0 + double(c.n) * 2 * sizeof(S);
+        xcur[size_t(nl - 1)] = c.x;
+      }
+      for(int l = nl - 2; l >= 0; --l)
+      {
+        DevLevel& f = L(l);
+        void* xf = xcur[size_t(l)];
+        if(!dry) k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.P, 1, 1) + f.n;
+        if(!dry) k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+          (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.A, 2, 2) + f.n;
+        const bool top = pcg_top && l == 0;
+        void* ca = f.c;
+        void* cb = f.c2;
+        if(steps == 1)
+        {
+          if(!dry)
+          {
+            if(top)
+              k_post_final<S, true><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot, s->sc);
+            else
+              k_post_final<S, false><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n, s->slot, s->sc);
+          }
+          ++launches;
+          bytes += double(f.n) * sizeof(S) * 3;
+        }
+        for(int k = 2; k <= steps; ++k)
+        {
+          const bool last = (k == steps);
+          if(dry)
+            ;
+          else if(!last)
+            k_post2<V, S, false, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+              (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+          else if(top)
+            k_post2<V, S, true, true><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+              (S*)cb, (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+          else
+            k_post2<V, S, true, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+              (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+          ++launches;
+          bytes += csr_bytes(f.A, 3, 1) + f.n;
+          std::swap(ca, cb);
+        }
+      }
+    }
+
+    const DevMat& A64() { return s->cfg.precision == FB_PREC_F64 ? L(0).A : L(0).A64; }
+
+    void pcg_init()
+    {
+      DevLevel& t = L(0);
+      const bool f64 = s->cfg.precision == FB_PREC_F64;
+      const DevMat& A = A64();
+      if(!dry) k_pcg_init<S><<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->rhs, s->x, s->r, t.dm,
+        f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->hist, s->slot, s->sc, 0);
+      ++launches;
+      bytes += double(A.nnz) * 12.0 + double(t.n + 1) * 4 + double(t.n) * 8 * 4 + t.n;
+      if(!f64)
+      {
+        if(!dry) k_mg_prep<S><<<blocks(t.n), NT, 0, st>>>(s->r, (S*)t.b, (S*)t.x, (const S*)t.dinv, t.dm, t.skip_pre, t.n, 1,
+          s->slot, s->sc);
+        ++launches;
+        bytes += double(t.n) * (8 + 3 * sizeof(S)) + t.n;
+      }
+    }
+
+    void pcg_tail(bool first, cudaGraphConditionalHandle cond)
+    {
+      DevLevel& t = L(0);
+      const bool f64 = s->cfg.precision == FB_PREC_F64;
+      const DevMat& A = A64();
+      if(!dry) k_pcg_p<<<blocks(t.n), NT, 0, st>>>(s->p, s->z, t.n, first ? 1 : 0, s->sc);
+      if(!dry) k_pcg_q<<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->p, s->q, t.dm, s->slot, s->sc);
+      if(dry)
+        ;
+      else if(f64)
+        k_pcg_x<S, false><<<blocks(t.n), NT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
+          (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
+      else
+        k_pcg_x<S, true><<<blocks(t.n), NT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)t.b, (S*)t.x,
+          (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
+      launches += 3;
+      bytes += double(t.n) * 8 * (first ? 2 : 3);                                    // P
+      bytes += double(A.nnz) * 12.0 + double(t.n + 1) * 4 + double(t.n) * 8 * 3 + t.n; // Q
+      bytes += double(t.n) * 8 * 6 + double(t.n) * (f64 ? 16 : 12) + t.n;             // X
+    }
+  };
+
+  template<typename V, typename S>
+  static fb_status set_smem_attrs()
+  {
+    const int mx = 100 * 1024;
+    FB_CUDA(cudaFuncSetAttribute(k_smooth<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_defect<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_restrict<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_prolong<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_post1<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_pcg_init<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_pcg_q, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    return FB_OK;
+  }
+
+  template<typename V, typename S>
+  static fb_status build_graphs(fb_solver* s)
+  {
+    cudaStream_t st = s->stream;
+    {
+      Launcher<V, S> li{s, st, true};
+      li.pcg_init();
+      li.vcycle(true);
+      li.pcg_tail(true, 0);
+      s->launches_init = li.launches;
+      s->bytes_init = li.bytes;
+      Launcher<V, S> lb{s, st, true};
+      lb.vcycle(true);
+      lb.pcg_tail(false, 0);
+      s->launches_body = lb.launches;
+      s->bytes_body = lb.bytes;
+      Launcher<V, S> lv{s, st, true};
+      lv.vcycle(false);
+      s->launches_vcycle = lv.launches + 2;
+    }
+    if(!s->cfg.use_graph)
+      return FB_OK;
+    FB_CUDA(cudaGraphCreate(&s->graph, 0));
+    cudaGraphConditionalHandle cond;
+    FB_CUDA(cudaGraphConditionalHandleCreate(&cond, s->graph, 0u, cudaGraphCondAssignDefault));
+    FB_CUDA(cudaStreamBeginCaptureToGraph(st, s->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    {
+      Launcher<V, S> l{s, st, false};
+      l.pcg_init();
+      l.vcycle(true);
+      l.pcg_tail(true, cond);
+    }
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t capg = nullptr;
+    FB_CUDA(cudaStreamGetCaptureInfo(st, &cst, nullptr, &capg, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    FB_CUDA(cudaGraphAddNode(&cnode, capg, deps, ndeps, &cp));
+    FB_CUDA(cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t g_out = nullptr;
+    FB_CUDA(cudaStreamEndCapture(st, &g_out));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    FB_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    {
+      Launcher<V, S> l{s, st, false};
+      l.vcycle(true);
+      l.pcg_tail(false, cond);
+    }
+    cudaGraph_t b_out = nullptr;
+    FB_CUDA(cudaStreamEndCapture(st, &b_out));
+    FB_CUDA(cudaGraphInstantiate(&s->gexec, s->graph, 0));
+    return FB_OK;
+  }
+
+  template<typename V, typename S>
+  static fb_status run_solve(fb_solver* s)
+  {
+    cudaStream_t st = s->stream;
+    if(s->cfg.use_graph)
+    {
+      FB_CUDA(cudaGraphLaunch(s->gexec, st));
+      FB_CUDA(cudaGetLastError());
+      return FB_OK;
+    }
+    Launcher<V, S> li{s, st, false};
+    li.pcg_init();
+    li.vcycle(true);
+    li.pcg_tail(true, 0);
+    FB_LAUNCHED(0);
+    while(true)
+    {
+      Scalars h;
+      FB_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+      FB_CUDA(cudaStreamSynchronize(st));
+      if(h.status != FB_SOLVER_PROGRESS)
+        break;
+      Launcher<V, S> lb{s, st, false};
+      lb.vcycle(true);
+      lb.pcg_tail(false, 0);
+      FB_LAUNCHED(0);
+    }
+    return FB_OK;
+  }
+
+  template<typename V, typename S>
+  static fb_status run_vcycle(fb_solver* s)
+  {
+    cudaStream_t st = s->stream;
+    DevLevel& t = s->lv[0];
+    Launcher<V, S> l{s, st, false};
+    // the status gate must be open for the V-cycle passes
+    k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_PROGRESS);
+    // FP64 mode: the top level's b aliases r and is not rewritten
+    const bool f64 = s->cfg.precision == FB_PREC_F64;
+    k_mg_prep<S><<<blocks(t.n), NT, 0, st>>>(s->r, f64 ? (S*)nullptr : (S*)t.b, (S*)t.x, (const S*)t.dinv, t.dm,
+      t.skip_pre, t.n, 0, s->slot, s->sc);
+    FB_LAUNCHED(2);
+    l.vcycle(false);
+    FB_LAUNCHED(l.launches);
+    return FB_OK;
+  }
+} // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+void fb_solver_config_default(fb_solver_config* c)
+{
+  if(!c)
+    return;
+  c->precision = FB_PREC_F64;
+  c->ordering = FB_ORDER_NATIVE;
+  c->omega = 0.7;
+  c->smooth_steps = 2;
+  c->tol_rel = 1e-8;
+  c->tol_abs = 1.0 / (EPS64 * EPS64);
+  c->max_iter = 100;
+  c->min_iter = 0;
+  c->use_graph = 1;
+  c->rows_per_block = 0;
+}
+
+fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
+{
+  if(!out || num_levels < 1 || num_levels > 32)
+  {
+    set_error("hierarchy_create: bad arguments");
+    return FB_ERR_ARG;
+  }
+  *out = new fb_hierarchy();
+  (*out)->levels.resize(size_t(num_levels));
+  return FB_OK;
+}
+
+void fb_hierarchy_destroy(fb_hierarchy* h) { delete h; }
+
+fb_status fb_hierarchy_set_level(fb_hierarchy* h, int level, const fb_csr_host* A, const uint64_t* filter_idx,
+  const double* filter_val, uint64_t nf, const fb_csr_host* P, const fb_csr_host* R)
+{
+  if(!h || level < 0 || size_t(level) >= h->levels.size() || !A)
+  {
+    set_error("hierarchy_set_level: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const bool coarsest = size_t(level) + 1 == h->levels.size();
+  if(!coarsest && (!P || !R))
+  {
+    set_error("hierarchy_set_level: P and R are required on every level but the coarsest");
+    return FB_ERR_ARG;
+  }
+  if(A->rows != A->columns)
+  {
+    set_error("hierarchy_set_level: system matrix is not square");
+    return FB_ERR_ARG;
+  }
+  HostLevel& L = h->levels[size_t(level)];
+  std::string e = import_csr(L.A, A->rows, A->columns, A->used_elements, A->row_ptr, A->col_ind, A->val, false);
+  if(e.empty() && !coarsest)
+  {
+    if(P->rows != A->rows || R->columns != A->rows || R->rows != P->columns)
+      e = "transfer matrix sizes do not match the system matrix";
+    if(e.empty())
+      e = import_csr(L.P, P->rows, P->columns, P->used_elements, P->row_ptr, P->col_ind, P->val, true);
+    if(e.empty())
+      e = import_csr(L.R, R->rows, R->columns, R->used_elements, R->row_ptr, R->col_ind, R->val, true);
+  }
+  if(!e.empty())
+  {
+    set_error("hierarchy_set_level: " + e);
+    return FB_ERR_ARG;
+  }
+  L.dmask.assign(A->rows, 0);
+  L.fidx.assign(filter_idx, filter_idx + nf);
+  L.fval.assign(filter_val ? filter_val : filter_val, filter_val ? filter_val + nf : filter_val);
+  for(uint64_t k = 0; k < nf; ++k)
+  {
+    if(filter_idx[k] >= A->rows)
+    {
+      set_error("hierarchy_set_level: filter index out of range");
+      return FB_ERR_ARG;
+    }
+    L.dmask[filter_idx[k]] = 1;
+  }
+  L.set = true;
+  return FB_OK;
+}
+
+void fb_solver_destroy(fb_solver* s)
+{
+  if(!s)
+    return;
+  if(s->gexec) cudaGraphExecDestroy(s->gexec);
+  if(s->graph) cudaGraphDestroy(s->graph);
+  if(s->ev0) cudaEventDestroy(s->ev0);
+  if(s->ev1) cudaEventDestroy(s->ev1);
+  if(s->stream) cudaStreamDestroy(s->stream);
+  for(void* p : s->allocs)
+    cudaFree(p);
+  delete s;
+}
+
+fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_config* cfg_in)
+{
+  if(!out || !h)
+  {
+    set_error("solver_create: bad arguments");
+    return FB_ERR_ARG;
+  }
+  for(const HostLevel& L : h->levels)
+    if(!L.set)
+    {
+      set_error("solver_create: every level must be set");
+      return FB_ERR_STATE;
+    }
+  fb_solver_config cfg;
+  if(cfg_in)
+    cfg = *cfg_in;
+  else
+    fb_solver_config_default(&cfg);
+  if(cfg.precision < FB_PREC_F64 || cfg.precision > FB_PREC_F32_BF16 || cfg.smooth_steps < 1 || cfg.max_iter < 0)
+  {
+    set_error("solver_create: bad configuration");
+    return FB_ERR_ARG;
+  }
+  std::unique_ptr<fb_solver, void (*)(fb_solver*)> s(new fb_solver(), fb_solver_destroy);
+  s->cfg = cfg;
+  s->h = h;
+  s->nlev = int(h->levels.size());
+  const int prec = cfg.precision;
+  FB_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  FB_CUDA(cudaEventCreate(&s->ev0));
+  FB_CUDA(cudaEventCreate(&s->ev1));
+
+  // orderings (device row k = caller row perm[k])
+  s->perms.assign(size_t(s->nlev), std::vector<uint32_t>());
+  if(cfg.ordering == FB_ORDER_RCM)
+    for(int l = 0; l < s->nlev; ++l)
+      s->perms[size_t(l)] = rcm_order(h->levels[size_t(l)].A);
+
+  s->lv.resize(size_t(s->nlev));
+  const size_t vs = vsize_of(prec);
+  uint32_t max_blocks = 1;
+  for(int l = 0; l < s->nlev; ++l)
+  {
+    const HostLevel& H = h->levels[size_t(l)];
+    DevLevel& D = s->lv[size_t(l)];
+    const std::vector<uint32_t>& pf = s->perms[size_t(l)];
+    const std::vector<uint32_t> inv_f = pf.empty() ? std::vector<uint32_t>() : inverse_perm(pf);
+    D.n = H.A.rows;
+    max_blocks = std::max(max_blocks, blocks(D.n));
+    HostCsr A = permute(H.A, pf, inv_f);
+    FB_TRY(upload_mat(s.get(), D.A, A, prec));
+    if(l == 0 && prec != FB_PREC_F64)
+      FB_TRY(upload_mat(s.get(), D.A64, A, FB_PREC_F64));
+    if(l + 1 < s->nlev)
+    {
+      const std::vector<uint32_t>& pc = s->perms[size_t(l + 1)];
+      const std::vector<uint32_t> inv_c = pc.empty() ? std::vector<uint32_t>() : inverse_perm(pc);
+      FB_TRY(upload_mat(s.get(), D.P, permute(H.P, pf, inv_c), prec));
+      FB_TRY(upload_mat(s.get(), D.R, permute(H.R, pc, inv_f), prec));
+    }
+    std::vector<uint8_t> dm(D.n);
+    for(uint32_t k = 0; k < D.n; ++k)
+      dm[k] = H.dmask[pf.empty() ? k : pf[k]];
+    FB_TRY(dalloc(s.get(), (void**)&D.dm, D.n));
+    FB_CUDA(cudaMemcpy(D.dm, dm.data(), D.n, cudaMemcpyHostToDevice));
+    std::vector<double> dinv = inv_diagonal(A, cfg.omega);
+    if(prec == FB_PREC_F64)
+      FB_TRY(upload_vec<double>(s.get(), &D.dinv, dinv));
+    else
+      FB_TRY(upload_vec<float>(s.get(), &D.dinv, dinv));
+    for(void** v : {&D.b, &D.x, &D.x2, &D.d, &D.c, &D.c2})
+      FB_TRY(dalloc(s.get(), v, vs * D.n));
+    FB_TRY(dalloc(s.get(), (void**)&D.skip_pre, 2 * sizeof(int)));
+    D.skip_post = D.skip_pre + 1;
+    if(l == s->nlev - 1)
+    {
+      // exact inverse on the caller numbering; free DOFs mapped to device rows
+      std::vector<uint32_t> fr;
+      std::vector<double> inv;
+      coarse_inverse(H.A, H.dmask, fr, inv);
+      const std::vector<uint32_t> invp = pf.empty() ? std::vector<uint32_t>() : inverse_perm(pf);
+      for(uint32_t& f : fr)
+        f = invp.empty() ? f : invp[f];
+      s->nfree = uint32_t(fr.size());
+      FB_TRY(dalloc(s.get(), (void**)&s->free_dofs, sizeof(uint32_t) * std::max<size_t>(1, fr.size())));
+      FB_TRY(dalloc(s.get(), (void**)&s->cinv, sizeof(double) * std::max<size_t>(1, inv.size())));
+      if(!fr.empty())
+      {
+        FB_CUDA(cudaMemcpy(s->free_dofs, fr.data(), sizeof(uint32_t) * fr.size(), cudaMemcpyHostToDevice));
+        FB_CUDA(cudaMemcpy(s->cinv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
+      }
+    }
+  }
+  // FP64 mode: the top level's V-cycle input b aliases the PCG defect r
+  const uint32_t n0 = s->lv[0].n;
+  FB_TRY(dalloc(s.get(), (void**)&s->x, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->r, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->p, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->q, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->rhs, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->tmp_in, 8 * size_t(n0)));
+  FB_TRY(dalloc(s.get(), (void**)&s->tmp_out, 8 * size_t(n0)));
+  if(prec == FB_PREC_F64)
+  {
+    s->lv[0].b = s->r;
+    // z is the top level's final solution buffer: POST2 (TOP) writes it directly
+    FB_TRY(dalloc(s.get(), (void**)&s->z, 8 * size_t(n0)));
+  }
+  else
+    FB_TRY(dalloc(s.get(), (void**)&s->z, 8 * size_t(n0)));
+  if(!s->perms[0].empty())
+  {
+    FB_TRY(dalloc(s.get(), (void**)&s->perm0, sizeof(uint32_t) * n0));
+    FB_CUDA(cudaMemcpy(s->perm0, s->perms[0].data(), sizeof(uint32_t) * n0, cudaMemcpyHostToDevice));
+  }
+  FB_TRY(dalloc(s.get(), (void**)&s->hist, sizeof(double) * (size_t(cfg.max_iter) + 2)));
+  FB_TRY(dalloc(s.get(), (void**)&s->sc, sizeof(Scalars)));
+  FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * (max_blocks + 1)));
+  FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
+  Scalars h0;
+  std::memset(&h0, 0, sizeof(h0));
+  h0.tol_rel = cfg.tol_rel;
+  h0.tol_abs = cfg.tol_abs;
+  h0.div_rel = 1.0 / EPS64;
+  h0.div_abs = 1.0 / (EPS64 * EPS64);
+  h0.min_iter = cfg.min_iter;
+  h0.max_iter = cfg.max_iter;
+  h0.mg_scale = 1.0;
+  h0.mg_inv_scale = 1.0;
+  FB_CUDA(cudaMemcpy(s->sc, &h0, sizeof(h0), cudaMemcpyHostToDevice));
+
+  fb_status e = FB_OK;
+  if(prec == FB_PREC_F64)
+  {
+    e = set_smem_attrs<double, double>();
+    if(e == FB_OK) e = build_graphs<double, double>(s.get());
+  }
+  else if(prec == FB_PREC_F32)
+  {
+    e = set_smem_attrs<float, float>();
+    if(e == FB_OK) e = set_smem_attrs<double, float>();
+    if(e == FB_OK) e = build_graphs<float, float>(s.get());
+  }
+  else
+  {
+    e = set_smem_attrs<bf16_t, float>();
+    if(e == FB_OK) e = set_smem_attrs<double, float>();
+    if(e == FB_OK) e = build_graphs<bf16_t, float>(s.get());
+  }
+  if(e != FB_OK)
+    return e;
+  FB_CUDA(cudaDeviceSynchronize());
+  *out = s.release();
+  return FB_OK;
+}
+
+} // extern "C"
+
+namespace fb
+{
+  template<typename V, typename S>
+  static fb_status solve_dispatch(fb_solver* s) { return run_solve<V, S>(s); }
+  template<typename V, typename S>
+  static fb_status vcycle_dispatch(fb_solver* s) { return run_vcycle<V, S>(s); }
+
+} // namespace fb
+
+extern "C" {
+
+static fb_status solve_common(fb_solver* s, fb_solve_info* info)
+{
+  cudaStream_t st = s->stream;
+  const uint32_t n0 = s->lv[0].n;
+  FB_CUDA(cudaEventRecord(s->ev0, st));
+  fb_status e = FB_OK;
+  if(s->cfg.precision == FB_PREC_F64)
+    e = solve_dispatch<double, double>(s);
+  else if(s->cfg.precision == FB_PREC_F32)
+    e = solve_dispatch<float, float>(s);
+  else
+    e = solve_dispatch<bf16_t, float>(s);
+  if(e != FB_OK)
+    return e;
+  FB_CUDA(cudaEventRecord(s->ev1, st));
+  Scalars h;
+  FB_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+  FB_CUDA(cudaStreamSynchronize(st));
+  (void)n0;
+  count_launches(s->launches_init + (h.iter > 1 ? uint64_t(h.iter - 1) : 0) * s->launches_body);
+  if(info)
+  {
+    info->status = h.status;
+    info->iterations = h.iter;
+    info->def_init = h.def_init;
+    info->def_final = h.def_cur;
+    float ms = 0.f;
+    FB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    info->solve_ms = double(ms);
+    const uint64_t body_runs = h.iter > 1 ? uint64_t(h.iter - 1) : 0;
+    info->kernel_launches = s->launches_init + body_runs * s->launches_body;
+    info->bytes_moved = s->bytes_init + double(body_runs) * s->bytes_body;
+  }
+  return FB_OK;
+}
+
+// copies a caller-numbered device vector into the device numbering (or plain copy)
+static fb_status to_device_order(fb_solver* s, double* dst, const double* src)
+{
+  const uint32_t n = s->lv[0].n;
+  if(s->perm0)
+  {
+    k_gather<<<blocks(n), NT, 0, s->stream>>>(dst, src, s->perm0, n);
+    FB_LAUNCHED(1);
+  }
+  else
+    FB_CUDA(cudaMemcpyAsync(dst, src, 8 * size_t(n), cudaMemcpyDeviceToDevice, s->stream));
+  return FB_OK;
+}
+
+static fb_status from_device_order(fb_solver* s, double* dst, const double* src)
+{
+  const uint32_t n = s->lv[0].n;
+  if(s->perm0)
+  {
+    k_scatter<<<blocks(n), NT, 0, s->stream>>>(dst, src, s->perm0, n);
+    FB_LAUNCHED(1);
+  }
+  else
+    FB_CUDA(cudaMemcpyAsync(dst, src, 8 * size_t(n), cudaMemcpyDeviceToDevice, s->stream));
+  return FB_OK;
+}
+
+fb_status fb_solver_solve(fb_solver* s, double* sol, const double* rhs, fb_solve_info* info)
+{
+  if(!s || !sol || !rhs)
+  {
+    set_error("solver_solve: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const uint32_t n = s->lv[0].n;
+  FB_CUDA(cudaMemcpyAsync(s->tmp_in, rhs, 8 * size_t(n), cudaMemcpyHostToDevice, s->stream));
+  FB_TRY(to_device_order(s, s->rhs, s->tmp_in));
+  FB_CUDA(cudaMemcpyAsync(s->tmp_in, sol, 8 * size_t(n), cudaMemcpyHostToDevice, s->stream));
+  FB_TRY(to_device_order(s, s->x, s->tmp_in));
+  FB_TRY(solve_common(s, info));
+  FB_TRY(from_device_order(s, s->tmp_out, s->x));
+  FB_CUDA(cudaMemcpyAsync(sol, s->tmp_out, 8 * size_t(n), cudaMemcpyDeviceToHost, s->stream));
+  FB_CUDA(cudaStreamSynchronize(s->stream));
+  return FB_OK;
+}
+
+fb_status fb_solver_solve_device(fb_solver* s, double* sol, const double* rhs, void* stream, fb_solve_info* info)
+{
+  if(!s || !sol || !rhs)
+  {
+    set_error("solver_solve_device: bad arguments");
+    return FB_ERR_ARG;
+  }
+  cudaStream_t cs = as_stream(stream);
+  // order the solver's private stream after the caller's stream, and the caller's after the solve
+  cudaEvent_t ev;
+  FB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  FB_CUDA(cudaEventRecord(ev, cs));
+  FB_CUDA(cudaStreamWaitEvent(s->stream, ev, 0));
+  FB_TRY(to_device_order(s, s->rhs, rhs));
+  FB_TRY(to_device_order(s, s->x, sol));
+  fb_status e = solve_common(s, info);
+  if(e == FB_OK)
+    e = from_device_order(s, sol, s->x);
+  FB_CUDA(cudaEventRecord(ev, s->stream));
+  FB_CUDA(cudaStreamWaitEvent(cs, ev, 0));
+  FB_CUDA(cudaStreamSynchronize(s->stream));
+  cudaEventDestroy(ev);
+  return e;
+}
+
+fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def)
+{
+  if(!s || !cor || !def)
+  {
+    set_error("solver_vcycle: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const uint32_t n = s->lv[0].n;
+  FB_CUDA(cudaMemcpyAsync(s->tmp_in, def, 8 * size_t(n), cudaMemcpyHostToDevice, s->stream));
+  FB_TRY(to_device_order(s, s->r, s->tmp_in));
+  fb_status e = FB_OK;
+  if(s->cfg.precision == FB_PREC_F64)
+    e = vcycle_dispatch<double, double>(s);
+  else if(s->cfg.precision == FB_PREC_F32)
+    e = vcycle_dispatch<float, float>(s);
+  else
+    e = vcycle_dispatch<bf16_t, float>(s);
+  if(e != FB_OK)
+    return e;
+  // the top level's solution: the buffer the last post-smoothing step wrote (x or x2 by parity)
+  const DevLevel& t = s->lv[0];
+  const int steps = std::max(1, s->cfg.smooth_steps);
+  void* xtop = ((steps - 1) % 2 == 0) ? t.x : t.x2;
+  if(s->cfg.precision == FB_PREC_F64)
+    FB_TRY(from_device_order(s, s->tmp_out, (const double*)xtop));
+  else
+  {
+    fb_status ce = fb_convert_f32_to_f64(s->tmp_in, (const float*)xtop, n, s->stream);
+    if(ce != FB_OK)
+      return ce;
+    FB_TRY(from_device_order(s, s->tmp_out, s->tmp_in));
+  }
+  FB_CUDA(cudaMemcpyAsync(cor, s->tmp_out, 8 * size_t(n), cudaMemcpyDeviceToHost, s->stream));
+  FB_CUDA(cudaStreamSynchronize(s->stream));
+  return FB_OK;
+}
+
+fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
+  double* bytes_per_launch)
+{
+  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || (which != FB_KERNEL_PCG_SPMV && which != FB_KERNEL_MG_DEFECT))
+  {
+    set_error("solver_time_kernel: bad arguments");
+    return FB_ERR_ARG;
+  }
+  cudaStream_t st = s->stream;
+  const DevLevel& t = s->lv[0];
+  const bool f64 = s->cfg.precision == FB_PREC_F64;
+  const size_t flush_bytes = size_t(256) << 20;
+  if(flush_l2 && !s->flush)
+    FB_TRY(dalloc(s, &s->flush, flush_bytes));
+  const DevMat& A64 = f64 ? t.A : t.A64;
+  const double vb = double(valsize_of(s->cfg.precision));
+  const double sv = double(vsize_of(s->cfg.precision));
+  if(which == FB_KERNEL_PCG_SPMV)
+    *bytes_per_launch = double(A64.nnz) * 12.0 + double(t.n + 1) * 4.0 + double(t.n) * 8.0 * 2.0 + double(t.n);
+  else
+    *bytes_per_launch = double(t.A.nnz) * (vb + 4.0) + double(t.n + 1) * 4.0 + double(t.n) * sv * 3.0 + double(t.n);
+  k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_PROGRESS);
+  FB_LAUNCHED(1);
+  double total = 0.0;
+  for(int k = 0; k < reps; ++k)
+  {
+    if(flush_l2)
+      FB_CUDA(cudaMemsetAsync(s->flush, k & 0xff, flush_bytes, st));
+    FB_CUDA(cudaEventRecord(s->ev0, st));
+    if(which == FB_KERNEL_PCG_SPMV)
+      k_pcg_q<<<blocks(t.n), NT, A64.smem, st>>>(view<double>(A64), s->p, s->q, t.dm, s->slot, s->sc);
+    else if(s->cfg.precision == FB_PREC_F64)
+      k_defect<double, double><<<blocks(t.n), NT, t.A.smem, st>>>(view<double>(t.A), (const double*)t.b,
+        (const double*)t.x, (double*)t.d, t.dm, s->sc);
+    else if(s->cfg.precision == FB_PREC_F32)
+      k_defect<float, float><<<blocks(t.n), NT, t.A.smem, st>>>(view<float>(t.A), (const float*)t.b,
+        (const float*)t.x, (float*)t.d, t.dm, s->sc);
+    else
+      k_defect<bf16_t, float><<<blocks(t.n), NT, t.A.smem, st>>>(view<bf16_t>(t.A), (const float*)t.b,
+        (const float*)t.x, (float*)t.d, t.dm, s->sc);
+    FB_LAUNCHED(1);
+    FB_CUDA(cudaEventRecord(s->ev1, st));
+    FB_CUDA(cudaEventSynchronize(s->ev1));
+    float ms = 0.f;
+    FB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    total += double(ms);
+  }
+  k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_SUCCESS);
+  FB_LAUNCHED(1);
+  FB_CUDA(cudaStreamSynchronize(st));
+  *avg_ms = total / reps;
+  return FB_OK;
+}
+
+fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out)
+{
+  if(!s || !out)
+  {
+    set_error("solver_level_info: bad arguments");
+    return FB_ERR_ARG;
+  }
+  for(int l = 0; l < s->nlev; ++l)
+  {
+    out[3 * l + 0] = s->lv[size_t(l)].n;
+    out[3 * l + 1] = s->lv[size_t(l)].A.nnz;
+    out[3 * l + 2] = s->lv[size_t(l)].P.nnz;
+  }
+  return FB_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,51 @@
+// Host-side set-up of the multigrid hierarchy: validation, explicit-zero removal on the transfer
+// matrices, reverse Cuthill-McKee reordering, index narrowing to u32, inverse diagonals and the
+// exact coarse-grid inverse.  Plain C++ (no CUDA), run once per solver.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fb
+{
+  struct HostCsr
+  {
+    uint32_t rows = 0, cols = 0;
+    std::vector<uint32_t> rp, col;
+    std::vector<double> val;
+    uint64_t nnz() const { return col.size(); }
+  };
+
+  struct HostLevel
+  {
+    HostCsr A, P, R;            // P: this <- coarser, R: coarser <- this (empty on the coarsest)
+    std::vector<uint8_t> dmask; // 1 = Dirichlet DOF
+    std::vector<uint64_t> fidx; // Dirichlet DOFs (caller numbering)
+    std::vector<double> fval;
+    std::vector<uint32_t> perm; // device row k = caller row perm[k] (empty = identity)
+    bool set = false;
+  };
+
+  // Converts a caller CSR (u64) into a HostCsr; drop_zeros removes stored entries equal to +-0.
+  // Returns an empty string on success, else a message.
+  std::string import_csr(HostCsr& out, uint64_t rows, uint64_t cols, uint64_t nnz, const uint64_t* rp,
+                         const uint64_t* col, const double* val, bool drop_zeros);
+
+  // Reverse Cuthill-McKee ordering of the symmetric pattern of A: perm[k] = old row.
+  std::vector<uint32_t> rcm_order(const HostCsr& A);
+
+  // B = Pr * M * Pc^T with row order perm_r (new row k = old row perm_r[k]) and column map
+  // inv_c (new column = inv_c[old column]); entries keep their stored order within each row.
+  HostCsr permute(const HostCsr& M, const std::vector<uint32_t>& perm_r, const std::vector<uint32_t>& inv_c);
+
+  // omega / a_ii, a_ii = 0 when the row stores no diagonal entry (JacobiPrecond::init_numeric).
+  std::vector<double> inv_diagonal(const HostCsr& A, double omega);
+
+  // Inverse of A restricted to the non-Dirichlet DOFs (Gauss-Jordan, partial pivoting), row-major
+  // m x m, and the free DOF list.
+  void coarse_inverse(const HostCsr& A, const std::vector<uint8_t>& dmask, std::vector<uint32_t>& free_dofs,
+                      std::vector<double>& inv);
+
+  std::vector<uint32_t> inverse_perm(const std::vector<uint32_t>& perm);
+} // namespace fb

@@ -1,0 +1,313 @@
+"""Host-side mirror of the reference's Solver API for the PCG + geometric-multigrid path.
+
+Reads like the reference's own set-up (tutorials/tutorial_05_multigrid.cpp:363-460):
+
+    hierarchy = MultiGridHierarchy(len(levels))
+    for lvl in fine levels:
+        jacobi = new_jacobi_precond(lvl.matrix, lvl.filter, 0.7)
+        smoother = new_richardson(lvl.matrix, lvl.filter, 1.0, jacobi)
+        smoother.set_min_iter(2); smoother.set_max_iter(2)
+        hierarchy.push_level(lvl.matrix, lvl.filter, lvl.transfer, smoother, smoother, smoother)
+    hierarchy.push_level(coarse.matrix, coarse.filter, new_coarse_inverse())
+    multigrid = new_multigrid(hierarchy, MultiGridCycle.V)
+    solver = new_pcg(fine.matrix, fine.filter, multigrid)
+    solver.set_tol_rel(1e-8)
+    hierarchy.init(); solver.init()
+    status = solve(solver, vec_sol, vec_rhs, fine.matrix, fine.filter)
+
+Everything below ``solver.init()`` runs on the GPU through the C ABI (fb_hierarchy_* /
+fb_solver_*).  The device V-cycle implements exactly the configuration above (Richardson(1) +
+Jacobi(omega) with min_iter = max_iter for pre- and post-smoothing, exact coarse solve); any other
+configuration raises ``FeatB200Error`` instead of running something else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _lib
+from .lafem import DenseVector, SparseMatrixCSR, Transfer, UnitFilter
+
+
+class Status(enum.Enum):
+    undefined = 0
+    progress = 1
+    success = 2
+    aborted = 3
+    diverged = 4
+    max_iter = 5
+    stagnated = 6
+
+
+def status_success(st):
+    return st == Status.success
+
+
+class MultiGridCycle(enum.Enum):
+    V = 0
+    F = 1
+    W = 2
+
+
+class JacobiPrecond:
+    def __init__(self, matrix, filter, omega=1.0):
+        self.matrix, self.filter, self.omega = matrix, filter, float(omega)
+
+
+class Richardson:
+    def __init__(self, matrix, filter, omega=1.0, precond=None):
+        self.matrix, self.filter, self.omega, self.precond = matrix, filter, float(omega), precond
+        self.min_iter, self.max_iter = 0, 100
+
+    def set_min_iter(self, k):
+        self.min_iter = int(k)
+
+    def set_max_iter(self, k):
+        self.max_iter = int(k)
+
+
+class CoarseInverse:
+    """Exact coarse-grid solve: inverse of the matrix restricted to the free DOFs."""
+
+
+def new_jacobi_precond(matrix, filter, omega=1.0):
+    return JacobiPrecond(matrix, filter, omega)
+
+
+def new_richardson(matrix, filter, omega=1.0, precond=None):
+    return Richardson(matrix, filter, omega, precond)
+
+
+def new_coarse_inverse(*_args):
+    return CoarseInverse()
+
+
+class MultiGridHierarchy:
+    """MultiGridHierarchy<SparseMatrixCSR, UnitFilter, Transfer> (kernel/solver/multigrid.hpp:419)."""
+
+    def __init__(self, size):
+        self.size = int(size)
+        self.levels = []
+        self._h = None
+
+    def push_level(self, matrix, filter, transfer_or_coarse, smoother_pre=None, smoother_post=None,
+                   smoother_peak=None):
+        if isinstance(transfer_or_coarse, Transfer):
+            self.levels.append({"matrix": matrix, "filter": filter, "transfer": transfer_or_coarse,
+                                "pre": smoother_pre, "post": smoother_post})
+        else:
+            if not isinstance(transfer_or_coarse, CoarseInverse):
+                raise _lib.FeatB200Error("the device multigrid supports the exact coarse inverse only")
+            self.levels.append({"matrix": matrix, "filter": filter, "coarse": transfer_or_coarse})
+
+    def smoother_params(self):
+        omega = steps = None
+        for lv in self.levels[:-1]:
+            for sm in (lv["pre"], lv["post"]):
+                if not isinstance(sm, Richardson) or sm.omega != 1.0 or sm.min_iter != sm.max_iter or \
+                        not isinstance(sm.precond, JacobiPrecond):
+                    raise _lib.FeatB200Error(
+                        "the device V-cycle implements Richardson(omega=1)+Jacobi smoothing with "
+                        "min_iter == max_iter on every level")
+                if omega is None:
+                    omega, steps = sm.precond.omega, sm.max_iter
+                elif (omega, steps) != (sm.precond.omega, sm.max_iter):
+                    raise _lib.FeatB200Error("all levels must use the same smoother parameters")
+        return (0.7 if omega is None else omega), (2 if steps is None else steps)
+
+    def init(self):
+        if len(self.levels) != self.size:
+            raise _lib.FeatB200Error(f"hierarchy has {len(self.levels)} of {self.size} levels")
+        if "coarse" not in self.levels[-1]:
+            raise _lib.FeatB200Error("the last pushed level must carry the coarse solver")
+        L = _lib.lib()
+        h = C.c_void_p()
+        _lib.check(L.fb_hierarchy_create(C.byref(h), self.size), "fb_hierarchy_create")
+        self._h = h
+        for i, lv in enumerate(self.levels):
+            A = lv["matrix"].c_host()
+            f: UnitFilter = lv["filter"]
+            if "transfer" in lv:
+                Pm, Rm = lv["transfer"].prol, lv["transfer"].rest
+                Pc, Rc = Pm.c_host(), Rm.c_host()
+                _lib.check(L.fb_hierarchy_set_level(h, i, C.byref(A), f.indices.ctypes.data_as(C.c_void_p),
+                                                    f.values.ctypes.data_as(C.c_void_p), f.indices.size,
+                                                    C.byref(Pc), C.byref(Rc)), "fb_hierarchy_set_level")
+            else:
+                _lib.check(L.fb_hierarchy_set_level(h, i, C.byref(A), f.indices.ctypes.data_as(C.c_void_p),
+                                                    f.values.ctypes.data_as(C.c_void_p), f.indices.size,
+                                                    None, None), "fb_hierarchy_set_level")
+
+    def done(self):
+        if self._h is not None:
+            _lib.lib().fb_hierarchy_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.done()
+        except Exception:
+            pass
+
+
+class MultiGrid:
+    def __init__(self, hierarchy, cycle=MultiGridCycle.V):
+        if cycle != MultiGridCycle.V:
+            raise _lib.FeatB200Error("the device multigrid implements the V-cycle")
+        self.hierarchy, self.cycle = hierarchy, cycle
+
+
+def new_multigrid(hierarchy, cycle=MultiGridCycle.V):
+    return MultiGrid(hierarchy, cycle)
+
+
+class PCG:
+    """PCG<SparseMatrixCSR, UnitFilter> preconditioned by MultiGrid (kernel/solver/pcg.hpp)."""
+
+    def __init__(self, matrix, filter, precond: MultiGrid):
+        if not isinstance(precond, MultiGrid):
+            raise _lib.FeatB200Error("the device PCG is preconditioned by the multigrid V-cycle")
+        self.matrix, self.filter, self.precond = matrix, filter, precond
+        self.cfg = _lib.SolverConfig()
+        _lib.lib().fb_solver_config_default(C.byref(self.cfg))
+        self._s = None
+        self.info = _lib.SolveInfo()
+        self.plot_mode = "none"
+
+    # IterativeSolver setters (kernel/solver/iterative.hpp:258-300)
+    def set_tol_rel(self, v):
+        self.cfg.tol_rel = float(v)
+
+    def set_tol_abs(self, v):
+        self.cfg.tol_abs = float(v)
+
+    def set_max_iter(self, k):
+        self.cfg.max_iter = int(k)
+
+    def set_min_iter(self, k):
+        self.cfg.min_iter = int(k)
+
+    def set_plot_mode(self, mode):
+        self.plot_mode = str(mode)
+
+    # device options
+    def set_precision(self, p):
+        self.cfg.precision = _lib.PREC[p]
+
+    def set_ordering(self, o):
+        self.cfg.ordering = _lib.ORDER[o]
+
+    def set_use_graph(self, flag):
+        self.cfg.use_graph = 1 if flag else 0
+
+    def init(self):
+        h = self.precond.hierarchy
+        omega, steps = h.smoother_params()
+        self.cfg.omega = omega
+        self.cfg.smooth_steps = steps
+        if h._h is None:
+            h.init()
+        s = C.c_void_p()
+        _lib.check(_lib.lib().fb_solver_create(C.byref(s), h._h, C.byref(self.cfg)), "fb_solver_create")
+        self._s = s
+
+    def done(self):
+        if self._s is not None:
+            _lib.lib().fb_solver_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.done()
+        except Exception:
+            pass
+
+    def correct(self, vec_sol: DenseVector, vec_rhs: DenseVector):
+        if self._s is None:
+            raise _lib.FeatB200Error("PCG.init() was not called")
+        _lib.check(_lib.lib().fb_solver_solve(self._s, vec_sol.elements.ctypes.data_as(C.c_void_p),
+                                              vec_rhs.elements.ctypes.data_as(C.c_void_p), C.byref(self.info)),
+                   "fb_solver_solve")
+        st = Status(self.info.status)
+        if self.plot_mode != "none":
+            print(f"PCG: {self.info.iterations} iterations, |d0| {self.info.def_init:.6e} -> "
+                  f"|d| {self.info.def_final:.6e} ({st.name}, {self.info.solve_ms:.3f} ms)")
+        return st
+
+    def correct_device(self, sol, rhs, stream=None):
+        """Solve with CUDA tensors (caller numbering) on `stream` (default: torch's current)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        _lib.check(_lib.lib().fb_solver_solve_device(self._s, C.c_void_p(sol.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                                     C.c_void_p(stream.cuda_stream), C.byref(self.info)),
+                   "fb_solver_solve_device")
+        return Status(self.info.status)
+
+    def apply_precond(self, vec_def: DenseVector):
+        """One V-cycle: MultiGrid::apply (kernel/solver/multigrid.hpp:1270)."""
+        out = DenseVector(vec_def.size())
+        _lib.check(_lib.lib().fb_solver_vcycle(self._s, out.elements.ctypes.data_as(C.c_void_p),
+                                               vec_def.elements.ctypes.data_as(C.c_void_p)), "fb_solver_vcycle")
+        return out
+
+    def get_num_iter(self):
+        return int(self.info.iterations)
+
+    def get_def_initial(self):
+        return float(self.info.def_init)
+
+    def get_def_final(self):
+        return float(self.info.def_final)
+
+    def get_status(self):
+        return Status(self.info.status)
+
+    def time_kernel(self, which="pcg_spmv", reps=20, flush_l2=True):
+        """Mean launch time (ms) and algorithmic bytes of one solver kernel timed alone."""
+        code = {"pcg_spmv": 0, "mg_defect": 1}[which]
+        ms, by = C.c_double(), C.c_double()
+        _lib.check(_lib.lib().fb_solver_time_kernel(self._s, code, int(reps), 1 if flush_l2 else 0, C.byref(ms),
+                                                     C.byref(by)), "fb_solver_time_kernel")
+        return ms.value, by.value
+
+    def level_info(self):
+        n = len(self.precond.hierarchy.levels)
+        out = np.zeros(3 * n, dtype=np.uint64)
+        _lib.check(_lib.lib().fb_solver_level_info(self._s, out.ctypes.data_as(C.c_void_p)), "fb_solver_level_info")
+        return out.reshape(n, 3)
+
+
+def new_pcg(matrix, filter, precond):
+    return PCG(matrix, filter, precond)
+
+
+def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
+    """Solver::solve (kernel/solver/iterative.hpp:930-939): calls solver.correct(sol, rhs)."""
+    return solver.correct(vec_sol, vec_rhs)
+
+
+def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
+                        ordering="native", use_graph=True):
+    """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
+    transfer (all but the coarsest)."""
+    h = MultiGridHierarchy(len(levels))
+    for lv in levels[:-1]:
+        jac = new_jacobi_precond(lv["matrix"], lv["filter"], omega)
+        sm = new_richardson(lv["matrix"], lv["filter"], 1.0, jac)
+        sm.set_min_iter(steps)
+        sm.set_max_iter(steps)
+        h.push_level(lv["matrix"], lv["filter"], lv["transfer"], sm, sm, sm)
+    h.push_level(levels[-1]["matrix"], levels[-1]["filter"], new_coarse_inverse())
+    mg = new_multigrid(h, MultiGridCycle.V)
+    s = new_pcg(levels[0]["matrix"], levels[0]["filter"], mg)
+    s.set_tol_rel(tol_rel)
+    s.set_max_iter(max_iter)
+    s.set_precision(precision)
+    s.set_ordering(ordering)
+    s.set_use_graph(use_graph)
+    h.init()
+    s.init()
+    return s

@@ -1,0 +1,235 @@
+/*
+ * featb200.h - C ABI of the B200 (sm_100a) geometric-multigrid Poisson path.
+ *
+ * Two seams, matching the two places where the reference's solve path can be replaced:
+ *
+ *  1. Op level: drop-in replacements of the reference's LAFEM::Arch backend kernels
+ *     (kernel/lafem/arch/*.hpp).  Raw DEVICE pointers, element counts and scalars; no ownership
+ *     transfer.  Each call is enqueued on `stream` (NULL = legacy default stream) and, like the
+ *     reference's *_cuda functions, returns after the work is complete unless noted otherwise.
+ *     Index variants: _u64 = the reference's default `Index` (unsigned long),
+ *     _u32 = FEAT_INDEX_U32 builds.  Value variants: _f64, _f32.
+ *
+ *  2. Solver level: an opaque-handle PCG preconditioned by a geometric-multigrid V-cycle
+ *     (kernel/solver/pcg.hpp + kernel/solver/multigrid.hpp), built from the same per-level data
+ *     the reference's MultiGridHierarchy::push_level receives (system matrix, unit filter,
+ *     prolongation and restriction matrices, kernel/solver/multigrid.hpp:612-690).  Host buffers
+ *     in, uploaded once; solves run on the device without host round trips.
+ *
+ * Every function returns an fb_status (0 = success).  fb_last_error() returns a message for the
+ * most recent failure on the calling thread.
+ */
+#ifndef FEATB200_H
+#define FEATB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int fb_status;
+#define FB_OK 0
+#define FB_ERR_ARG 1          /* invalid argument (sizes, null pointers, aliasing) */
+#define FB_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define FB_ERR_STATE 3        /* object not initialised / wrong order of calls */
+#define FB_ERR_NOMEM 4        /* device allocation failed */
+#define FB_ERR_UNSUPPORTED 5  /* option not available in this build */
+
+/* Solver status codes: the reference's Solver::Status (kernel/solver/base.hpp:48-64). */
+#define FB_SOLVER_UNDEFINED 0
+#define FB_SOLVER_PROGRESS 1
+#define FB_SOLVER_SUCCESS 2
+#define FB_SOLVER_ABORTED 3
+#define FB_SOLVER_DIVERGED 4
+#define FB_SOLVER_MAX_ITER 5
+#define FB_SOLVER_STAGNATED 6
+
+const char* fb_last_error(void);
+/* Library version string and the compute capability it was built for. */
+const char* fb_version(void);
+/* Number of this library's kernels launched since load (all threads, all devices). */
+uint64_t fb_kernel_launch_count(void);
+
+/* ------------------------------------------------------------------------------------------ */
+/* 1. Op level: LAFEM::Arch equivalents (device pointers)                                     */
+/* ------------------------------------------------------------------------------------------ */
+
+/* r = a * A * x + b * y, or r = a * A^T * x + b * y when transposed != 0.  |b| < eps(DT) means y
+ * is not read (r is cleared first).  r may alias y, must not alias x.
+ * Replaces Arch::Apply::csr (kernel/lafem/arch/apply.hpp:44-79; generic semantics
+ * apply_generic.hpp:25-69; CUDA backend apply.cu:176-261).  Non-transposed rows are summed
+ * in stored entry order without FMA contraction, so FP64 results equal the generic backend's
+ * bit for bit. */
+fb_status fb_apply_csr_f64_u64(double* r, double a, const double* x, double b, const double* y,
+                               const double* val, const uint64_t* col_ind, const uint64_t* row_ptr,
+                               uint64_t rows, uint64_t columns, uint64_t used_elements,
+                               int transposed, void* stream);
+fb_status fb_apply_csr_f64_u32(double* r, double a, const double* x, double b, const double* y,
+                               const double* val, const uint32_t* col_ind, const uint32_t* row_ptr,
+                               uint64_t rows, uint64_t columns, uint64_t used_elements,
+                               int transposed, void* stream);
+fb_status fb_apply_csr_f32_u64(float* r, float a, const float* x, float b, const float* y,
+                               const float* val, const uint64_t* col_ind, const uint64_t* row_ptr,
+                               uint64_t rows, uint64_t columns, uint64_t used_elements,
+                               int transposed, void* stream);
+fb_status fb_apply_csr_f32_u32(float* r, float a, const float* x, float b, const float* y,
+                               const float* val, const uint32_t* col_ind, const uint32_t* row_ptr,
+                               uint64_t rows, uint64_t columns, uint64_t used_elements,
+                               int transposed, void* stream);
+
+/* r = a * x + y; r may alias x or y.  Replaces Arch::Axpy::value (axpy.hpp:21-54, axpy.cu:18-75). */
+fb_status fb_axpy_f64(double* r, double a, const double* x, const double* y, uint64_t n, void* stream);
+fb_status fb_axpy_f32(float* r, float a, const float* x, const float* y, uint64_t n, void* stream);
+
+/* *result = x^T y (FP64 accumulation for both value types); result is a HOST pointer and the
+ * call synchronises `stream`.  Replaces Arch::DotProduct::value (dot_product.hpp:21, dot_product.cu:21-61). */
+fb_status fb_dot_f64(double* result, const double* x, const double* y, uint64_t n, void* stream);
+fb_status fb_dot_f32(float* result, const float* x, const float* y, uint64_t n, void* stream);
+
+/* *result = ||x||_2; HOST result, synchronises.  Replaces Arch::Norm2::value (norm.hpp:21, norm.cu:20-59). */
+fb_status fb_norm2_f64(double* result, const double* x, uint64_t n, void* stream);
+fb_status fb_norm2_f32(float* result, const float* x, uint64_t n, void* stream);
+
+/* r_i = x_i * y_i.  Replaces Arch::ComponentProduct::value (component_product.cu:20-55; unlike the
+ * reference's CUDA kernel, the FP64 product is not rounded through float). */
+fb_status fb_component_product_f64(double* r, const double* x, const double* y, uint64_t n, void* stream);
+fb_status fb_component_product_f32(float* r, const float* x, const float* y, uint64_t n, void* stream);
+
+/* r_i = s / x_i.  Replaces Arch::ComponentInvert::value (component_invert.cu:19-64). */
+fb_status fb_component_invert_f64(double* r, const double* x, double s, uint64_t n, void* stream);
+fb_status fb_component_invert_f32(float* r, const float* x, float s, uint64_t n, void* stream);
+
+/* r_i = s * x_i.  Replaces Arch::Scale::value (scale.hpp:21, scale.cu:17-58). */
+fb_status fb_scale_f64(double* r, const double* x, double s, uint64_t n, void* stream);
+fb_status fb_scale_f32(float* r, const float* x, float s, uint64_t n, void* stream);
+
+/* v[idx[k]] = vals[k] (rhs/sol) and v[idx[k]] = 0 (def/cor).
+ * Replaces Arch::UnitFilter::filter_rhs / filter_def (unit_filter.hpp:21-71, unit_filter.cu:19-91). */
+fb_status fb_unit_filter_rhs_f64_u64(double* v, const double* vals, const uint64_t* idx, uint64_t ue, void* stream);
+fb_status fb_unit_filter_def_f64_u64(double* v, const uint64_t* idx, uint64_t ue, void* stream);
+fb_status fb_unit_filter_rhs_f32_u32(float* v, const float* vals, const uint32_t* idx, uint64_t ue, void* stream);
+fb_status fb_unit_filter_def_f32_u32(float* v, const uint32_t* idx, uint64_t ue, void* stream);
+
+/* diag[row] = position of the diagonal entry of `row`, or row_ptr[rows] when the row has none.
+ * Replaces Arch::Diagonal::csr (diagonal.cu:18-62). */
+fb_status fb_diagonal_csr_u64(uint64_t* diag, const uint64_t* col_ind, const uint64_t* row_ptr,
+                              uint64_t rows, void* stream);
+
+/* Precision conversion (MemoryPool::convert / Util::cuda_convert, cuda_util.cu:228-262). */
+fb_status fb_convert_f64_to_f32(float* dst, const double* src, uint64_t n, void* stream);
+fb_status fb_convert_f32_to_f64(double* dst, const float* src, uint64_t n, void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* 2. Solver level: PCG + geometric multigrid                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct fb_hierarchy fb_hierarchy;
+typedef struct fb_solver fb_solver;
+
+/* A CSR matrix in HOST memory with the reference's default index type (SparseMatrixCSR<double,
+ * Index>, kernel/lafem/sparse_matrix_csr.hpp:280-302): row_ptr[rows+1], col_ind[nnz], val[nnz]. */
+typedef struct
+{
+  uint64_t rows, columns, used_elements;
+  const uint64_t* row_ptr;
+  const uint64_t* col_ind;
+  const double* val;
+} fb_csr_host;
+
+/* Create an empty hierarchy of `num_levels` levels on the current CUDA device.
+ * Levels are numbered finest = 0 as in MultiGridHierarchy (kernel/solver/multigrid.hpp:419). */
+fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels);
+
+/* Set level `level` (0 = finest).  A: system matrix; filter_idx/filter_val[nf]: unit-filter
+ * (Dirichlet) DOFs and values (UnitFilter, kernel/lafem/unit_filter.hpp:30); P: prolongation
+ * level <- level+1 and R: restriction level+1 <- level (LAFEM::Transfer, kernel/lafem/transfer.hpp;
+ * both NULL on the coarsest level).  Mirrors MultiGridHierarchy::push_level
+ * (kernel/solver/multigrid.hpp:633-690).  Data is copied; the host buffers may be freed after. */
+fb_status fb_hierarchy_set_level(fb_hierarchy* h, int level, const fb_csr_host* A,
+                                 const uint64_t* filter_idx, const double* filter_val, uint64_t nf,
+                                 const fb_csr_host* P, const fb_csr_host* R);
+
+void fb_hierarchy_destroy(fb_hierarchy* h);
+
+/* Precision of the multigrid preconditioner. */
+#define FB_PREC_F64 0        /* plain FP64 (the reference's path; parity mode) */
+#define FB_PREC_F32 1        /* FP32 V-cycle inside FP64 PCG (iterative refinement) */
+#define FB_PREC_F32_BF16 2   /* as FB_PREC_F32, with BF16 matrix values in the V-cycle */
+
+/* DOF ordering used on the device. */
+#define FB_ORDER_NATIVE 0    /* the caller's numbering */
+#define FB_ORDER_RCM 1       /* reverse Cuthill-McKee per level (host, at setup); vectors are
+                                permuted on the way in and out of fb_solver_solve */
+
+typedef struct
+{
+  int precision;        /* FB_PREC_* */
+  int ordering;         /* FB_ORDER_* */
+  double omega;         /* Jacobi damping (JacobiPrecond omega; 0.7 in the configured problems) */
+  int smooth_steps;     /* Richardson min_iter = max_iter for pre- and post-smoothing (2 = V(2,2)) */
+  double tol_rel;       /* PCG relative tolerance (IterativeSolver tol_rel) */
+  double tol_abs;       /* PCG absolute tolerance (default 1/eps^2) */
+  int max_iter;         /* PCG max_iter (default 100) */
+  int min_iter;         /* PCG min_iter (default 0) */
+  int use_graph;        /* capture the whole solve in one CUDA graph (1) or launch per kernel (0) */
+  int rows_per_block;   /* CSR kernel rows per block, 0 = autotuned */
+} fb_solver_config;
+
+/* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
+ * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks. */
+void fb_solver_config_default(fb_solver_config* cfg);
+
+typedef struct
+{
+  int status;           /* FB_SOLVER_* */
+  int iterations;
+  double def_init;      /* initial defect norm */
+  double def_final;     /* final defect norm */
+  double solve_ms;      /* device time of the solve (CUDA events) */
+  uint64_t kernel_launches;  /* kernels of this library launched by the solve */
+  double bytes_moved;   /* algorithmic bytes of every launched kernel */
+} fb_solve_info;
+
+/* Build the solver: uploads every level, forms the Jacobi inverse diagonals, the exact coarse
+ * inverse and (for FB_PREC_F32*) the low-precision copies.  Mirrors MultiGridHierarchy::init +
+ * PCG::init.  The hierarchy must stay alive while the solver exists. */
+fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_config* cfg);
+void fb_solver_destroy(fb_solver* s);
+
+/* PCG::correct semantics (kernel/solver/pcg.hpp:159-170): sol holds the initial guess on entry
+ * and the solution on return.  HOST buffers of the finest level's size; copies in and out are
+ * part of the call.  Synchronous. */
+fb_status fb_solver_solve(fb_solver* s, double* sol, const double* rhs, fb_solve_info* info);
+
+/* As fb_solver_solve with DEVICE buffers in the caller's numbering, enqueued on `stream`;
+ * returns after the solve completed. */
+fb_status fb_solver_solve_device(fb_solver* s, double* sol, const double* rhs, void* stream,
+                                 fb_solve_info* info);
+
+/* One application of the preconditioner (MultiGrid::apply, kernel/solver/multigrid.hpp:1270):
+ * cor = V-cycle(def).  HOST buffers of the finest level's size. */
+fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
+
+/* Kernels that fb_solver_time_kernel can time in isolation. */
+#define FB_KERNEL_PCG_SPMV 0   /* q = F(A p) with q.p, finest level, FP64 (the PCG matrix product) */
+#define FB_KERNEL_MG_DEFECT 1  /* d = F(b - A x), finest level, in the V-cycle's precision */
+
+/* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
+ * on that stream; with flush_l2 != 0 a 256 MiB buffer is overwritten before each launch (outside
+ * the timed interval) so every launch starts with a cold L2.  Returns the mean launch time and the
+ * kernel's algorithmic bytes per launch (matrix values + indices + row pointers + vector reads and
+ * writes).  No counterpart in the reference: a measurement aid for the SpMV roofline. */
+fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
+                                double* bytes_per_launch);
+
+/* Per-level sizes after upload: rows, nnz of A, nnz of P (as stored on the device, explicit zeros
+ * removed).  `out` holds 3 * num_levels entries. */
+fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FEATB200_H */

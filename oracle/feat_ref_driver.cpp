@@ -15,6 +15,7 @@
 // CoarseInverseSolver below; the reference offers no third-party-free direct solver).
 //
 // Usage:
+//   feat_oracle fd M D DIR     (the reference's basic_solver-test problem, see run_fd)
 //   feat_oracle solve --dim D --level L --out DIR [--rhs sine|gauss] [--params FILE]
 //                     [--kappa FILE] [--omega W] [--steps S] [--tol T] [--iterates K]
 //                     [--vcycle] [--dump-levels] [--time REPS] [--no-dump]
@@ -45,6 +46,8 @@
 #include <kernel/lafem/sparse_matrix_csr.hpp>
 #include <kernel/lafem/unit_filter.hpp>
 #include <kernel/lafem/transfer.hpp>
+#include <kernel/lafem/pointstar_factory.hpp>
+#include <kernel/lafem/none_filter.hpp>
 #include <kernel/solver/pcg.hpp>
 #include <kernel/solver/richardson.hpp>
 #include <kernel/solver/jacobi_precond.hpp>
@@ -594,20 +597,59 @@ namespace Oracle
         times.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
     }
     double median = 0.0;
+    std::string times_json = "[";
+    for(std::size_t k = 0; k < times.size(); ++k)
+      times_json += (k ? ", " : "") + std::to_string(times[k]);
+    times_json += "]";
     if(!times.empty())
     {
-      std::sort(times.begin(), times.end());
-      median = times[times.size() / 2];
+      std::vector<double> sorted(times);
+      std::sort(sorted.begin(), sorted.end());
+      median = sorted[sorted.size() / 2];
     }
 
     solver->done();
     hierarchy->done();
 
     std::printf("{\"dim\": %d, \"level\": %lu, \"dofs\": %lu, \"nnz\": %lu, \"status\": \"%s\", \"iters\": %lu, "
-      "\"def_init\": %.17g, \"def_final\": %.17g, \"setup_s\": %.3f, \"solve_ms_median\": %.6f, \"reps\": %zu}\n",
+      "\"def_init\": %.17g, \"def_final\": %.17g, \"setup_s\": %.3f, \"solve_ms_median\": %.6f, \"reps\": %zu, "
+      "\"times_ms\": %s}\n",
       dim_, (unsigned long)opt.level, (unsigned long)top.matrix.rows(), (unsigned long)top.matrix.used_elements(),
       Solver::status_success(st) ? "success" : "failure", (unsigned long)iters, def_init, def_final, setup_s,
-      median, times.size());
+      median, times.size(), times_json.c_str());
+    return 0;
+  }
+  // The reference's own solver test problem (kernel/solver/basic_solver-test.cpp:98-140): the
+  // 5-point finite-difference matrix of PointstarFactoryFD(m, d), the Q2-bubble reference solution,
+  // rhs = A * ref, and the iteration counts of the reference's CG and PCG-Jacobi from a zero guess.
+  int run_fd(Index m, Index d, const std::string& out)
+  {
+    LAFEM::PointstarFactoryFD<DataType, IndexType> psf(m, d);
+    MatrixType matrix(psf.matrix_csr());
+    VectorType vec_ref(psf.vector_q2_bubble());
+    VectorType vec_rhs = matrix.create_vector_r();
+    matrix.apply(vec_rhs, vec_ref);
+    LAFEM::NoneFilter<DataType, IndexType> filter;
+    dump_csr(out + "/fd_A", matrix);
+    dump_vec(out + "/fd_ref.npy", vec_ref);
+    dump_vec(out + "/fd_rhs.npy", vec_rhs);
+    Index iters[2];
+    for(int k = 0; k < 2; ++k)
+    {
+      VectorType vec_sol = matrix.create_vector_r();
+      vec_sol.format();
+      std::shared_ptr<Solver::SolverBase<VectorType>> pre;
+      if(k == 1)
+        pre = Solver::new_jacobi_precond(matrix, filter);
+      auto solver = Solver::new_pcg(matrix, filter, pre);
+      solver->init();
+      solver->apply(vec_sol, vec_rhs);
+      iters[k] = solver->get_num_iter();
+      solver->done();
+      dump_vec(out + (k == 0 ? "/fd_sol_cg.npy" : "/fd_sol_pcgjac.npy"), vec_sol);
+    }
+    std::printf("{\"m\": %lu, \"d\": %lu, \"cg_iters\": %lu, \"pcg_jac_iters\": %lu}\n", (unsigned long)m,
+      (unsigned long)d, (unsigned long)iters[0], (unsigned long)iters[1]);
     return 0;
   }
 } // namespace Oracle
@@ -616,6 +658,8 @@ int main(int argc, char* argv[])
 {
   Runtime::ScopeGuard guard(argc, argv);
   Oracle::Options opt;
+  if(argc == 5 && std::strcmp(argv[1], "fd") == 0)
+    return Oracle::run_fd(Index(std::stoul(argv[2])), Index(std::stoul(argv[3])), argv[4]);
   if(argc < 2 || std::strcmp(argv[1], "solve") != 0)
   {
     std::fprintf(stderr, "usage: feat_oracle solve --dim D --level L --out DIR [...]\n");

@@ -1,0 +1,147 @@
+"""GPU parity of the solver seam (PCG + V-cycle) against the reference.
+
+FP64 ("plain") mode: the V-cycle is bitwise equal to the reference (no global reductions inside it
+other than the smoother's skip test), the PCG iterates and the solution agree to 1e-12 relative
+(only the dot products and norms are summed in a different order).  Low-precision modes report
+their error against the FP64 result (north-star bound 1e-7 relative, residual 1e-8)."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from helpers import CASES, load_golden, rel_err, to_lafem_levels, to_oracle_levels
+
+pytestmark = pytest.mark.gpu
+
+PARITY = 1e-12
+
+
+def _solve(fb, levels, rhs, **kw):
+    s = fb.build_pcg_multigrid(levels, **kw)
+    x = fb.DenseVector(rhs.size)
+    st = fb.solve(s, x, fb.DenseVector(rhs))
+    return s, x.elements, st
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("ordering,graph", [("native", True), ("native", False), ("rcm", True)])
+def test_fp64_matches_reference(featlib, cuda, name, ordering, graph):
+    fb = featlib
+    g = load_golden(name)
+    lv = to_lafem_levels(g["levels"])
+    s, x, st = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph)
+    z = s.apply_precond(fb.DenseVector(g["rhs"])).elements
+    assert np.array_equal(z, g["vcycle"]), rel_err(z, g["vcycle"])
+    assert st == fb.Status.success
+    assert s.get_num_iter() == g["summary"]["iters"]
+    assert rel_err(x, g["sol"]) <= PARITY
+    assert abs(s.get_def_initial() - g["summary"]["def_init"]) <= PARITY * g["summary"]["def_init"]
+    assert abs(s.get_def_final() - g["summary"]["def_final"]) <= 1e-9 * g["summary"]["def_final"]
+    if ordering == "native" and graph:
+        for k, xk_ref in enumerate(g["iterates"], start=1):
+            sk, xk, stk = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, max_iter=k)
+            assert rel_err(xk, xk_ref) <= PARITY, k
+            assert abs(sk.get_def_final() - g["defects"][k - 1]) <= 1e-9 * g["defects"][k - 1]
+
+
+def _live_reference(tmp, level, dim=2, **kw):
+    import oracle as O
+    if not O.feat_available():
+        pytest.skip("reference binary oracle/_ref/feat_oracle not built")
+    summ = O.feat_solve(tmp, dim=dim, level=level, dump_levels=True, vcycle=True, iterates=2, **kw)
+    levels = O.load_dump(tmp, level)
+    return summ, levels
+
+
+@pytest.mark.parametrize("level,dim", [(7, 2), (9, 2), (5, 3)])
+def test_fp64_matches_live_reference(featlib, cuda, level, dim):
+    """Larger hierarchies straight from the reference's own assembly (reference numbering)."""
+    import oracle as O
+    from helpers import to_lafem_levels as conv
+    fb = featlib
+    with tempfile.TemporaryDirectory() as tmp:
+        summ, levels = _live_reference(tmp, level, dim)
+        rhs = np.load(os.path.join(tmp, "rhs.npy"))
+        sol = np.load(os.path.join(tmp, "sol.npy"))
+        vc = np.load(os.path.join(tmp, "vcycle.npy"))
+        it2 = np.load(os.path.join(tmp, "iterate_2.npy"))
+    lv = conv(levels)
+    for ordering in ("native", "rcm"):
+        s, x, st = _solve(fb, lv, rhs, ordering=ordering)
+        assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc)
+        assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
+        assert rel_err(x, sol) <= PARITY
+    s2, x2, _ = _solve(fb, lv, rhs, max_iter=2)
+    assert rel_err(x2, it2) <= PARITY
+
+
+def test_fp64_full_size_against_oracle(featlib, cuda, oracle_lib):
+    """Level 10 (1,050,625 DOFs, Gaussian right-hand side): the product's own problem generator, the
+    GPU solve and the C restatement on the same inputs."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(10, 2, rhs="gauss", gauss=AS.gauss_params(1, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    z_ref = mg.vcycle(b)
+    s, x, st = _solve(fb, levels, b, ordering="rcm")
+    assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref)
+    assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+    assert rel_err(x, x_ref) <= PARITY
+
+
+@pytest.mark.parametrize("precision", ["f32", "f32_bf16"])
+@pytest.mark.parametrize("level", [7, 10])
+def test_mixed_precision_error_against_fp64(featlib, cuda, oracle_lib, precision, level):
+    """FP32 (and BF16-value) V-cycle inside FP64 PCG: reaches relative residual 1e-8 and stays within
+    1e-7 relative of the FP64 oracle's solution."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(level, 2, rhs="gauss", gauss=AS.gauss_params(1, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    s, x, st = _solve(fb, levels, b, precision=precision, ordering="rcm")
+    assert st == fb.Status.success
+    A = levels[0]["matrix"].to_scipy()
+    r = b - A @ x
+    r[levels[0]["filter"].indices.astype(np.int64)] = 0.0
+    assert np.linalg.norm(r) <= 1.05e-8 * np.linalg.norm(b)
+    assert rel_err(x, x_ref) <= 1e-7
+    assert s.get_num_iter() <= info["iters"] + 2
+
+
+def test_status_codes_without_fault(featlib, cuda):
+    """Failure detection on the device, reported through the status word (no trap, no fault):
+    zero rhs -> success after 0 iterations; NaN rhs -> aborted; max_iter reached -> max_iter."""
+    fb = featlib
+    g = load_golden("c1_L4")
+    lv = to_lafem_levels(g["levels"])
+    s = fb.build_pcg_multigrid(lv)
+    x = fb.DenseVector(g["rhs"].size)
+    assert fb.solve(s, x, fb.DenseVector(np.zeros_like(g["rhs"]))) == fb.Status.success
+    assert s.get_num_iter() == 0 and np.all(x.elements == 0)
+    bad = g["rhs"].copy()
+    bad[bad.size // 2] = np.nan
+    assert fb.solve(s, fb.DenseVector(bad.size), fb.DenseVector(bad)) == fb.Status.aborted
+    s2 = fb.build_pcg_multigrid(lv, max_iter=2)
+    assert fb.solve(s2, fb.DenseVector(bad.size), fb.DenseVector(g["rhs"])) == fb.Status.max_iter
+    assert s2.get_num_iter() == 2
+    # the context is still usable after the failures
+    assert fb.solve(s, x, fb.DenseVector(g["rhs"])) == fb.Status.success
+
+
+def test_device_entry_point_and_launch_count(featlib, cuda):
+    """fb_solver_solve_device on torch CUDA tensors matches the host entry point; the library's
+    launch counter advances by the reported number of kernels."""
+    torch = cuda
+    fb = featlib
+    g = load_golden("c1_L5")
+    lv = to_lafem_levels(g["levels"])
+    s = fb.build_pcg_multigrid(lv, ordering="rcm")
+    rhs = torch.tensor(g["rhs"], device="cuda")
+    sol = torch.zeros_like(rhs)
+    c0 = fb.launch_count()
+    assert s.correct_device(sol, rhs) == fb.Status.success
+    assert fb.launch_count() - c0 >= s.info.kernel_launches > 0
+    assert rel_err(sol.cpu().numpy(), g["sol"]) <= PARITY
