@@ -60,7 +60,7 @@ def read_peaks():
 
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
-    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+    FIELDS = "timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
 
     def __init__(self, gpu_index):
@@ -77,7 +77,8 @@ class ClockSampler:
         except (OSError, FileNotFoundError):
             self.proc = None
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
+        """Samples taken between wall-clock times t0 and t1 (the timed region), or all."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -86,22 +87,32 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         self.out.seek(0)
-        sm, smax, reasons = [], [], set()
+        import datetime
+        sm, smax, reasons, power = [], [], set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.out.read().splitlines():
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                mhz, mx = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            if t0 is not None and not (t0 - 0.25 <= ts <= t1 + 0.25):
+                continue
+            sm.append(mhz)
+            smax.append(mx)
+            try:
+                power.append(float(parts[4]))
+            except ValueError:
+                pass
+            for n, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_median": float(np.median(power)) if power else None}
 
 
 def build_problem(dim, level, rhs_kind):
@@ -158,12 +169,15 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
+    ap.add_argument("--profile-solves", type=int, default=0,
+                    help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
+    ap.add_argument("--tail-rows", type=int, default=None)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -184,7 +198,7 @@ def main():
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
     levels, b, gauss = build_problem(dim, level, rhs_kind)
     n = b.size
-    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm")
+    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm", tail_rows=args.tail_rows)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
@@ -197,13 +211,22 @@ def main():
         st = solver.correct_device(sol_d, rhs_d, stream)
         return st
 
+    clocks = ClockSampler(local)
+    if not args.profile_solves:
+        clocks.start()
     for _ in range(args.warmup):
         st = one_step()
     torch.cuda.synchronize()
+    if args.profile_solves:
+        for _ in range(args.profile_solves):
+            one_step()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_solves": args.profile_solves, "iterations": solver.get_num_iter()}))
+        return 0
     if pg:
         pg.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
+    time.sleep(0.3)
+    wall0 = time.time()
     launches0 = fb.launch_count()
     times = []
     iters = []
@@ -222,7 +245,9 @@ def main():
             raise SystemExit(f"solve failed: {st}")
     torch.cuda.synchronize()
     launches = fb.launch_count() - launches0
-    clk = clocks.stop()
+    wall1 = time.time()
+    time.sleep(0.3)
+    clk = clocks.stop(wall0, wall1)
     total_ms = float(np.sum(times))
     if pg:
         t = torch.tensor([total_ms], device="cuda")

@@ -41,14 +41,20 @@ namespace fb
   constexpr int NT = 256;   // rows (threads) per block of every pass
 
   // ------------------------------------------------------------------ device views
+  // Sliced ELL with slices of 32 rows (one warp): slice s holds K_s = (soff[s+1]-soff[s])/32
+  // entries per row, entry k of row 32s+lane at soff[s] + 32k + lane, in the row's stored order.
+  // Shorter rows are padded with value 0 and a column whose vector entry is always 0 (the zero
+  // slot at index `cols`, or the row itself for narrow storage).  Rows whose result the unit
+  // filter discards (Dirichlet rows) are stored empty.  Column indices are either absolute u32
+  // (`col`) or, for square matrices whose |col - row| fits, int16 offsets from the row (`dcol`).
   template<typename V>
   struct DCsr
   {
-    const uint32_t* rp;
-    const uint32_t* col;
+    const uint32_t* soff;
+    const uint32_t* col;    // absolute columns, or nullptr
+    const int16_t* dcol;    // column - row, or nullptr
     const V* val;
     uint32_t rows;
-    uint32_t cap;     // staging capacity in entries (multiple of 8); 0 = read rows directly
   };
 
   struct Scalars
@@ -60,72 +66,48 @@ namespace fb
     int iter, status, min_iter, max_iter;
   };
 
-  template<typename V>
-  struct Staged
+  __device__ __forceinline__ double ldg_v(const double* p) { return __ldg(p); }
+  __device__ __forceinline__ float ldg_v(const float* p) { return __ldg(p); }
+  __device__ __forceinline__ bf16_t ldg_v(const bf16_t* p)
   {
-    const V* sv;
-    const uint32_t* sc;
-    uint32_t offv, offc;
-    bool staged;
-  };
-
-  __device__ __forceinline__ uint4 ld_nc(const uint4* p)
-  {
-    uint4 v;
-    asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
-    return v;
+    bf16_t b;
+    b.bits = __ldg(reinterpret_cast<const unsigned short*>(p));
+    return b;
   }
 
-  // Stage the block's entries [rp[r0], rp[r0+NT]) of col/val into shared memory.  The copy starts
-  // at the 16-byte boundary below the first entry and ends at the one above the last; device
-  // arrays are allocated with >= 16 bytes of padding, so the over-read stays inside them.
-  template<typename V>
-  __device__ __forceinline__ Staged<V> stage_rows(const DCsr<V>& M, uint32_t r0, unsigned char* smem)
-  {
-    Staged<V> s;
-    constexpr uint32_t EV = 16u / sizeof(V);
-    const uint32_t rend = min(r0 + uint32_t(NT), M.rows);
-    const uint32_t s0 = M.rp[r0], s1 = M.rp[rend];
-    const uint32_t a0v = s0 & ~(EV - 1u), a0c = s0 & ~3u;
-    const uint32_t nv4 = (s1 - a0v + EV - 1u) / EV, nc4 = (s1 - a0c + 3u) / 4u;
-    s.staged = (nv4 * EV <= M.cap) && (nc4 * 4u <= M.cap);
-    V* sv = reinterpret_cast<V*>(smem);
-    uint32_t* sc = reinterpret_cast<uint32_t*>(smem + size_t(M.cap) * sizeof(V));
-    if(s.staged)
-    {
-      const uint4* gv = reinterpret_cast<const uint4*>(M.val + a0v);
-      const uint4* gc = reinterpret_cast<const uint4*>(M.col + a0c);
-      uint4* dv = reinterpret_cast<uint4*>(sv);
-      uint4* dc = reinterpret_cast<uint4*>(sc);
-      for(uint32_t k = threadIdx.x; k < nv4; k += NT)
-        dv[k] = ld_nc(gv + k);
-      for(uint32_t k = threadIdx.x; k < nc4; k += NT)
-        dc[k] = ld_nc(gc + k);
-    }
-    __syncthreads();
-    s.sv = sv;
-    s.sc = sc;
-    s.offv = a0v;
-    s.offc = a0c;
-    return s;
-  }
-
-  template<typename V, typename S>
-  __device__ __forceinline__ typename ValueTraits<V>::acc row_sum(const Staged<V>& st, const DCsr<V>& M, uint32_t row,
-    const S* __restrict__ x)
+  // Row sum of row `row` in stored entry order; every product and sum rounded separately.  NC:
+  // gather the vector through the read-only path (vectors not written by the same kernel).
+  template<typename V, typename S, bool NC = true>
+  __device__ __forceinline__ typename ValueTraits<V>::acc row_sum(const DCsr<V>& M, uint32_t row, const S* x)
   {
     typedef typename ValueTraits<V>::acc A;
-    const uint32_t j0 = M.rp[row], j1 = M.rp[row + 1];
+    constexpr uint32_t U = 9;
+    const uint32_t sl = row >> 5;
+    const uint32_t b0 = __ldg(M.soff + sl);
+    const uint32_t K = (__ldg(M.soff + sl + 1) - b0) >> 5;
+    const uint32_t base = b0 + (row & 31u);
     A sum = A(0);
-    if(st.staged)
+    for(uint32_t k0 = 0; k0 < K; k0 += U)
     {
-      for(uint32_t j = j0; j < j1; ++j)
-        sum = add(sum, mul(to_acc(st.sv[j - st.offv]), A(x[st.sc[j - st.offc]])));
-    }
-    else
-    {
-      for(uint32_t j = j0; j < j1; ++j)
-        sum = add(sum, mul(to_acc(M.val[j]), A(x[M.col[j]])));
+      A v[U];
+      uint32_t c[U];
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        if(k0 + u < K)
+        {
+          const uint32_t e = base + (k0 + u) * 32u;
+          v[u] = to_acc(ldg_v(M.val + e));
+          c[u] = M.dcol ? uint32_t(int32_t(row) + int32_t(__ldg(M.dcol + e))) : __ldg(M.col + e);
+        }
+      A xv[U];
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        if(k0 + u < K)
+          xv[u] = NC ? A(__ldg(x + c[u])) : A(x[c[u]]);
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        if(k0 + u < K)
+          sum = add(sum, mul(v[u], xv[u]));
     }
     return sum;
   }
@@ -148,77 +130,145 @@ namespace fb
   }
 
   // ------------------------------------------------------------------ V-cycle passes
+  // Per-row bodies shared by the grid kernels (one thread per row) and the single-block tail
+  // kernel (block-stride loops), so both produce bitwise identical values.
+
+  // Richardson step k >= 2 of the pre-smoother: x' = x + F(D .* F(b - A x)); skipped -> 0
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ S smooth_row(const DCsr<V>& A, const S* b, const S* x, const S* dinv,
+    const uint8_t* dm, bool skipped, uint32_t i)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(skipped)
+      return S(0);
+    const Ac sum = row_sum<V, S, NC>(A, i, x);
+    const bool d = __ldg(dm + i) != 0;
+    const Ac d1 = d ? Ac(0) : sub(Ac(b[i]), sum);
+    const Ac c = d ? Ac(0) : mul(Ac(__ldg(dinv + i)), d1);
+    return S(add(Ac(x[i]), c));
+  }
+
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ S defect_row(const DCsr<V>& A, const S* b, const S* x, const uint8_t* dm, uint32_t i)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const Ac sum = row_sum<V, S, NC>(A, i, x);
+    return __ldg(dm + i) ? S(0) : S(sub(Ac(b[i]), sum));
+  }
+
+  // b_c = F_c(R d) and (xc != null) sol1_c = F_c(D_c .* b_c); returns b_c^2
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ double restrict_row(const DCsr<V>& R, const S* d, S* bc, S* xc, const S* dinvc,
+    const uint8_t* dmc, uint32_t j)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const bool dc = __ldg(dmc + j) != 0;
+    const Ac sum = row_sum<V, S, NC>(R, j, d);
+    const Ac v = dc ? Ac(0) : add(sum, Ac(0));
+    bc[j] = S(v);
+    if(xc)
+    {
+      const Ac c = dc ? Ac(0) : mul(Ac(__ldg(dinvc + j)), v);
+      xc[j] = S(add(Ac(0), c));
+    }
+    return double(v) * double(v);
+  }
+
+  // x + F(P xc)
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ S prolong_row(const DCsr<V>& P, const S* xc, const S* x, const uint8_t* dm, uint32_t i)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const Ac sum = row_sum<V, S, NC>(P, i, xc);
+    const Ac c = __ldg(dm + i) ? Ac(0) : add(sum, Ac(0));
+    return S(add(Ac(x[i]), c));
+  }
+
+  // d = F(b - A x), c = F(D .* d); returns d^2
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ double post1_row(const DCsr<V>& A, const S* b, const S* x, S* d, S* c, const S* dinv,
+    const uint8_t* dm, uint32_t i)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const bool dd = __ldg(dm + i) != 0;
+    const Ac sum = row_sum<V, S, NC>(A, i, x);
+    const Ac dv = dd ? Ac(0) : sub(Ac(b[i]), sum);
+    d[i] = S(dv);
+    const Ac cv = dd ? Ac(0) : mul(Ac(__ldg(dinv + i)), dv);
+    c[i] = S(add(Ac(0), cv));
+    return double(dv) * double(dv);
+  }
+
+  // post-smoothing step k >= 2: c + F(D .* F(d - A c)); skipped -> 0
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ typename ValueTraits<V>::acc post2_row(const DCsr<V>& A, const S* d, const S* c,
+    const S* dinv, const uint8_t* dm, bool skipped, uint32_t i)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(skipped)
+      return Ac(0);
+    const bool dd = __ldg(dm + i) != 0;
+    const Ac sum = row_sum<V, S, NC>(A, i, c);
+    const Ac dk = dd ? Ac(0) : sub(Ac(d[i]), sum);
+    const Ac ck = dd ? Ac(0) : mul(Ac(__ldg(dinv + i)), dk);
+    return add(Ac(c[i]), ck);
+  }
+
+  // exact coarse solve on the free DOFs (FP64 arithmetic whatever S is), one block of NB threads
+  template<typename S, int NB>
+  __device__ __forceinline__ void coarse_block(const S* b, S* x, uint32_t n, const uint32_t* free_dofs,
+    const double* inv, uint32_t m)
+  {
+    for(uint32_t i = threadIdx.x; i < n; i += NB)
+      x[i] = S(0);
+    __syncthreads();
+    for(uint32_t i = threadIdx.x; i < m; i += NB)
+    {
+      double s = 0.0;
+      for(uint32_t j = 0; j < m; ++j)
+        s = add(s, mul(__ldg(inv + size_t(i) * m + j), double(b[__ldg(free_dofs + j)])));
+      x[__ldg(free_dofs + i)] = S(s);
+    }
+  }
+
   template<typename V, typename S>
   __global__ void __launch_bounds__(NT) k_smooth(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ xo, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip,
     const Scalars* __restrict__ sc)
   {
-    typedef typename ValueTraits<V>::acc Ac;
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(A, r0, smem);
-    const uint32_t i = r0 + threadIdx.x;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
     if(i >= A.rows)
       return;
-    S out = S(0);
-    if(!*skip)
-    {
-      const Ac sum = row_sum<V, S>(st, A, i, x);
-      const bool d = dm[i] != 0;
-      const Ac d1 = d ? Ac(0) : sub(Ac(b[i]), sum);
-      const Ac c = d ? Ac(0) : mul(Ac(dinv[i]), d1);
-      out = S(add(Ac(x[i]), c));
-    }
-    xo[i] = out;
+    xo[i] = smooth_row<V, S, true>(A, b, x, dinv, dm, *skip != 0, i);
   }
 
   template<typename V, typename S>
   __global__ void __launch_bounds__(NT) k_defect(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ d, const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
   {
-    typedef typename ValueTraits<V>::acc Ac;
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(A, r0, smem);
-    const uint32_t i = r0 + threadIdx.x;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
     if(i >= A.rows)
       return;
-    const Ac sum = row_sum<V, S>(st, A, i, x);
-    d[i] = dm[i] ? S(0) : S(sub(Ac(b[i]), sum));
+    d[i] = defect_row<V, S, true>(A, b, x, dm, i);
   }
 
-  // coarse rows: b_c = F_c(R d); with_sol: sol1_c = F_c(D_c .* b_c) and ||b_c|| -> skip flag
+  // coarse rows: b_c = F_c(R d); with xc: sol1_c = F_c(D_c .* b_c) and ||b_c|| -> skip flag
   template<typename V, typename S>
   __global__ void __launch_bounds__(NT) k_restrict(DCsr<V> R, const S* __restrict__ d, S* __restrict__ bc,
     S* __restrict__ xc, const S* __restrict__ dinvc, const uint8_t* __restrict__ dmc, int* __restrict__ skipc,
     RedSlot slot, const Scalars* __restrict__ sc)
   {
-    typedef typename ValueTraits<V>::acc Ac;
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(R, r0, smem);
-    const uint32_t j = r0 + threadIdx.x;
+    const uint32_t j = blockIdx.x * NT + threadIdx.x;
     double sq = 0.0;
     if(j < R.rows)
-    {
-      const bool dc = dmc[j] != 0;
-      const Ac sum = row_sum<V, S>(st, R, j, d);
-      const Ac v = dc ? Ac(0) : add(sum, Ac(0));
-      bc[j] = S(v);
-      if(xc)
-      {
-        const Ac c = dc ? Ac(0) : mul(Ac(dinvc[j]), v);
-        xc[j] = S(add(Ac(0), c));
-      }
-      sq = double(v) * double(v);
-    }
+      sq = restrict_row<V, S, true>(R, d, bc, xc, dinvc, dmc, j);
     if(!xc)
       return;
     double total;
@@ -226,41 +276,25 @@ namespace fb
       *skipc = skip_from_norm<S>(sqrt(total));
   }
 
-  // exact coarse solve on the free DOFs (FP64 arithmetic whatever S is)
   template<typename S>
   __global__ void __launch_bounds__(NT) k_coarse(const S* __restrict__ b, S* __restrict__ x, uint32_t n,
     const uint32_t* __restrict__ free_dofs, const double* __restrict__ inv, uint32_t m, const Scalars* __restrict__ sc)
   {
     if(gate_closed(sc))
       return;
-    for(uint32_t i = threadIdx.x; i < n; i += NT)
-      x[i] = S(0);
-    __syncthreads();
-    for(uint32_t i = threadIdx.x; i < m; i += NT)
-    {
-      double s = 0.0;
-      for(uint32_t j = 0; j < m; ++j)
-        s = add(s, mul(inv[size_t(i) * m + j], double(b[free_dofs[j]])));
-      x[free_dofs[i]] = S(s);
-    }
+    coarse_block<S, NT>(b, x, n, free_dofs, inv, m);
   }
 
   template<typename V, typename S>
   __global__ void __launch_bounds__(NT) k_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ x,
     const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
   {
-    typedef typename ValueTraits<V>::acc Ac;
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(P, r0, smem);
-    const uint32_t i = r0 + threadIdx.x;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
     if(i >= P.rows)
       return;
-    const Ac sum = row_sum<V, S>(st, P, i, xc);
-    const Ac c = dm[i] ? Ac(0) : add(sum, Ac(0));
-    x[i] = S(add(Ac(x[i]), c));
+    x[i] = prolong_row<V, S, true>(P, xc, x, dm, i);
   }
 
   template<typename V, typename S>
@@ -268,25 +302,13 @@ namespace fb
     S* __restrict__ d, S* __restrict__ c, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
     int* __restrict__ skip, RedSlot slot, const Scalars* __restrict__ sc)
   {
-    typedef typename ValueTraits<V>::acc Ac;
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(A, r0, smem);
-    const uint32_t i = r0 + threadIdx.x;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
     double sq = 0.0;
     if(i < A.rows)
-    {
-      const bool dd = dm[i] != 0;
-      const Ac sum = row_sum<V, S>(st, A, i, x);
-      const Ac dv = dd ? Ac(0) : sub(Ac(b[i]), sum);
-      d[i] = S(dv);
-      const Ac cv = dd ? Ac(0) : mul(Ac(dinv[i]), dv);
-      c[i] = S(add(Ac(0), cv));
-      sq = double(dv) * double(dv);
-    }
+      sq = post1_row<V, S, true>(A, b, x, d, c, dinv, dm, i);
     double total;
     if(grid_sum_last<NT>(sq, slot, sh, total))
       *skip = skip_from_norm<S>(sqrt(total));
@@ -304,23 +326,12 @@ namespace fb
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t r0 = blockIdx.x * NT;
-    Staged<V> st = stage_rows<V>(A, r0, smem);
-    const uint32_t i = r0 + threadIdx.x;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
     const bool skipped = *skip != 0;
     double rz = 0.0;
     if(i < A.rows)
     {
-      Ac cn = Ac(0);
-      if(!skipped)
-      {
-        const bool dd = dm[i] != 0;
-        const Ac sum = row_sum<V, S>(st, A, i, c);
-        const Ac dk = dd ? Ac(0) : sub(Ac(d[i]), sum);
-        const Ac ck = dd ? Ac(0) : mul(Ac(dinv[i]), dk);
-        cn = add(Ac(c[i]), ck);
-      }
+      const Ac cn = post2_row<V, S, true>(A, d, c, dinv, dm, skipped, i);
       if(!LAST)
         co[i] = S(cn);
       else
@@ -382,6 +393,128 @@ namespace fb
     }
   }
 
+  // ------------------------------------------------------------------ coarse-level tail
+  // The bottom of the V-cycle (levels whose row count is at most the tail threshold, down to the
+  // coarsest) in ONE block of TAIL_NT threads: block-stride loops separated by __syncthreads
+  // replace one kernel launch per pass.  Vectors are read with coherent loads (they are written
+  // inside this kernel); the row bodies are the grid kernels' own.
+  constexpr int TAIL_NT = 512;
+  constexpr int MAX_TAIL = 12;
+
+  template<typename V, typename S>
+  struct TailLevel
+  {
+    DCsr<V> A, P, R;       // P: this <- next coarser, R: next coarser <- this
+    S *b, *x, *x2, *d, *c, *c2;
+    const S* dinv;
+    const uint8_t* dm;
+    int* skip_pre;
+    int* skip_post;
+    uint32_t n;
+  };
+
+  template<typename V, typename S>
+  struct TailParams
+  {
+    TailLevel<V, S> lv[MAX_TAIL];
+    int count;             // tail levels including the coarsest
+    int steps;
+    const uint32_t* free_dofs;
+    const double* inv;
+    uint32_t m;
+  };
+
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(TAIL_NT) k_tail(const __grid_constant__ TailParams<V, S> tp, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    if(gate_closed(sc))
+      return;
+    S* xcur[MAX_TAIL];
+    const int cnt = tp.count;
+    for(int t = 0; t + 1 < cnt; ++t)
+    {
+      const TailLevel<V, S>& f = tp.lv[t];
+      const TailLevel<V, S>& c = tp.lv[t + 1];
+      S* xa = f.x;
+      S* xb = f.x2;
+      for(int k = 1; k < tp.steps; ++k)
+      {
+        const bool skipped = *(volatile int*)f.skip_pre != 0;
+        for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+          xb[i] = smooth_row<V, S, false>(f.A, f.b, xa, f.dinv, f.dm, skipped, i);
+        __syncthreads();
+        S* tmp = xa;
+        xa = xb;
+        xb = tmp;
+      }
+      xcur[t] = xa;
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        f.d[i] = defect_row<V, S, false>(f.A, f.b, xa, f.dm, i);
+      __syncthreads();
+      const bool coarsest = (t + 2 == cnt);
+      double sq = 0.0;
+      for(uint32_t j = threadIdx.x; j < c.n; j += TAIL_NT)
+        sq += restrict_row<V, S, false>(f.R, f.d, c.b, coarsest ? (S*)nullptr : c.x, c.dinv, c.dm, j);
+      const double tot = block_sum<TAIL_NT>(sq, sh);
+      if(threadIdx.x == 0 && !coarsest)
+        *(volatile int*)c.skip_pre = skip_from_norm<S>(sqrt(tot));
+      __syncthreads();
+    }
+    {
+      const TailLevel<V, S>& c = tp.lv[cnt - 1];
+      coarse_block<S, TAIL_NT>(c.b, c.x, c.n, tp.free_dofs, tp.inv, tp.m);
+      xcur[cnt - 1] = c.x;
+      __syncthreads();
+    }
+    for(int t = cnt - 2; t >= 0; --t)
+    {
+      const TailLevel<V, S>& f = tp.lv[t];
+      S* xf = xcur[t];
+      const S* xc = xcur[t + 1];
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
+      __syncthreads();
+      double sq = 0.0;
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        sq += post1_row<V, S, false>(f.A, f.b, xf, f.d, f.c, f.dinv, f.dm, i);
+      const double tot = block_sum<TAIL_NT>(sq, sh);
+      __shared__ int skipped_sh;
+      if(threadIdx.x == 0)
+      {
+        skipped_sh = skip_from_norm<S>(sqrt(tot));
+        *(volatile int*)f.skip_post = skipped_sh;
+      }
+      __syncthreads();
+      const bool skipped = skipped_sh != 0;
+      S* ca = f.c;
+      S* cb = f.c2;
+      if(tp.steps == 1)
+      {
+        for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+          xf[i] = S(add(Ac(xf[i]), skipped ? Ac(0) : Ac(ca[i])));
+        __syncthreads();
+      }
+      for(int k = 2; k <= tp.steps; ++k)
+      {
+        const bool last = (k == tp.steps);
+        for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        {
+          const Ac cn = post2_row<V, S, false>(f.A, f.d, ca, f.dinv, f.dm, skipped, i);
+          if(last)
+            xf[i] = S(add(Ac(xf[i]), cn));
+          else
+            cb[i] = S(cn);
+        }
+        __syncthreads();
+        S* tmp = ca;
+        ca = cb;
+        cb = tmp;
+      }
+    }
+  }
+
   // ------------------------------------------------------------------ PCG passes (FP64)
   // writes the V-cycle input of the top level: b = S(r * scale) (FP32 modes) and
   // sol1 = F(D .* b); returns the scale used.
@@ -414,15 +547,13 @@ namespace fb
     Scalars* __restrict__ sc, cudaGraphConditionalHandle cond)
   {
     __shared__ double sh[32];
-    extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t r0 = blockIdx.x * NT;
-    Staged<double> st = stage_rows<double>(A, r0, smem);
     const uint32_t i = r0 + threadIdx.x;
     double sq = 0.0;
     if(i < A.rows)
     {
       const bool dd = dm[i] != 0;
-      const double sum = row_sum<double, double>(st, A, i, x);
+      const double sum = row_sum<double, double>(A, i, x);
       const double rv = dd ? 0.0 : sub(rhs[i], sum);
       r[i] = rv;
       if(x1)
@@ -487,14 +618,12 @@ namespace fb
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
-    extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t r0 = blockIdx.x * NT;
-    Staged<double> st = stage_rows<double>(A, r0, smem);
     const uint32_t i = r0 + threadIdx.x;
     double qp = 0.0;
     if(i < A.rows)
     {
-      const double sum = row_sum<double, double>(st, A, i, p);
+      const double sum = row_sum<double, double>(A, i, p);
       const double qv = dm[i] ? 0.0 : add(sum, 0.0);
       q[i] = qv;
       qp = mul(qv, p[i]);
@@ -606,15 +735,19 @@ namespace fb
 
   struct DevMat
   {
-    uint32_t rows = 0, cols = 0, nnz = 0, cap = 0;
-    uint32_t *rp = nullptr, *col = nullptr;
-    void* val = nullptr;   // value array in the level's storage type
+    uint32_t rows = 0, cols = 0, nnz = 0;   // nnz: stored entries of non-empty rows
+    uint64_t entries = 0;                   // slots including padding
+    uint32_t* soff = nullptr;
+    uint32_t* col = nullptr;
+    int16_t* dcol = nullptr;
+    void* val = nullptr;                    // value array in the level's storage type
     size_t smem = 0;
+    double bytes = 0;                       // matrix bytes one sweep reads
   };
 
   template<typename V> DCsr<V> view(const DevMat& m)
   {
-    return DCsr<V>{m.rp, m.col, static_cast<const V*>(m.val), m.rows, m.cap};
+    return DCsr<V>{m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows};
   }
 
   struct DevLevel
@@ -657,6 +790,7 @@ struct fb_solver
   cudaGraph_t vgraph = nullptr;
   cudaGraphExec_t vexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   uint64_t launches_init = 0, launches_body = 0, launches_vcycle = 0;
   double bytes_init = 0, bytes_body = 0;
   uint64_t counting = 0;
@@ -689,23 +823,6 @@ namespace fb
   static size_t vsize_of(int prec) { return prec == FB_PREC_F64 ? 8 : 4; }
   static size_t valsize_of(int prec) { return prec == FB_PREC_F64 ? 8 : (prec == FB_PREC_F32 ? 4 : 2); }
 
-  // staging capacity: max over blocks of the aligned slice length, if it fits 96 KB of shared memory
-  static uint32_t staging_cap(const HostCsr& M, size_t vbytes)
-  {
-    uint32_t cap = 0;
-    for(uint32_t r0 = 0; r0 < M.rows; r0 += NT)
-    {
-      const uint32_t re = std::min<uint32_t>(r0 + NT, M.rows);
-      const uint32_t len = M.rp[re] - M.rp[r0] + 16u;
-      cap = std::max(cap, len);
-    }
-    cap = (cap + 7u) & ~7u;
-    const size_t limit = 96 * 1024;
-    if(size_t(cap) * (vbytes + 4) > limit)
-      cap = uint32_t(limit / (vbytes + 4)) & ~7u;
-    return cap;
-  }
-
   static uint16_t to_bf16_rne(float f)
   {
     uint32_t u;
@@ -717,35 +834,105 @@ namespace fb
     return uint16_t(u >> 16);
   }
 
-  static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec)
+  // CSR -> sliced ELL (32-row slices), rows flagged in `empty` stored without entries.
+  static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty)
   {
-    d.rows = M.rows;
-    d.cols = M.cols;
-    d.nnz = uint32_t(M.nnz());
-    const size_t vb = valsize_of(prec);
-    d.cap = staging_cap(M, vb);
-    d.smem = size_t(d.cap) * (vb + 4);
-    FB_TRY(dalloc(s, (void**)&d.rp, sizeof(uint32_t) * (size_t(M.rows) + 1)));
-    FB_TRY(dalloc(s, (void**)&d.col, sizeof(uint32_t) * std::max<size_t>(1, M.nnz())));
-    FB_TRY(dalloc(s, &d.val, vb * std::max<size_t>(1, M.nnz())));
-    FB_CUDA(cudaMemcpy(d.rp, M.rp.data(), sizeof(uint32_t) * (size_t(M.rows) + 1), cudaMemcpyHostToDevice));
-    if(M.nnz())
+    const uint32_t n = M.rows, ns = (n + 31u) / 32u;
+    std::vector<uint32_t> soff(size_t(ns) + 1, 0u);
+    bool narrow = (M.rows == M.cols);
+    uint64_t nnz = 0;
+    auto len = [&](uint32_t r) -> uint32_t
     {
-      FB_CUDA(cudaMemcpy(d.col, M.col.data(), sizeof(uint32_t) * M.nnz(), cudaMemcpyHostToDevice));
+      if(r >= n || (empty && (*empty)[r]))
+        return 0u;
+      return M.rp[r + 1] - M.rp[r];
+    };
+    for(uint32_t sl = 0; sl < ns; ++sl)
+    {
+      uint32_t K = 0;
+      for(uint32_t r = sl * 32u; r < std::min(n, sl * 32u + 32u); ++r)
+      {
+        const uint32_t L = len(r);
+        K = std::max(K, L);
+        nnz += L;
+        for(uint32_t j = M.rp[r]; j < M.rp[r] + L; ++j)
+        {
+          const int64_t dlt = int64_t(M.col[j]) - int64_t(r);
+          if(dlt < -32768 || dlt > 32767)
+            narrow = false;
+        }
+      }
+      soff[sl + 1] = soff[sl] + K * 32u;
+    }
+    const uint64_t entries = soff[ns];
+    std::vector<uint32_t> col;
+    std::vector<int16_t> dcol;
+    std::vector<double> val(entries, 0.0);
+    if(narrow)
+      dcol.assign(entries, 0);
+    else
+      col.assign(entries, M.cols);   // padding reads the zero slot x[cols]
+    for(uint32_t sl = 0; sl < ns; ++sl)
+    {
+      const uint32_t K = (soff[sl + 1] - soff[sl]) / 32u;
+      for(uint32_t lane = 0; lane < 32u; ++lane)
+      {
+        const uint32_t r = sl * 32u + lane;
+        const uint32_t L = len(r);
+        for(uint32_t k = 0; k < K; ++k)
+        {
+          const uint64_t e = soff[sl] + uint64_t(k) * 32u + lane;
+          if(k < L)
+          {
+            const uint32_t j = M.rp[r] + k;
+            val[e] = M.val[j];
+            if(narrow)
+              dcol[e] = int16_t(int64_t(M.col[j]) - int64_t(r));
+            else
+              col[e] = M.col[j];
+          }
+        }
+      }
+    }
+    d.rows = n;
+    d.cols = M.cols;
+    d.nnz = uint32_t(nnz);
+    d.entries = entries;
+    const size_t vb = valsize_of(prec);
+    const size_t cb = narrow ? 2 : 4;
+    d.bytes = double(entries) * double(vb + cb) + double(ns + 1) * 4.0;
+    FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * soff.size()));
+    FB_CUDA(cudaMemcpy(d.soff, soff.data(), sizeof(uint32_t) * soff.size(), cudaMemcpyHostToDevice));
+    const size_t ne = std::max<size_t>(1, size_t(entries));
+    if(narrow)
+    {
+      FB_TRY(dalloc(s, (void**)&d.dcol, 2 * ne));
+      if(entries)
+        FB_CUDA(cudaMemcpy(d.dcol, dcol.data(), 2 * entries, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+      FB_TRY(dalloc(s, (void**)&d.col, 4 * ne));
+      if(entries)
+        FB_CUDA(cudaMemcpy(d.col, col.data(), 4 * entries, cudaMemcpyHostToDevice));
+    }
+    FB_TRY(dalloc(s, &d.val, vb * ne));
+    if(entries)
+    {
       if(prec == FB_PREC_F64)
-        FB_CUDA(cudaMemcpy(d.val, M.val.data(), 8 * M.nnz(), cudaMemcpyHostToDevice));
+        FB_CUDA(cudaMemcpy(d.val, val.data(), 8 * entries, cudaMemcpyHostToDevice));
       else if(prec == FB_PREC_F32)
       {
-        std::vector<float> f(M.nnz());
+        std::vector<float> f(entries);
         for(size_t k = 0; k < f.size(); ++k)
-          f[k] = float(M.val[k]);
+          f[k] = float(val[k]);
         FB_CUDA(cudaMemcpy(d.val, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
       }
       else
       {
-        std::vector<uint16_t> h(M.nnz());
+        std::vector<uint16_t> h(entries);
         for(size_t k = 0; k < h.size(); ++k)
-          h[k] = to_bf16_rne(float(M.val[k]));
+          h[k] = to_bf16_rne(float(val[k]));
         FB_CUDA(cudaMemcpy(d.val, h.data(), 2 * h.size(), cudaMemcpyHostToDevice));
       }
     }
@@ -776,10 +963,10 @@ namespace fb
     DevLevel& L(int i) { return s->lv[size_t(i)]; }
 
     // algorithmic bytes of one CSR sweep: nnz*(val+idx) + (rows+1)*idx + reads of x + rows*out
+    // algorithmic bytes of one sweep: the matrix as stored + gathered vector + row-wise vectors
     double csr_bytes(const DevMat& m, double vec_in, double vec_out)
     {
-      return double(m.nnz) * (double(valsize_of(s->cfg.precision)) + 4.0) + double(m.rows + 1) * 4.0 +
-             double(m.cols) * sizeof(S) + double(m.rows) * sizeof(S) * (vec_in + vec_out);
+      return m.bytes + double(m.cols) * sizeof(S) + double(m.rows) * sizeof(S) * (vec_in + vec_out);
     }
 
     // V-cycle from the top level; the top level's b and sol1 and skip_pre are in place.
@@ -788,9 +975,12 @@ namespace fb
     {
       const int nl = s->nlev;
       const int steps = std::max(1, s->cfg.smooth_steps);
+      const int lt = s->tail_first;   // first level of the single-block tail, -1 = none
       std::vector<void*> xcur(static_cast<size_t>(nl));
       for(int l = 0; l + 1 < nl; ++l)
       {
+        if(lt >= 0 && l >= lt)
+          break;
         DevLevel& f = L(l);
         DevLevel& c = L(l + 1);
         void* xa = f.x;
@@ -813,6 +1003,45 @@ namespace fb
         ++launches;
         bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
       }
+      if(lt >= 0)
+      {
+        TailParams<V, S> tp;
+        std::memset(&tp, 0, sizeof(tp));
+        tp.count = nl - lt;
+        tp.steps = steps;
+        tp.free_dofs = s->free_dofs;
+        tp.inv = s->cinv;
+        tp.m = s->nfree;
+        for(int l = lt; l < nl; ++l)
+        {
+          DevLevel& f = L(l);
+          TailLevel<V, S>& t = tp.lv[l - lt];
+          t.A = view<V>(f.A);
+          if(l + 1 < nl)
+          {
+            t.P = view<V>(f.P);
+            t.R = view<V>(f.R);
+          }
+          t.b = (S*)f.b;
+          t.x = (S*)f.x;
+          t.x2 = (S*)f.x2;
+          t.d = (S*)f.d;
+          t.c = (S*)f.c;
+          t.c2 = (S*)f.c2;
+          t.dinv = (const S*)f.dinv;
+          t.dm = f.dm;
+          t.skip_pre = f.skip_pre;
+          t.skip_post = f.skip_post;
+          t.n = f.n;
+          xcur[size_t(l)] = (l + 1 == nl) ? f.x : (((steps - 1) % 2) ? f.x2 : f.x);
+          if(l + 1 < nl)
+            bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
+        }
+        bytes += double(s->nfree) * s->nfree * 8.0;
+        if(!dry) k_tail<V, S><<<1, TAIL_NT, 0, st>>>(tp, s->sc);
+        ++launches;
+      }
+      else
       {
         DevLevel& c = L(nl - 1);
         if(!dry) k_coarse<S><<<1, NT, 0, st>>>((const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
@@ -822,6 +1051,8 @@ namespace fb
       }
       for(int l = nl - 2; l >= 0; --l)
       {
+        if(lt >= 0 && l >= lt)
+          continue;
         DevLevel& f = L(l);
         void* xf = xcur[size_t(l)];
         if(!dry) k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
@@ -877,7 +1108,7 @@ namespace fb
       if(!dry) k_pcg_init<S><<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->rhs, s->x, s->r, t.dm,
         f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->hist, s->slot, s->sc, 0);
       ++launches;
-      bytes += double(A.nnz) * 12.0 + double(t.n + 1) * 4 + double(t.n) * 8 * 4 + t.n;
+      bytes += A.bytes + double(t.n) * 8 * 4 + t.n;
       if(!f64)
       {
         if(!dry) k_mg_prep<S><<<blocks(t.n), NT, 0, st>>>(s->r, (S*)t.b, (S*)t.x, (const S*)t.dinv, t.dm, t.skip_pre, t.n, 1,
@@ -904,27 +1135,10 @@ namespace fb
           (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
       launches += 3;
       bytes += double(t.n) * 8 * (first ? 2 : 3);                                    // P
-      bytes += double(A.nnz) * 12.0 + double(t.n + 1) * 4 + double(t.n) * 8 * 3 + t.n; // Q
+      bytes += A.bytes + double(t.n) * 8 * 3 + t.n;                                   // Q
       bytes += double(t.n) * 8 * 6 + double(t.n) * (f64 ? 16 : 12) + t.n;             // X
     }
   };
-
-  template<typename V, typename S>
-  static fb_status set_smem_attrs()
-  {
-    const int mx = 100 * 1024;
-    FB_CUDA(cudaFuncSetAttribute(k_smooth<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_defect<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_restrict<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_prolong<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_post1<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_post2<V, S, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_pcg_init<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_pcg_q, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    return FB_OK;
-  }
 
   template<typename V, typename S>
   static fb_status build_graphs(fb_solver* s)
@@ -1054,6 +1268,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->min_iter = 0;
   c->use_graph = 1;
   c->rows_per_block = 0;
+  c->tail_rows = 4096;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -1176,6 +1391,16 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   s->lv.resize(size_t(s->nlev));
   const size_t vs = vsize_of(prec);
   uint32_t max_blocks = 1;
+  // Dirichlet masks in device numbering: their rows are stored empty (the filter discards them)
+  std::vector<std::vector<uint8_t>> dms(size_t(s->nlev));
+  for(int l = 0; l < s->nlev; ++l)
+  {
+    const HostLevel& H = h->levels[size_t(l)];
+    const std::vector<uint32_t>& pf = s->perms[size_t(l)];
+    dms[size_t(l)].resize(H.A.rows);
+    for(uint32_t k = 0; k < H.A.rows; ++k)
+      dms[size_t(l)][k] = H.dmask[pf.empty() ? k : pf[k]];
+  }
   for(int l = 0; l < s->nlev; ++l)
   {
     const HostLevel& H = h->levels[size_t(l)];
@@ -1185,19 +1410,17 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     D.n = H.A.rows;
     max_blocks = std::max(max_blocks, blocks(D.n));
     HostCsr A = permute(H.A, pf, inv_f);
-    FB_TRY(upload_mat(s.get(), D.A, A, prec));
+    FB_TRY(upload_mat(s.get(), D.A, A, prec, &dms[size_t(l)]));
     if(l == 0 && prec != FB_PREC_F64)
-      FB_TRY(upload_mat(s.get(), D.A64, A, FB_PREC_F64));
+      FB_TRY(upload_mat(s.get(), D.A64, A, FB_PREC_F64, &dms[size_t(l)]));
     if(l + 1 < s->nlev)
     {
       const std::vector<uint32_t>& pc = s->perms[size_t(l + 1)];
       const std::vector<uint32_t> inv_c = pc.empty() ? std::vector<uint32_t>() : inverse_perm(pc);
-      FB_TRY(upload_mat(s.get(), D.P, permute(H.P, pf, inv_c), prec));
-      FB_TRY(upload_mat(s.get(), D.R, permute(H.R, pc, inv_f), prec));
+      FB_TRY(upload_mat(s.get(), D.P, permute(H.P, pf, inv_c), prec, &dms[size_t(l)]));
+      FB_TRY(upload_mat(s.get(), D.R, permute(H.R, pc, inv_f), prec, &dms[size_t(l + 1)]));
     }
-    std::vector<uint8_t> dm(D.n);
-    for(uint32_t k = 0; k < D.n; ++k)
-      dm[k] = H.dmask[pf.empty() ? k : pf[k]];
+    const std::vector<uint8_t>& dm = dms[size_t(l)];
     FB_TRY(dalloc(s.get(), (void**)&D.dm, D.n));
     FB_CUDA(cudaMemcpy(D.dm, dm.data(), D.n, cudaMemcpyHostToDevice));
     std::vector<double> dinv = inv_diagonal(A, cfg.omega);
@@ -1254,6 +1477,16 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   FB_TRY(dalloc(s.get(), (void**)&s->sc, sizeof(Scalars)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * (max_blocks + 1)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
+  // the tail starts at the first level (below the top) with at most tail_rows rows, if it has a
+  // coarser level below it
+  s->tail_first = -1;
+  if(cfg.tail_rows > 0)
+    for(int l = 1; l + 1 < s->nlev; ++l)
+      if(s->lv[size_t(l)].n <= uint32_t(cfg.tail_rows))
+      {
+        s->tail_first = (s->nlev - l <= MAX_TAIL) ? l : -1;
+        break;
+      }
   Scalars h0;
   std::memset(&h0, 0, sizeof(h0));
   h0.tol_rel = cfg.tol_rel;
@@ -1269,20 +1502,15 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   fb_status e = FB_OK;
   if(prec == FB_PREC_F64)
   {
-    e = set_smem_attrs<double, double>();
-    if(e == FB_OK) e = build_graphs<double, double>(s.get());
+    e = build_graphs<double, double>(s.get());
   }
   else if(prec == FB_PREC_F32)
   {
-    e = set_smem_attrs<float, float>();
-    if(e == FB_OK) e = set_smem_attrs<double, float>();
-    if(e == FB_OK) e = build_graphs<float, float>(s.get());
+    e = build_graphs<float, float>(s.get());
   }
   else
   {
-    e = set_smem_attrs<bf16_t, float>();
-    if(e == FB_OK) e = set_smem_attrs<double, float>();
-    if(e == FB_OK) e = build_graphs<bf16_t, float>(s.get());
+    e = build_graphs<bf16_t, float>(s.get());
   }
   if(e != FB_OK)
     return e;
@@ -1463,12 +1691,11 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   if(flush_l2 && !s->flush)
     FB_TRY(dalloc(s, &s->flush, flush_bytes));
   const DevMat& A64 = f64 ? t.A : t.A64;
-  const double vb = double(valsize_of(s->cfg.precision));
   const double sv = double(vsize_of(s->cfg.precision));
   if(which == FB_KERNEL_PCG_SPMV)
-    *bytes_per_launch = double(A64.nnz) * 12.0 + double(t.n + 1) * 4.0 + double(t.n) * 8.0 * 2.0 + double(t.n);
+    *bytes_per_launch = A64.bytes + double(t.n) * 8.0 * 2.0 + double(t.n);
   else
-    *bytes_per_launch = double(t.A.nnz) * (vb + 4.0) + double(t.n + 1) * 4.0 + double(t.n) * sv * 3.0 + double(t.n);
+    *bytes_per_launch = t.A.bytes + double(t.n) * sv * 3.0 + double(t.n);
   k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_PROGRESS);
   FB_LAUNCHED(1);
   double total = 0.0;

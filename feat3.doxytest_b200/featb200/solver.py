@@ -202,6 +202,10 @@ class PCG:
     def set_use_graph(self, flag):
         self.cfg.use_graph = 1 if flag else 0
 
+    def set_tail_rows(self, rows):
+        """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
+        self.cfg.tail_rows = int(rows)
+
     def init(self):
         h = self.precond.hierarchy
         omega, steps = h.smoother_params()
@@ -290,7 +294,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
-                        ordering="native", use_graph=True):
+                        ordering="native", use_graph=True, tail_rows=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -308,6 +312,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
     s.set_precision(precision)
     s.set_ordering(ordering)
     s.set_use_graph(use_graph)
+    if tail_rows is not None:
+        s.set_tail_rows(tail_rows)
     h.init()
     s.init()
     return s

@@ -175,10 +175,12 @@ typedef struct
   int min_iter;         /* PCG min_iter (default 0) */
   int use_graph;        /* capture the whole solve in one CUDA graph (1) or launch per kernel (0) */
   int rows_per_block;   /* CSR kernel rows per block, 0 = autotuned */
+  int tail_rows;        /* levels (below the finest) with at most this many rows, down to the
+                           coarsest, run in one single-block kernel per V-cycle; 0 = off */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
- * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks. */
+ * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks, tail below 4096 rows. */
 void fb_solver_config_default(fb_solver_config* cfg);
 
 typedef struct

@@ -25,12 +25,14 @@ def _solve(fb, levels, rhs, **kw):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("ordering,graph", [("native", True), ("native", False), ("rcm", True)])
-def test_fp64_matches_reference(featlib, cuda, name, ordering, graph):
+@pytest.mark.parametrize("ordering,graph,tail", [("native", True, None), ("native", False, None), ("rcm", True, None),
+                                                 ("native", True, 0), ("rcm", False, 0)])
+def test_fp64_matches_reference(featlib, cuda, name, ordering, graph, tail):
+    """tail None: coarse levels in the single-block tail kernel (default); 0: one launch per pass."""
     fb = featlib
     g = load_golden(name)
     lv = to_lafem_levels(g["levels"])
-    s, x, st = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph)
+    s, x, st = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, tail_rows=tail)
     z = s.apply_precond(fb.DenseVector(g["rhs"])).elements
     assert np.array_equal(z, g["vcycle"]), rel_err(z, g["vcycle"])
     assert st == fb.Status.success
@@ -40,7 +42,7 @@ def test_fp64_matches_reference(featlib, cuda, name, ordering, graph):
     assert abs(s.get_def_final() - g["summary"]["def_final"]) <= 1e-9 * g["summary"]["def_final"]
     if ordering == "native" and graph:
         for k, xk_ref in enumerate(g["iterates"], start=1):
-            sk, xk, stk = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, max_iter=k)
+            sk, xk, stk = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, max_iter=k, tail_rows=tail)
             assert rel_err(xk, xk_ref) <= PARITY, k
             assert abs(sk.get_def_final() - g["defects"][k - 1]) <= 1e-9 * g["defects"][k - 1]
 
@@ -67,8 +69,8 @@ def test_fp64_matches_live_reference(featlib, cuda, level, dim):
         vc = np.load(os.path.join(tmp, "vcycle.npy"))
         it2 = np.load(os.path.join(tmp, "iterate_2.npy"))
     lv = conv(levels)
-    for ordering in ("native", "rcm"):
-        s, x, st = _solve(fb, lv, rhs, ordering=ordering)
+    for ordering, tail in (("native", None), ("rcm", None), ("rcm", 0)):
+        s, x, st = _solve(fb, lv, rhs, ordering=ordering, tail_rows=tail)
         assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc)
         assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
         assert rel_err(x, sol) <= PARITY
