@@ -198,7 +198,9 @@ def main():
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
     levels, b, gauss = build_problem(dim, level, rhs_kind)
     n = b.size
-    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm", tail_rows=args.tail_rows)
+    # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
+    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm", tail_rows=args.tail_rows,
+                                    use_graph=not args.profile_solves)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
