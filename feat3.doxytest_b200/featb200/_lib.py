@@ -59,6 +59,7 @@ _PROTOS = {
     "fb_axpy_f32": (I, [P, F, P, P, U64, P]),
     "fb_dot_f64": (I, [P, P, P, U64, P]),
     "fb_dot_f32": (I, [P, P, P, U64, P]),
+    "fb_dot_f64_noalloc": (I, [P, P, P, U64, P]),
     "fb_norm2_f64": (I, [P, P, U64, P]),
     "fb_norm2_f32": (I, [P, P, U64, P]),
     "fb_component_product_f64": (I, [P, P, P, U64, P]),

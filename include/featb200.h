@@ -88,6 +88,17 @@ fb_status fb_axpy_f32(float* r, float a, const float* x, const float* y, uint64_
 fb_status fb_dot_f64(double* result, const double* x, const double* y, uint64_t n, void* stream);
 fb_status fb_dot_f32(float* result, const float* x, const float* y, uint64_t n, void* stream);
 
+/* *result = x^T y like fb_dot_f64, but without allocating any device memory, for callers that
+ * cannot allocate when they need the reduction: processes that give all device memory to their
+ * own pool allocator at start-up, and loops that must not stall on cudaMalloc/cudaFree, which can
+ * synchronise the device.  Its scratch is a fixed 32 KiB array in the library's device image, held
+ * by every GPU that loads the library; n may be at most FB_DOT_NOALLOC_MAX_N (longer vectors are
+ * rejected with FB_ERR_ARG).  The first call on a device looks up the array's device address (with
+ * that device current).  All calls share the array: calls that overlap on the GPU race.
+ * No counterpart in the reference: an addition of this library. */
+#define FB_DOT_NOALLOC_MAX_N 16777216ull
+fb_status fb_dot_f64_noalloc(double* result, const double* x, const double* y, uint64_t n, void* stream);
+
 /* *result = ||x||_2; HOST result, synchronises.  Replaces Arch::Norm2::value (norm.hpp:21, norm.cu:20-59). */
 fb_status fb_norm2_f64(double* result, const double* x, uint64_t n, void* stream);
 fb_status fb_norm2_f32(float* result, const float* x, uint64_t n, void* stream);
