@@ -178,6 +178,8 @@ def main():
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
+    ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
+                    help="device DOF ordering (the generated problems are numbered lexicographically)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -199,7 +201,7 @@ def main():
     levels, b, gauss = build_problem(dim, level, rhs_kind)
     n = b.size
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
-    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering="rcm", tail_rows=args.tail_rows,
+    solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves)
     info_lv = solver.level_info()
 
@@ -268,7 +270,7 @@ def main():
 
     extra = {}
     if not args.no_plain and precision != "f64":
-        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering="rcm")
+        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush.fill_(1)
@@ -324,7 +326,7 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if precision != "f64" else "f64", "data": "synthetic",
                 "config": {"workload": args.workload + ": " + desc, "dofs": int(n), "nnz": int(info_lv[0][1]),
-                           "levels": int(info_lv.shape[0]), "ordering": "rcm", "precision": precision,
+                           "levels": int(info_lv.shape[0]), "ordering": args.ordering, "precision": precision,
                            "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before every timed solve",
                            "iterations": int(np.median(iters))},
                 "spmv_gbs": spmv_gbs, "rel_residual": rel_res,

@@ -50,11 +50,12 @@ namespace fb
   template<typename V>
   struct DCsr
   {
-    const uint32_t* soff;
+    const uint32_t* soff;   // slice offsets (sliced ELL), or nullptr for uniform width
     const uint32_t* col;    // absolute columns, or nullptr
     const int16_t* dcol;    // column - row, or nullptr
     const V* val;
     uint32_t rows;
+    uint32_t kw;            // uniform entries per row (ELL: slice s starts at 32*kw*s), 0 = sliced
   };
 
   struct Scalars
@@ -83,8 +84,18 @@ namespace fb
     typedef typename ValueTraits<V>::acc A;
     constexpr uint32_t U = 9;
     const uint32_t sl = row >> 5;
-    const uint32_t b0 = __ldg(M.soff + sl);
-    const uint32_t K = (__ldg(M.soff + sl + 1) - b0) >> 5;
+    uint32_t b0, K;
+    if(M.kw)
+    {
+      // uniform width: the slice start is computed, no dependent load before the entry loads
+      K = M.kw;
+      b0 = sl * 32u * K;
+    }
+    else
+    {
+      b0 = __ldg(M.soff + sl);
+      K = (__ldg(M.soff + sl + 1) - b0) >> 5;
+    }
     const uint32_t base = b0 + (row & 31u);
     A sum = A(0);
     for(uint32_t k0 = 0; k0 < K; k0 += U)
@@ -141,19 +152,23 @@ namespace fb
     typedef typename ValueTraits<V>::acc Ac;
     if(skipped)
       return S(0);
-    const Ac sum = row_sum<V, S, NC>(A, i, x);
+    // row-wise loads first: they do not depend on the row sum's gathers
     const bool d = __ldg(dm + i) != 0;
-    const Ac d1 = d ? Ac(0) : sub(Ac(b[i]), sum);
-    const Ac c = d ? Ac(0) : mul(Ac(__ldg(dinv + i)), d1);
-    return S(add(Ac(x[i]), c));
+    const Ac bi = Ac(b[i]), xi = Ac(x[i]), di = Ac(__ldg(dinv + i));
+    const Ac sum = row_sum<V, S, NC>(A, i, x);
+    const Ac d1 = d ? Ac(0) : sub(bi, sum);
+    const Ac c = d ? Ac(0) : mul(di, d1);
+    return S(add(xi, c));
   }
 
   template<typename V, typename S, bool NC>
   __device__ __forceinline__ S defect_row(const DCsr<V>& A, const S* b, const S* x, const uint8_t* dm, uint32_t i)
   {
     typedef typename ValueTraits<V>::acc Ac;
+    const bool d = __ldg(dm + i) != 0;
+    const Ac bi = Ac(b[i]);
     const Ac sum = row_sum<V, S, NC>(A, i, x);
-    return __ldg(dm + i) ? S(0) : S(sub(Ac(b[i]), sum));
+    return d ? S(0) : S(sub(bi, sum));
   }
 
   // b_c = F_c(R d) and (xc != null) sol1_c = F_c(D_c .* b_c); returns b_c^2
@@ -163,12 +178,13 @@ namespace fb
   {
     typedef typename ValueTraits<V>::acc Ac;
     const bool dc = __ldg(dmc + j) != 0;
+    const Ac di = xc ? Ac(__ldg(dinvc + j)) : Ac(0);
     const Ac sum = row_sum<V, S, NC>(R, j, d);
     const Ac v = dc ? Ac(0) : add(sum, Ac(0));
     bc[j] = S(v);
     if(xc)
     {
-      const Ac c = dc ? Ac(0) : mul(Ac(__ldg(dinvc + j)), v);
+      const Ac c = dc ? Ac(0) : mul(di, v);
       xc[j] = S(add(Ac(0), c));
     }
     return double(v) * double(v);
@@ -179,9 +195,11 @@ namespace fb
   __device__ __forceinline__ S prolong_row(const DCsr<V>& P, const S* xc, const S* x, const uint8_t* dm, uint32_t i)
   {
     typedef typename ValueTraits<V>::acc Ac;
+    const bool d = __ldg(dm + i) != 0;
+    const Ac xi = Ac(x[i]);
     const Ac sum = row_sum<V, S, NC>(P, i, xc);
-    const Ac c = __ldg(dm + i) ? Ac(0) : add(sum, Ac(0));
-    return S(add(Ac(x[i]), c));
+    const Ac c = d ? Ac(0) : add(sum, Ac(0));
+    return S(add(xi, c));
   }
 
   // d = F(b - A x), c = F(D .* d); returns d^2
@@ -191,10 +209,11 @@ namespace fb
   {
     typedef typename ValueTraits<V>::acc Ac;
     const bool dd = __ldg(dm + i) != 0;
+    const Ac bi = Ac(b[i]), di = Ac(__ldg(dinv + i));
     const Ac sum = row_sum<V, S, NC>(A, i, x);
-    const Ac dv = dd ? Ac(0) : sub(Ac(b[i]), sum);
+    const Ac dv = dd ? Ac(0) : sub(bi, sum);
     d[i] = S(dv);
-    const Ac cv = dd ? Ac(0) : mul(Ac(__ldg(dinv + i)), dv);
+    const Ac cv = dd ? Ac(0) : mul(di, dv);
     c[i] = S(add(Ac(0), cv));
     return double(dv) * double(dv);
   }
@@ -208,10 +227,11 @@ namespace fb
     if(skipped)
       return Ac(0);
     const bool dd = __ldg(dm + i) != 0;
+    const Ac di_ = Ac(d[i]), ci = Ac(c[i]), dv = Ac(__ldg(dinv + i));
     const Ac sum = row_sum<V, S, NC>(A, i, c);
-    const Ac dk = dd ? Ac(0) : sub(Ac(d[i]), sum);
-    const Ac ck = dd ? Ac(0) : mul(Ac(__ldg(dinv + i)), dk);
-    return add(Ac(c[i]), ck);
+    const Ac dk = dd ? Ac(0) : sub(di_, sum);
+    const Ac ck = dd ? Ac(0) : mul(dv, dk);
+    return add(ci, ck);
   }
 
   // exact coarse solve on the free DOFs (FP64 arithmetic whatever S is), one block of NB threads
@@ -553,8 +573,9 @@ namespace fb
     if(i < A.rows)
     {
       const bool dd = dm[i] != 0;
+      const double ri = rhs[i];
       const double sum = row_sum<double, double>(A, i, x);
-      const double rv = dd ? 0.0 : sub(rhs[i], sum);
+      const double rv = dd ? 0.0 : sub(ri, sum);
       r[i] = rv;
       if(x1)
         mg_input<S>(i, rv, dd, 1.0, (S*)nullptr, x1, dinv);
@@ -623,10 +644,12 @@ namespace fb
     double qp = 0.0;
     if(i < A.rows)
     {
+      const bool dd = dm[i] != 0;
+      const double pi = p[i];
       const double sum = row_sum<double, double>(A, i, p);
-      const double qv = dm[i] ? 0.0 : add(sum, 0.0);
+      const double qv = dd ? 0.0 : add(sum, 0.0);
       q[i] = qv;
-      qp = mul(qv, p[i]);
+      qp = mul(qv, pi);
     }
     double total;
     if(grid_sum_last<NT>(qp, slot, sh, total))
@@ -720,10 +743,6 @@ namespace fb
 } // namespace fb
 
 // ==================================================================== host side
-struct fb_hierarchy
-{
-  std::vector<fb::HostLevel> levels;
-};
 
 namespace fb
 {
@@ -743,11 +762,12 @@ namespace fb
     void* val = nullptr;                    // value array in the level's storage type
     size_t smem = 0;
     double bytes = 0;                       // matrix bytes one sweep reads
+    uint32_t kw = 0;                        // uniform width (ELL), 0 = sliced
   };
 
   template<typename V> DCsr<V> view(const DevMat& m)
   {
-    return DCsr<V>{m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows};
+    return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw};
   }
 
   struct DevLevel
@@ -864,6 +884,14 @@ namespace fb
       }
       soff[sl + 1] = soff[sl] + K * 32u;
     }
+    // uniform width (plain ELL) when it stores at most 12.5% more entries than the slices do
+    uint32_t kmax = 0;
+    for(uint32_t sl = 0; sl < ns; ++sl)
+      kmax = std::max(kmax, (soff[sl + 1] - soff[sl]) / 32u);
+    const bool uniform = uint64_t(kmax) * 32u * ns <= soff[ns] + soff[ns] / 8;
+    if(uniform)
+      for(uint32_t sl = 0; sl <= ns; ++sl)
+        soff[sl] = sl * 32u * kmax;
     const uint64_t entries = soff[ns];
     std::vector<uint32_t> col;
     std::vector<int16_t> dcol;
@@ -898,9 +926,10 @@ namespace fb
     d.cols = M.cols;
     d.nnz = uint32_t(nnz);
     d.entries = entries;
+    d.kw = uniform ? kmax : 0u;
     const size_t vb = valsize_of(prec);
     const size_t cb = narrow ? 2 : 4;
-    d.bytes = double(entries) * double(vb + cb) + double(ns + 1) * 4.0;
+    d.bytes = double(entries) * double(vb + cb) + (uniform ? 0.0 : double(ns + 1) * 4.0);
     FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * soff.size()));
     FB_CUDA(cudaMemcpy(d.soff, soff.data(), sizeof(uint32_t) * soff.size(), cudaMemcpyHostToDevice));
     const size_t ne = std::max<size_t>(1, size_t(entries));

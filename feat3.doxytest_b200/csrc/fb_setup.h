@@ -49,3 +49,9 @@ namespace fb
 
   std::vector<uint32_t> inverse_perm(const std::vector<uint32_t>& perm);
 } // namespace fb
+
+// the opaque hierarchy handle of the C ABI: levels finest first, as pushed by the caller
+struct fb_hierarchy
+{
+  std::vector<fb::HostLevel> levels;
+};

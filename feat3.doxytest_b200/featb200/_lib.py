@@ -87,6 +87,10 @@ _PROTOS = {
     "fb_solver_vcycle": (I, [P, P, P]),
     "fb_solver_level_info": (I, [P, P]),
     "fb_solver_time_kernel": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
+    "fb_msolver_create": (I, [C.POINTER(P), P, C.POINTER(SolverConfig), I]),
+    "fb_msolver_destroy": (None, [P]),
+    "fb_msolver_solve": (I, [P, P, P, P]),
+    "fb_msolver_solve_device": (I, [P, P, P, P, P]),
 }
 
 _lib = None

@@ -317,3 +317,77 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
     h.init()
     s.init()
     return s
+
+
+class MultiRhsPCG:
+    """PCG + V-cycle for K = 32 or 64 right-hand sides at once (fb_msolver_*): every right-hand side
+    follows the single-RHS algorithm with its own scalars and stopping test; the matrices are read
+    once per pass for all of them.  Vectors are [rows, K] (right-hand side index fastest), the
+    element layout of the reference's DenseVectorBlocked."""
+
+    def __init__(self, hierarchy: MultiGridHierarchy, num_rhs, tol_rel=1e-8, max_iter=100, precision="f64",
+                 ordering="native", use_graph=True):
+        omega, steps = hierarchy.smoother_params()
+        self.k = int(num_rhs)
+        self.cfg = _lib.SolverConfig()
+        _lib.lib().fb_solver_config_default(C.byref(self.cfg))
+        self.cfg.omega, self.cfg.smooth_steps = omega, steps
+        self.cfg.tol_rel, self.cfg.max_iter = float(tol_rel), int(max_iter)
+        self.cfg.precision, self.cfg.ordering = _lib.PREC[precision], _lib.ORDER[ordering]
+        self.cfg.use_graph = 1 if use_graph else 0
+        if hierarchy._h is None:
+            hierarchy.init()
+        self.hierarchy = hierarchy
+        s = C.c_void_p()
+        _lib.check(_lib.lib().fb_msolver_create(C.byref(s), hierarchy._h, C.byref(self.cfg), self.k),
+                   "fb_msolver_create")
+        self._s = s
+        self.info = (_lib.SolveInfo * self.k)()
+
+    def solve(self, sol, rhs):
+        """sol (initial guesses, overwritten) and rhs: float64 arrays of shape [rows, K]."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        _lib.check(_lib.lib().fb_msolver_solve(self._s, sol.ctypes.data_as(C.c_void_p), rhs.ctypes.data_as(C.c_void_p),
+                                               self.info), "fb_msolver_solve")
+        return sol
+
+    def solve_device(self, sol, rhs, stream=None):
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        _lib.check(_lib.lib().fb_msolver_solve_device(self._s, C.c_void_p(sol.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                                      C.c_void_p(stream.cuda_stream), self.info),
+                   "fb_msolver_solve_device")
+
+    def statuses(self):
+        return [Status(i.status) for i in self.info]
+
+    def iterations(self):
+        return [int(i.iterations) for i in self.info]
+
+    def done(self):
+        if self._s is not None:
+            _lib.lib().fb_msolver_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.done()
+        except Exception:
+            pass
+
+
+def build_hierarchy(levels, omega=0.7, steps=2):
+    """MultiGridHierarchy of Richardson(1)+Jacobi(omega) smoothers and the exact coarse inverse
+    from a finest-first list of level dicts (matrix, filter, transfer)."""
+    h = MultiGridHierarchy(len(levels))
+    for lv in levels[:-1]:
+        jac = new_jacobi_precond(lv["matrix"], lv["filter"], omega)
+        sm = new_richardson(lv["matrix"], lv["filter"], 1.0, jac)
+        sm.set_min_iter(steps)
+        sm.set_max_iter(steps)
+        h.push_level(lv["matrix"], lv["filter"], lv["transfer"], sm, sm, sm)
+    h.push_level(levels[-1]["matrix"], levels[-1]["filter"], new_coarse_inverse())
+    h.init()
+    return h

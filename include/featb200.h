@@ -241,6 +241,26 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
  * removed).  `out` holds 3 * num_levels entries. */
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
 
+/* ------------------------------------------------------------------------------------------ */
+/* 3. Solver level, many right-hand sides: K = 32 or 64 systems with one hierarchy              */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct fb_msolver fb_msolver;
+
+/* Like fb_solver_create for num_rhs (32 or 64) right-hand sides solved together: every right-hand
+ * side runs its own PCG + V-cycle (own scalars, stopping test and smoother skip flags); each matrix
+ * entry is read once per pass for all of them.  FB_PREC_F64 or FB_PREC_F32, smooth_steps >= 2.
+ * Counterpart of solving with DenseVectorBlocked<double, Index, num_rhs> vectors (the reference's
+ * multi-vector CSR kernel, kernel/lafem/arch/apply.cu:109-135, handles up to 3 per row). */
+fb_status fb_msolver_create(fb_msolver** out, fb_hierarchy* h, const fb_solver_config* cfg, int num_rhs);
+void fb_msolver_destroy(fb_msolver* s);
+
+/* sol/rhs: HOST arrays of rows * num_rhs doubles, right-hand side index fastest (x[row*num_rhs+j]);
+ * sol holds the initial guesses.  info: NULL or num_rhs entries (per right-hand side). */
+fb_status fb_msolver_solve(fb_msolver* s, double* sol, const double* rhs, fb_solve_info* info);
+/* As fb_msolver_solve with DEVICE arrays, ordered on `stream`. */
+fb_status fb_msolver_solve_device(fb_msolver* s, double* sol, const double* rhs, void* stream, fb_solve_info* info);
+
 #ifdef __cplusplus
 }
 #endif
