@@ -41,6 +41,13 @@ WORKLOADS = {
                            "as poisson2d_l10_mixed with BF16 matrix values in the V-cycle"),
     "poisson2d_l10_fp64": (2, 10, "gauss", "f64", "plain FP64 PCG + V(2,2) multigrid, L10, 8-Gaussian RHS"),
     "poisson2d_l7_fp64": (2, 7, "sine", "f64", "2D Poisson Q1 L7 (16,641 DOFs), sine-bubble RHS, plain FP64"),
+    "poisson3d_l6_rhs64_mixed": (3, 6, "gauss64", "f32",
+                                 "3D Poisson Q1 unit cube L6 (274,625 DOFs, 27-point), 64 right-hand sides of 8 "
+                                 "Gaussians each (seeds 100..163), solved together, FP32 V(2,2) in FP64 PCG"),
+    "poisson2d_batch256_mixed": (2, 9, "batch", "f32",
+                                 "256 independent -div(kappa grad u)=f instances, levels uniform in 5..9 (seed 7), "
+                                 "kappa = exp(16x16-mode random field), 8-Gaussian RHS, one launch per V-cycle phase, "
+                                 "FP32 V(2,2) in FP64 PCG, tol 1e-8 per instance"),
 }
 DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
 
@@ -122,6 +129,105 @@ def build_problem(dim, level, rhs_kind):
     return levels, b, gauss
 
 
+def _batch_instance(args):
+    level, k = args
+    sys.path.insert(0, os.path.join(ROOT, "feat3.doxytest_b200"))
+    from featb200 import assembly as AS
+    lv, b = AS.poisson_hierarchy(level, 2, rhs="gauss", gauss=AS.gauss_params(10_000 + 2 * k, 2),
+                                 field=AS.field_params(10_001 + 2 * k))
+    return lv, b
+
+
+def batch_levels(count=256, seed=7):
+    return [int(v) for v in np.random.default_rng(seed).integers(5, 10, size=count)]
+
+
+def build_batch_problem(count=256):
+    """Config-4 family generated on a spawn-started process pool (before any CUDA use)."""
+    import multiprocessing as mp
+    levels = batch_levels(count)
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        inst = pool.map(_batch_instance, [(L, k) for k, L in enumerate(levels)])
+    return levels, inst
+
+
+def build_rhs64_problem():
+    from featb200 import assembly as AS
+    levels, _ = AS.poisson_hierarchy(6, 3, rhs="sine")
+    fidx = levels[0]["filter"].indices.astype(np.int64)
+    B = np.zeros((levels[0]["matrix"].rows(), 64))
+    for j in range(64):
+        g = AS.gauss_params(100 + j, 3, width=(0.03, 0.12))
+        b = AS.load_vector(6, lambda *xs: AS.gauss_eval(g, *xs), 3)
+        b[fidx] = 0.0
+        B[:, j] = b
+    return levels, B
+
+
+def run_multi(args, kind):
+    """Secondary workloads: the 64-RHS 3D solve and the 256-instance batch (value = ms per solve of
+    the whole set)."""
+    pre = build_batch_problem() if kind == "batch" else None
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    import featb200 as fb
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    if kind == "batch":
+        levels, inst = pre
+        hs = [fb.build_hierarchy(lv) for lv, _ in inst]
+        solver = fb.BatchPCG(hs, precision=precision, ordering=args.ordering)
+        rhs = np.concatenate([b for _, b in inst])
+        units, dofs = len(inst), int(rhs.size)
+    else:
+        lv, B = build_rhs64_problem()
+        solver = fb.MultiRhsPCG(fb.build_hierarchy(lv), 64, precision=precision, ordering=args.ordering)
+        rhs = B.ravel()
+        units, dofs = 64, int(B.shape[0])
+    stream = torch.cuda.current_stream()
+    rhs_d = torch.tensor(rhs, device="cuda")
+    sol_d = torch.zeros_like(rhs_d)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        sol_d.zero_()
+        solver.solve_device(sol_d, rhs_d, stream)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    wall0 = time.time()
+    l0 = fb.launch_count()
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        sol_d.zero_()
+        ev0.record(stream)
+        solver.solve_device(sol_d, rhs_d, stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+    launches = fb.launch_count() - l0
+    wall1 = time.time()
+    time.sleep(0.3)
+    clk = clocks.stop(wall0, wall1)
+    st = solver.statuses()
+    its = solver.iterations()
+    ms = float(np.mean(times))
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": ms / world, "unit": "ms", "n_gpus": world, "steps": args.steps,
+                          "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+                          "config": {"workload": args.workload + ": " + desc, "solves_per_step": units,
+                                     "dofs_per_step": dofs, "ordering": args.ordering,
+                                     "iterations_max": int(max(its)), "iterations_min": int(min(its)),
+                                     "all_success": all(x == fb.Status.success for x in st),
+                                     "l2": "flushed (256 MiB write) before every timed solve"},
+                          "solves_per_s": units * 1e3 / ms, "gpu_launches": int(launches), "clocks": clk}))
+    return 0
+
+
 def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900):
     """The reference's own CPU solver (oracle/_ref/feat_oracle, built from the reference's sources)
     on the same problem; returns its JSON summary with per-solve times (1 warm-up + reps)."""
@@ -185,6 +291,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload in ("poisson2d_batch256_mixed", "poisson3d_l6_rhs64_mixed"):
+        return run_multi(args, "batch" if "batch" in args.workload else "rhs64")
 
     import torch
     rank, world, local = dist_env()

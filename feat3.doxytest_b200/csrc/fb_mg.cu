@@ -28,6 +28,7 @@
 // (p = z + beta p; r.z and beta come out of the top level's last POST2).  All scalars stay on the
 // device; with use_graph the whole solve is one CUDA graph whose loop is a device-side WHILE node.
 #include "fb_common.cuh"
+#include "fb_rows.cuh"
 #include "fb_setup.h"
 
 #include <algorithm>
@@ -40,24 +41,6 @@ namespace fb
 {
   constexpr int NT = 256;   // rows (threads) per block of every pass
 
-  // ------------------------------------------------------------------ device views
-  // Sliced ELL with slices of 32 rows (one warp): slice s holds K_s = (soff[s+1]-soff[s])/32
-  // entries per row, entry k of row 32s+lane at soff[s] + 32k + lane, in the row's stored order.
-  // Shorter rows are padded with value 0 and a column whose vector entry is always 0 (the zero
-  // slot at index `cols`, or the row itself for narrow storage).  Rows whose result the unit
-  // filter discards (Dirichlet rows) are stored empty.  Column indices are either absolute u32
-  // (`col`) or, for square matrices whose |col - row| fits, int16 offsets from the row (`dcol`).
-  template<typename V>
-  struct DCsr
-  {
-    const uint32_t* soff;   // slice offsets (sliced ELL), or nullptr for uniform width
-    const uint32_t* col;    // absolute columns, or nullptr
-    const int16_t* dcol;    // column - row, or nullptr
-    const V* val;
-    uint32_t rows;
-    uint32_t kw;            // uniform entries per row (ELL: slice s starts at 32*kw*s), 0 = sliced
-  };
-
   struct Scalars
   {
     double gamma, gamma_prev, alpha, beta;
@@ -67,188 +50,9 @@ namespace fb
     int iter, status, min_iter, max_iter;
   };
 
-  __device__ __forceinline__ double ldg_v(const double* p) { return __ldg(p); }
-  __device__ __forceinline__ float ldg_v(const float* p) { return __ldg(p); }
-  __device__ __forceinline__ bf16_t ldg_v(const bf16_t* p)
-  {
-    bf16_t b;
-    b.bits = __ldg(reinterpret_cast<const unsigned short*>(p));
-    return b;
-  }
-
-  // Row sum of row `row` in stored entry order; every product and sum rounded separately.  NC:
-  // gather the vector through the read-only path (vectors not written by the same kernel).
-  template<typename V, typename S, bool NC = true>
-  __device__ __forceinline__ typename ValueTraits<V>::acc row_sum(const DCsr<V>& M, uint32_t row, const S* x)
-  {
-    typedef typename ValueTraits<V>::acc A;
-    constexpr uint32_t U = 9;
-    const uint32_t sl = row >> 5;
-    uint32_t b0, K;
-    if(M.kw)
-    {
-      // uniform width: the slice start is computed, no dependent load before the entry loads
-      K = M.kw;
-      b0 = sl * 32u * K;
-    }
-    else
-    {
-      b0 = __ldg(M.soff + sl);
-      K = (__ldg(M.soff + sl + 1) - b0) >> 5;
-    }
-    const uint32_t base = b0 + (row & 31u);
-    A sum = A(0);
-    for(uint32_t k0 = 0; k0 < K; k0 += U)
-    {
-      A v[U];
-      uint32_t c[U];
-      #pragma unroll
-      for(uint32_t u = 0; u < U; ++u)
-        if(k0 + u < K)
-        {
-          const uint32_t e = base + (k0 + u) * 32u;
-          v[u] = to_acc(ldg_v(M.val + e));
-          c[u] = M.dcol ? uint32_t(int32_t(row) + int32_t(__ldg(M.dcol + e))) : __ldg(M.col + e);
-        }
-      A xv[U];
-      #pragma unroll
-      for(uint32_t u = 0; u < U; ++u)
-        if(k0 + u < K)
-          xv[u] = NC ? A(__ldg(x + c[u])) : A(x[c[u]]);
-      #pragma unroll
-      for(uint32_t u = 0; u < U; ++u)
-        if(k0 + u < K)
-          sum = add(sum, mul(v[u], xv[u]));
-    }
-    return sum;
-  }
-
   __device__ __forceinline__ bool gate_closed(const Scalars* sc)
   {
     return sc->status != FB_SOLVER_PROGRESS;
-  }
-
-  template<typename S> __device__ __forceinline__ S eps_sq();
-  template<> __device__ __forceinline__ double eps_sq<double>() { return EPS64 * EPS64; }
-  template<> __device__ __forceinline__ float eps_sq<float>() { return EPS32 * EPS32; }
-
-  // Richardson's initial-defect test (iterative.hpp:748-771): smooth only if the norm is finite
-  // and above eps^2 of the smoother's precision.
-  template<typename S>
-  __device__ __forceinline__ int skip_from_norm(double nrm)
-  {
-    return (!isfinite(nrm) || nrm <= double(eps_sq<S>())) ? 1 : 0;
-  }
-
-  // ------------------------------------------------------------------ V-cycle passes
-  // Per-row bodies shared by the grid kernels (one thread per row) and the single-block tail
-  // kernel (block-stride loops), so both produce bitwise identical values.
-
-  // Richardson step k >= 2 of the pre-smoother: x' = x + F(D .* F(b - A x)); skipped -> 0
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ S smooth_row(const DCsr<V>& A, const S* b, const S* x, const S* dinv,
-    const uint8_t* dm, bool skipped, uint32_t i)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    if(skipped)
-      return S(0);
-    // row-wise loads first: they do not depend on the row sum's gathers
-    const bool d = __ldg(dm + i) != 0;
-    const Ac bi = Ac(b[i]), xi = Ac(x[i]), di = Ac(__ldg(dinv + i));
-    const Ac sum = row_sum<V, S, NC>(A, i, x);
-    const Ac d1 = d ? Ac(0) : sub(bi, sum);
-    const Ac c = d ? Ac(0) : mul(di, d1);
-    return S(add(xi, c));
-  }
-
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ S defect_row(const DCsr<V>& A, const S* b, const S* x, const uint8_t* dm, uint32_t i)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    const bool d = __ldg(dm + i) != 0;
-    const Ac bi = Ac(b[i]);
-    const Ac sum = row_sum<V, S, NC>(A, i, x);
-    return d ? S(0) : S(sub(bi, sum));
-  }
-
-  // b_c = F_c(R d) and (xc != null) sol1_c = F_c(D_c .* b_c); returns b_c^2
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ double restrict_row(const DCsr<V>& R, const S* d, S* bc, S* xc, const S* dinvc,
-    const uint8_t* dmc, uint32_t j)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    const bool dc = __ldg(dmc + j) != 0;
-    const Ac di = xc ? Ac(__ldg(dinvc + j)) : Ac(0);
-    const Ac sum = row_sum<V, S, NC>(R, j, d);
-    const Ac v = dc ? Ac(0) : add(sum, Ac(0));
-    bc[j] = S(v);
-    if(xc)
-    {
-      const Ac c = dc ? Ac(0) : mul(di, v);
-      xc[j] = S(add(Ac(0), c));
-    }
-    return double(v) * double(v);
-  }
-
-  // x + F(P xc)
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ S prolong_row(const DCsr<V>& P, const S* xc, const S* x, const uint8_t* dm, uint32_t i)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    const bool d = __ldg(dm + i) != 0;
-    const Ac xi = Ac(x[i]);
-    const Ac sum = row_sum<V, S, NC>(P, i, xc);
-    const Ac c = d ? Ac(0) : add(sum, Ac(0));
-    return S(add(xi, c));
-  }
-
-  // d = F(b - A x), c = F(D .* d); returns d^2
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ double post1_row(const DCsr<V>& A, const S* b, const S* x, S* d, S* c, const S* dinv,
-    const uint8_t* dm, uint32_t i)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    const bool dd = __ldg(dm + i) != 0;
-    const Ac bi = Ac(b[i]), di = Ac(__ldg(dinv + i));
-    const Ac sum = row_sum<V, S, NC>(A, i, x);
-    const Ac dv = dd ? Ac(0) : sub(bi, sum);
-    d[i] = S(dv);
-    const Ac cv = dd ? Ac(0) : mul(di, dv);
-    c[i] = S(add(Ac(0), cv));
-    return double(dv) * double(dv);
-  }
-
-  // post-smoothing step k >= 2: c + F(D .* F(d - A c)); skipped -> 0
-  template<typename V, typename S, bool NC>
-  __device__ __forceinline__ typename ValueTraits<V>::acc post2_row(const DCsr<V>& A, const S* d, const S* c,
-    const S* dinv, const uint8_t* dm, bool skipped, uint32_t i)
-  {
-    typedef typename ValueTraits<V>::acc Ac;
-    if(skipped)
-      return Ac(0);
-    const bool dd = __ldg(dm + i) != 0;
-    const Ac di_ = Ac(d[i]), ci = Ac(c[i]), dv = Ac(__ldg(dinv + i));
-    const Ac sum = row_sum<V, S, NC>(A, i, c);
-    const Ac dk = dd ? Ac(0) : sub(di_, sum);
-    const Ac ck = dd ? Ac(0) : mul(dv, dk);
-    return add(ci, ck);
-  }
-
-  // exact coarse solve on the free DOFs (FP64 arithmetic whatever S is), one block of NB threads
-  template<typename S, int NB>
-  __device__ __forceinline__ void coarse_block(const S* b, S* x, uint32_t n, const uint32_t* free_dofs,
-    const double* inv, uint32_t m)
-  {
-    for(uint32_t i = threadIdx.x; i < n; i += NB)
-      x[i] = S(0);
-    __syncthreads();
-    for(uint32_t i = threadIdx.x; i < m; i += NB)
-    {
-      double s = 0.0;
-      for(uint32_t j = 0; j < m; ++j)
-        s = add(s, mul(__ldg(inv + size_t(i) * m + j), double(b[__ldg(free_dofs + j)])));
-      x[__ldg(free_dofs + i)] = S(s);
-    }
   }
 
   template<typename V, typename S>
@@ -854,114 +658,49 @@ namespace fb
     return uint16_t(u >> 16);
   }
 
-  // CSR -> sliced ELL (32-row slices), rows flagged in `empty` stored without entries.
+  // CSR -> the device layout (build_sell), values converted to the storage precision.
   static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty)
   {
-    const uint32_t n = M.rows, ns = (n + 31u) / 32u;
-    std::vector<uint32_t> soff(size_t(ns) + 1, 0u);
-    bool narrow = (M.rows == M.cols);
-    uint64_t nnz = 0;
-    auto len = [&](uint32_t r) -> uint32_t
-    {
-      if(r >= n || (empty && (*empty)[r]))
-        return 0u;
-      return M.rp[r + 1] - M.rp[r];
-    };
-    for(uint32_t sl = 0; sl < ns; ++sl)
-    {
-      uint32_t K = 0;
-      for(uint32_t r = sl * 32u; r < std::min(n, sl * 32u + 32u); ++r)
-      {
-        const uint32_t L = len(r);
-        K = std::max(K, L);
-        nnz += L;
-        for(uint32_t j = M.rp[r]; j < M.rp[r] + L; ++j)
-        {
-          const int64_t dlt = int64_t(M.col[j]) - int64_t(r);
-          if(dlt < -32768 || dlt > 32767)
-            narrow = false;
-        }
-      }
-      soff[sl + 1] = soff[sl] + K * 32u;
-    }
-    // uniform width (plain ELL) when it stores at most 12.5% more entries than the slices do
-    uint32_t kmax = 0;
-    for(uint32_t sl = 0; sl < ns; ++sl)
-      kmax = std::max(kmax, (soff[sl + 1] - soff[sl]) / 32u);
-    const bool uniform = uint64_t(kmax) * 32u * ns <= soff[ns] + soff[ns] / 8;
-    if(uniform)
-      for(uint32_t sl = 0; sl <= ns; ++sl)
-        soff[sl] = sl * 32u * kmax;
-    const uint64_t entries = soff[ns];
-    std::vector<uint32_t> col;
-    std::vector<int16_t> dcol;
-    std::vector<double> val(entries, 0.0);
-    if(narrow)
-      dcol.assign(entries, 0);
-    else
-      col.assign(entries, M.cols);   // padding reads the zero slot x[cols]
-    for(uint32_t sl = 0; sl < ns; ++sl)
-    {
-      const uint32_t K = (soff[sl + 1] - soff[sl]) / 32u;
-      for(uint32_t lane = 0; lane < 32u; ++lane)
-      {
-        const uint32_t r = sl * 32u + lane;
-        const uint32_t L = len(r);
-        for(uint32_t k = 0; k < K; ++k)
-        {
-          const uint64_t e = soff[sl] + uint64_t(k) * 32u + lane;
-          if(k < L)
-          {
-            const uint32_t j = M.rp[r] + k;
-            val[e] = M.val[j];
-            if(narrow)
-              dcol[e] = int16_t(int64_t(M.col[j]) - int64_t(r));
-            else
-              col[e] = M.col[j];
-          }
-        }
-      }
-    }
-    d.rows = n;
-    d.cols = M.cols;
-    d.nnz = uint32_t(nnz);
-    d.entries = entries;
-    d.kw = uniform ? kmax : 0u;
+    const HostSell H = build_sell(M, empty);
+    const uint32_t ns = (H.rows + 31u) / 32u;
+    d.rows = H.rows;
+    d.cols = H.cols;
+    d.nnz = uint32_t(H.nnz);
+    d.entries = H.entries;
+    d.kw = H.kw;
     const size_t vb = valsize_of(prec);
-    const size_t cb = narrow ? 2 : 4;
-    d.bytes = double(entries) * double(vb + cb) + (uniform ? 0.0 : double(ns + 1) * 4.0);
-    FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * soff.size()));
-    FB_CUDA(cudaMemcpy(d.soff, soff.data(), sizeof(uint32_t) * soff.size(), cudaMemcpyHostToDevice));
-    const size_t ne = std::max<size_t>(1, size_t(entries));
-    if(narrow)
+    const size_t cb = H.narrow ? 2 : 4;
+    d.bytes = double(H.entries) * double(vb + cb) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
+    FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * H.soff.size()));
+    FB_CUDA(cudaMemcpy(d.soff, H.soff.data(), sizeof(uint32_t) * H.soff.size(), cudaMemcpyHostToDevice));
+    const size_t ne = std::max<size_t>(1, size_t(H.entries));
+    if(H.narrow)
     {
       FB_TRY(dalloc(s, (void**)&d.dcol, 2 * ne));
-      if(entries)
-        FB_CUDA(cudaMemcpy(d.dcol, dcol.data(), 2 * entries, cudaMemcpyHostToDevice));
+      if(H.entries)
+        FB_CUDA(cudaMemcpy(d.dcol, H.dcol.data(), 2 * H.entries, cudaMemcpyHostToDevice));
     }
     else
     {
       FB_TRY(dalloc(s, (void**)&d.col, 4 * ne));
-      if(entries)
-        FB_CUDA(cudaMemcpy(d.col, col.data(), 4 * entries, cudaMemcpyHostToDevice));
+      if(H.entries)
+        FB_CUDA(cudaMemcpy(d.col, H.col.data(), 4 * H.entries, cudaMemcpyHostToDevice));
     }
     FB_TRY(dalloc(s, &d.val, vb * ne));
-    if(entries)
+    if(H.entries)
     {
       if(prec == FB_PREC_F64)
-        FB_CUDA(cudaMemcpy(d.val, val.data(), 8 * entries, cudaMemcpyHostToDevice));
+        FB_CUDA(cudaMemcpy(d.val, H.val.data(), 8 * H.entries, cudaMemcpyHostToDevice));
       else if(prec == FB_PREC_F32)
       {
-        std::vector<float> f(entries);
-        for(size_t k = 0; k < f.size(); ++k)
-          f[k] = float(val[k]);
+        std::vector<float> f(H.val.begin(), H.val.end());
         FB_CUDA(cudaMemcpy(d.val, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
       }
       else
       {
-        std::vector<uint16_t> h(entries);
+        std::vector<uint16_t> h(H.entries);
         for(size_t k = 0; k < h.size(); ++k)
-          h[k] = to_bf16_rne(float(val[k]));
+          h[k] = to_bf16_rne(float(H.val[k]));
         FB_CUDA(cudaMemcpy(d.val, h.data(), 2 * h.size(), cudaMemcpyHostToDevice));
       }
     }

@@ -185,6 +185,76 @@ namespace fb
     return d;
   }
 
+  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow)
+  {
+    HostSell H;
+    const uint32_t n = M.rows, ns = (n + 31u) / 32u;
+    H.rows = n;
+    H.cols = M.cols;
+    H.soff.assign(size_t(ns) + 1, 0u);
+    bool narrow = allow_narrow && (M.rows == M.cols);
+    auto len = [&](uint32_t r) -> uint32_t
+    {
+      if(r >= n || (empty && (*empty)[r]))
+        return 0u;
+      return M.rp[r + 1] - M.rp[r];
+    };
+    for(uint32_t sl = 0; sl < ns; ++sl)
+    {
+      uint32_t K = 0;
+      for(uint32_t r = sl * 32u; r < std::min(n, sl * 32u + 32u); ++r)
+      {
+        const uint32_t L = len(r);
+        K = std::max(K, L);
+        H.nnz += L;
+        for(uint32_t j = M.rp[r]; j < M.rp[r] + L; ++j)
+        {
+          const int64_t dlt = int64_t(M.col[j]) - int64_t(r);
+          if(dlt < -32768 || dlt > 32767)
+            narrow = false;
+        }
+      }
+      H.soff[sl + 1] = H.soff[sl] + K * 32u;
+    }
+    uint32_t kmax = 0;
+    for(uint32_t sl = 0; sl < ns; ++sl)
+      kmax = std::max(kmax, (H.soff[sl + 1] - H.soff[sl]) / 32u);
+    const bool uniform = uint64_t(kmax) * 32u * ns <= H.soff[ns] + H.soff[ns] / 8;
+    if(uniform)
+    {
+      for(uint32_t sl = 0; sl <= ns; ++sl)
+        H.soff[sl] = sl * 32u * kmax;
+      H.kw = kmax;
+    }
+    H.entries = H.soff[ns];
+    H.narrow = narrow;
+    H.val.assign(H.entries, 0.0);
+    if(narrow)
+      H.dcol.assign(H.entries, 0);
+    else
+      H.col.assign(H.entries, M.cols);
+    for(uint32_t sl = 0; sl < ns; ++sl)
+    {
+      const uint32_t K = (H.soff[sl + 1] - H.soff[sl]) / 32u;
+      for(uint32_t lane = 0; lane < 32u; ++lane)
+      {
+        const uint32_t r = sl * 32u + lane;
+        const uint32_t L = len(r);
+        for(uint32_t k = 0; k < K && k < L; ++k)
+        {
+          const uint64_t e = H.soff[sl] + uint64_t(k) * 32u + lane;
+          const uint32_t j = M.rp[r] + k;
+          H.val[e] = M.val[j];
+          if(narrow)
+            H.dcol[e] = int16_t(int64_t(M.col[j]) - int64_t(r));
+          else
+            H.col[e] = M.col[j];
+        }
+      }
+    }
+    return H;
+  }
+
   void coarse_inverse(const HostCsr& A, const std::vector<uint8_t>& dmask, std::vector<uint32_t>& free_dofs,
                       std::vector<double>& inv)
   {

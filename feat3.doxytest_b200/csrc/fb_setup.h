@@ -48,6 +48,23 @@ namespace fb
                       std::vector<double>& inv);
 
   std::vector<uint32_t> inverse_perm(const std::vector<uint32_t>& perm);
+
+  // A matrix in the device layout of the solvers: sliced ELL with 32-row slices (entry k of row
+  // 32s+lane at soff[s] + 32k + lane, stored order kept), or plain ELL (uniform width kw, when it
+  // stores at most 12.5% more entries).  Rows flagged in `empty` are stored without entries;
+  // padding has value 0 and the zero-slot column `cols` (or offset 0 for narrow storage).  Square
+  // matrices whose |col - row| fits in int16 get 2-byte column offsets (dcol) instead of col.
+  struct HostSell
+  {
+    uint32_t rows = 0, cols = 0, kw = 0;
+    uint64_t nnz = 0, entries = 0;
+    bool narrow = false;
+    std::vector<uint32_t> soff;
+    std::vector<uint32_t> col;
+    std::vector<int16_t> dcol;
+    std::vector<double> val;
+  };
+  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow = true);
 } // namespace fb
 
 // the opaque hierarchy handle of the C ABI: levels finest first, as pushed by the caller

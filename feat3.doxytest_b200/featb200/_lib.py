@@ -91,6 +91,11 @@ _PROTOS = {
     "fb_msolver_destroy": (None, [P]),
     "fb_msolver_solve": (I, [P, P, P, P]),
     "fb_msolver_solve_device": (I, [P, P, P, P, P]),
+    "fb_batch_create": (I, [C.POINTER(P), I, C.POINTER(P), C.POINTER(SolverConfig)]),
+    "fb_batch_destroy": (None, [P]),
+    "fb_batch_sizes": (I, [P, P]),
+    "fb_batch_solve": (I, [P, P, P, P]),
+    "fb_batch_solve_device": (I, [P, P, P, P, P]),
 }
 
 _lib = None

@@ -391,3 +391,70 @@ def build_hierarchy(levels, omega=0.7, steps=2):
     h.push_level(levels[-1]["matrix"], levels[-1]["filter"], new_coarse_inverse())
     h.init()
     return h
+
+
+class BatchPCG:
+    """Many independent PCG + V-cycle solves of uneven size (fb_batch_*): every V-cycle pass is one
+    launch over all instances; each instance has its own scalars and stopping test.  Vectors are
+    packed: the instances' fine-level vectors concatenated in order."""
+
+    def __init__(self, hierarchies, tol_rel=1e-8, max_iter=100, precision="f64", ordering="native",
+                 use_graph=True):
+        omega, steps = hierarchies[0].smoother_params()
+        for h in hierarchies:
+            if h.smoother_params() != (omega, steps):
+                raise _lib.FeatB200Error("all instances must use the same smoother parameters")
+            if h._h is None:
+                h.init()
+        self.hierarchies = list(hierarchies)
+        self.j = len(self.hierarchies)
+        self.cfg = _lib.SolverConfig()
+        _lib.lib().fb_solver_config_default(C.byref(self.cfg))
+        self.cfg.omega, self.cfg.smooth_steps = omega, steps
+        self.cfg.tol_rel, self.cfg.max_iter = float(tol_rel), int(max_iter)
+        self.cfg.precision, self.cfg.ordering = _lib.PREC[precision], _lib.ORDER[ordering]
+        self.cfg.use_graph = 1 if use_graph else 0
+        arr = (C.c_void_p * self.j)(*[h._h.value for h in self.hierarchies])
+        s = C.c_void_p()
+        _lib.check(_lib.lib().fb_batch_create(C.byref(s), self.j, arr, C.byref(self.cfg)), "fb_batch_create")
+        self._s = s
+        sizes = np.zeros(self.j, dtype=np.uint64)
+        _lib.check(_lib.lib().fb_batch_sizes(self._s, sizes.ctypes.data_as(C.c_void_p)), "fb_batch_sizes")
+        self.sizes = sizes.astype(np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        self.info = (_lib.SolveInfo * self.j)()
+
+    def solve(self, sol, rhs):
+        """sol (initial guesses, overwritten) and rhs: packed float64 arrays."""
+        sol = np.ascontiguousarray(sol, dtype=np.float64)
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        _lib.check(_lib.lib().fb_batch_solve(self._s, sol.ctypes.data_as(C.c_void_p), rhs.ctypes.data_as(C.c_void_p),
+                                             self.info), "fb_batch_solve")
+        return sol
+
+    def solve_device(self, sol, rhs, stream=None):
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        _lib.check(_lib.lib().fb_batch_solve_device(self._s, C.c_void_p(sol.data_ptr()), C.c_void_p(rhs.data_ptr()),
+                                                    C.c_void_p(stream.cuda_stream), self.info), "fb_batch_solve_device")
+
+    def split(self, packed):
+        return [packed[self.offsets[k]:self.offsets[k + 1]] for k in range(self.j)]
+
+    def statuses(self):
+        return [Status(i.status) for i in self.info]
+
+    def iterations(self):
+        return [int(i.iterations) for i in self.info]
+
+    def done(self):
+        if self._s is not None:
+            _lib.lib().fb_batch_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.done()
+        except Exception:
+            pass

@@ -261,6 +261,27 @@ fb_status fb_msolver_solve(fb_msolver* s, double* sol, const double* rhs, fb_sol
 /* As fb_msolver_solve with DEVICE arrays, ordered on `stream`. */
 fb_status fb_msolver_solve_device(fb_msolver* s, double* sol, const double* rhs, void* stream, fb_solve_info* info);
 
+/* ------------------------------------------------------------------------------------------ */
+/* 4. Solver level, batches: many independent systems of uneven size                           */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct fb_batch fb_batch;
+
+/* A batch of num independent PCG + V-cycle solves, one hierarchy each (any number of levels, at
+ * least 2).  Every V-cycle pass runs as ONE launch over all instances present at that level
+ * (levels aligned from the coarsest); each instance keeps its own scalars, stopping test and
+ * skip flags, and converged instances stop working.  The reference solves such families one
+ * system after the other. */
+fb_status fb_batch_create(fb_batch** out, int num, fb_hierarchy* const* hierarchies, const fb_solver_config* cfg);
+void fb_batch_destroy(fb_batch* b);
+/* top_rows[num]: finest-level size of every instance (the packed vector is their concatenation) */
+fb_status fb_batch_sizes(const fb_batch* b, uint64_t* top_rows);
+/* sol/rhs: HOST packed arrays (instances concatenated in order, each in its caller numbering);
+ * sol holds the initial guesses.  info: NULL or num entries. */
+fb_status fb_batch_solve(fb_batch* b, double* sol, const double* rhs, fb_solve_info* info);
+/* As fb_batch_solve with DEVICE packed arrays, ordered on `stream`. */
+fb_status fb_batch_solve_device(fb_batch* b, double* sol, const double* rhs, void* stream, fb_solve_info* info);
+
 #ifdef __cplusplus
 }
 #endif
