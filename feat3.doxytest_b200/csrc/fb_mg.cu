@@ -29,6 +29,7 @@
 // device; with use_graph the whole solve is one CUDA graph whose loop is a device-side WHILE node.
 #include "fb_common.cuh"
 #include "fb_rows.cuh"
+#include "fb_tma.cuh"
 #include "fb_setup.h"
 
 #include <algorithm>
@@ -216,6 +217,132 @@ namespace fb
       sc->beta = total / sc->gamma_prev;
     }
   }
+
+  // ------------------------------------------------------------------ TMA-staged pass epilogues
+  // Row epilogues for k_tma_pass (fb_tma.cuh); each repeats the arithmetic of the matching row body
+  // (fb_rows.cuh) on a row sum computed from the staged chunk, so both paths round identically.
+  template<typename V, typename S>
+  struct OpSmooth
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b, x, di; bool d; };
+    static constexpr bool REDUCES = false;
+    const S* b; const S* x; S* xo; const S* dinv; const uint8_t* dm; const int* skip; const Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const { return Pre{Ac(b[i]), Ac(x[i]), Ac(__ldg(dinv + i)), __ldg(dm + i) != 0}; }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      S out = S(0);
+      if(!*skip)
+      {
+        const Ac d1 = p.d ? Ac(0) : sub(p.b, sum);
+        const Ac c = p.d ? Ac(0) : mul(p.di, d1);
+        out = S(add(p.x, c));
+      }
+      xo[i] = out;
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
+  template<typename V, typename S>
+  struct OpDefect
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b; bool d; };
+    static constexpr bool REDUCES = false;
+    const S* b; S* dv; const uint8_t* dm; const Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const { return Pre{Ac(b[i]), __ldg(dm + i) != 0}; }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      dv[i] = p.d ? S(0) : S(sub(p.b, sum));
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
+  template<typename V, typename S>
+  struct OpPost1
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b, di; bool d; };
+    static constexpr bool REDUCES = true;
+    const S* b; S* dv; S* cv; const S* dinv; const uint8_t* dm; int* skip; const Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const { return Pre{Ac(b[i]), Ac(__ldg(dinv + i)), __ldg(dm + i) != 0}; }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      const Ac d = p.d ? Ac(0) : sub(p.b, sum);
+      dv[i] = S(d);
+      const Ac c = p.d ? Ac(0) : mul(p.di, d);
+      cv[i] = S(add(Ac(0), c));
+      return double(d) * double(d);
+    }
+    __device__ void finish(double total) const { *skip = skip_from_norm<S>(sqrt(total)); }
+  };
+
+  template<typename V, typename S, bool LAST, bool TOP>
+  struct OpPost2
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac d, c, di, x; double r; bool dd; };
+    static constexpr bool REDUCES = LAST && TOP;
+    const S* dv; const S* cv; S* co; S* x; double* z; const double* r; const S* dinv; const uint8_t* dm;
+    const int* skip; Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      return Pre{Ac(dv[i]), Ac(cv[i]), Ac(__ldg(dinv + i)), LAST ? Ac(x[i]) : Ac(0), TOP ? r[i] : 0.0,
+                 __ldg(dm + i) != 0};
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      Ac cn = Ac(0);
+      if(!*skip)
+      {
+        const Ac dk = p.dd ? Ac(0) : sub(p.d, sum);
+        const Ac ck = p.dd ? Ac(0) : mul(p.di, dk);
+        cn = add(p.c, ck);
+      }
+      if(!LAST)
+      {
+        co[i] = S(cn);
+        return 0.0;
+      }
+      const S xn = S(add(p.x, cn));
+      if(TOP)
+      {
+        const double zi = mul(double(xn), sc->mg_inv_scale);
+        z[i] = zi;
+        return mul(p.r, zi);
+      }
+      x[i] = xn;
+      return 0.0;
+    }
+    __device__ void finish(double total) const
+    {
+      sc->gamma_prev = sc->gamma;
+      sc->gamma = total;
+      sc->beta = total / sc->gamma_prev;
+    }
+  };
+
+  struct OpPcgQ
+  {
+    struct Pre { double p; bool d; };
+    static constexpr bool REDUCES = true;
+    const double* p; double* q; const uint8_t* dm; Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const { return Pre{p[i], dm[i] != 0}; }
+    __device__ double operator()(uint32_t i, double sum, const Pre& pr) const
+    {
+      const double qv = pr.d ? 0.0 : add(sum, 0.0);
+      q[i] = qv;
+      return mul(qv, pr.p);
+    }
+    __device__ void finish(double total) const { sc->alpha = sc->gamma / total; }
+  };
 
   // ------------------------------------------------------------------ coarse-level tail
   // The bottom of the V-cycle (levels whose row count is at most the tail threshold, down to the
@@ -615,6 +742,8 @@ struct fb_solver
   cudaGraphExec_t vexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
+  int nsm = 148;          // streaming multiprocessors of the device
+  int* err = nullptr;     // device error word (bounded waits that expired)
   uint64_t launches_init = 0, launches_body = 0, launches_vcycle = 0;
   double bytes_init = 0, bytes_body = 0;
   uint64_t counting = 0;
@@ -725,6 +854,33 @@ namespace fb
     fb_solver* s;
     cudaStream_t st;
     bool dry = false;          // count launches and bytes only
+
+    bool use_tma_f64(const DevMat& m) const
+    {
+      if(s->cfg.tma_rows <= 0 || !m.kw || m.rows < uint32_t(s->cfg.tma_rows))
+        return false;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kw, m.dcol != nullptr) <= 100u * 1024u;
+    }
+
+    // the TMA-staged pass serves uniform-width matrices of at least tma_rows rows whose stages fit
+    bool use_tma(const DevMat& m) const
+    {
+      if(s->cfg.tma_rows <= 0 || !m.kw || m.rows < uint32_t(s->cfg.tma_rows))
+        return false;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kw, m.dcol != nullptr) <= 100u * 1024u;
+    }
+    template<typename VV, typename XS, class Op>
+    void tma(const DevMat& m, const void* x, const Op& op)
+    {
+      const uint32_t sb = tma_stage_bytes<VV>(m.kw, m.dcol != nullptr);
+      const size_t smem = size_t(TMA_STAGES) * sb;
+      const uint32_t padded = (m.rows + 31u) & ~31u;
+      const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
+      const uint32_t bps = std::max(1u, std::min(8u, uint32_t((200u * 1024u) / (smem + 2048u))));
+      const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
+      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, op, s->slot,
+                                                        s->err);
+    }
     uint64_t launches = 0;
     double bytes = 0;
 
@@ -755,14 +911,24 @@ namespace fb
         void* xb = f.x2;
         for(int k = 1; k < steps; ++k)
         {
-          if(!dry) k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
-            (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
+          if(dry)
+            ;
+          else if(use_tma(f.A))
+            tma<V, S>(f.A, xa, OpSmooth<V, S>{(const S*)f.b, (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.skip_pre, s->sc});
+          else
+            k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+              (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
           ++launches;
           bytes += csr_bytes(f.A, 3, 1) + f.n;
           std::swap(xa, xb);
         }
         xcur[size_t(l)] = xa;
-        if(!dry) k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
+        if(dry)
+          ;
+        else if(use_tma(f.A))
+          tma<V, S>(f.A, xa, OpDefect<V, S>{(const S*)f.b, (S*)f.d, f.dm, s->sc});
+        else
+          k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
         ++launches;
         bytes += csr_bytes(f.A, 1, 1) + f.n;
         const bool coarsest = (l + 2 == nl);
@@ -826,8 +992,13 @@ namespace fb
         if(!dry) k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
         ++launches;
         bytes += csr_bytes(f.P, 1, 1) + f.n;
-        if(!dry) k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
-          (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+        if(dry)
+          ;
+        else if(use_tma(f.A))
+          tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+        else
+          k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+            (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
         ++launches;
         bytes += csr_bytes(f.A, 2, 2) + f.n;
         const bool top = pcg_top && l == 0;
@@ -850,6 +1021,18 @@ namespace fb
           const bool last = (k == steps);
           if(dry)
             ;
+          else if(use_tma(f.A))
+          {
+            if(!last)
+              tma<V, S>(f.A, ca, OpPost2<V, S, false, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
+                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+            else if(top)
+              tma<V, S>(f.A, ca, OpPost2<V, S, true, true>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, s->z, s->r,
+                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+            else
+              tma<V, S>(f.A, ca, OpPost2<V, S, true, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
+                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+          }
           else if(!last)
             k_post2<V, S, false, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
               (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
@@ -892,7 +1075,12 @@ namespace fb
       const bool f64 = s->cfg.precision == FB_PREC_F64;
       const DevMat& A = A64();
       if(!dry) k_pcg_p<<<blocks(t.n), NT, 0, st>>>(s->p, s->z, t.n, first ? 1 : 0, s->sc);
-      if(!dry) k_pcg_q<<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->p, s->q, t.dm, s->slot, s->sc);
+      if(dry)
+        ;
+      else if(use_tma_f64(A))
+        tma<double, double>(A, s->p, OpPcgQ{s->p, s->q, t.dm, s->sc});
+      else
+        k_pcg_q<<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->p, s->q, t.dm, s->slot, s->sc);
       if(dry)
         ;
       else if(f64)
@@ -907,6 +1095,21 @@ namespace fb
       bytes += double(t.n) * 8 * 6 + double(t.n) * (f64 ? 16 : 12) + t.n;             // X
     }
   };
+
+  // dynamic shared memory above 48 KB for the TMA-staged passes
+  template<typename V, typename S>
+  static fb_status set_tma_attrs()
+  {
+    const int mx = 160 * 1024;
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpSmooth<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpDefect<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost1<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, false, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    return FB_OK;
+  }
 
   template<typename V, typename S>
   static fb_status build_graphs(fb_solver* s)
@@ -1037,6 +1240,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->use_graph = 1;
   c->rows_per_block = 0;
   c->tail_rows = 4096;
+  c->tma_rows = 32768;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -1243,6 +1447,12 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   }
   FB_TRY(dalloc(s.get(), (void**)&s->hist, sizeof(double) * (size_t(cfg.max_iter) + 2)));
   FB_TRY(dalloc(s.get(), (void**)&s->sc, sizeof(Scalars)));
+  FB_TRY(dalloc(s.get(), (void**)&s->err, sizeof(int)));
+  {
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    FB_CUDA(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev));
+  }
   FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * (max_blocks + 1)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
   // the tail starts at the first level (below the top) with at most tail_rows rows, if it has a
@@ -1268,6 +1478,14 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   FB_CUDA(cudaMemcpy(s->sc, &h0, sizeof(h0), cudaMemcpyHostToDevice));
 
   fb_status e = FB_OK;
+  if(prec == FB_PREC_F64)
+    e = set_tma_attrs<double, double>();
+  else if(prec == FB_PREC_F32)
+    e = set_tma_attrs<float, float>();
+  else
+    e = set_tma_attrs<bf16_t, float>();
+  if(e != FB_OK)
+    return e;
   if(prec == FB_PREC_F64)
   {
     e = build_graphs<double, double>(s.get());
@@ -1316,8 +1534,16 @@ static fb_status solve_common(fb_solver* s, fb_solve_info* info)
     return e;
   FB_CUDA(cudaEventRecord(s->ev1, st));
   Scalars h;
+  int err = 0;
   FB_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+  FB_CUDA(cudaMemcpyAsync(&err, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   FB_CUDA(cudaStreamSynchronize(st));
+  if(err)
+  {
+    FB_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
+    set_error("solve: a bounded wait for staged matrix data expired (results invalid)");
+    return FB_ERR_CUDA;
+  }
   (void)n0;
   count_launches(s->launches_init + (h.iter > 1 ? uint64_t(h.iter - 1) : 0) * s->launches_body);
   if(info)

@@ -1,0 +1,197 @@
+// TMA-staged row passes for uniform-width (ELL) matrices.
+//
+// A persistent block walks over chunks of CR consecutive rows.  The chunk's values and column
+// offsets (contiguous in ELL storage) are copied into shared memory by the bulk-copy engine
+// (cp.async.bulk ... mbarrier::complete_tx), NSTAGE chunks ahead of the threads, so the matrix
+// stream occupies no registers and stays in flight while the threads gather x from L1/L2 and
+// apply the pass's row epilogue.  Every mbarrier wait is bounded: on expiry the kernel records the
+// failure in an error word, waits (bounded) for its copies still in flight, and returns.
+#pragma once
+
+#include "fb_rows.cuh"
+
+namespace fb
+{
+  constexpr int TMA_NT = 256;          // threads = rows per chunk
+  constexpr int TMA_STAGES = 3;
+  constexpr uint32_t TMA_SPIN = 1u << 22;
+
+  __device__ __forceinline__ uint32_t smem_u32(const void* p)
+  {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+  }
+
+  __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+  {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+  }
+
+  __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+  {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+  }
+
+  __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+  {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+  }
+
+  // bounded wait for the phase with parity `par` of `bar`; false when the limit expired
+  __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t par)
+  {
+    const uint32_t a = smem_u32(bar);
+    for(uint32_t it = 0; it < TMA_SPIN; ++it)
+    {
+      uint32_t ok;
+      asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                   : "=r"(ok) : "r"(a), "r"(par) : "memory");
+      if(ok)
+        return true;
+      if(it > 32)
+        __nanosleep(128);
+    }
+    return false;
+  }
+
+  // row sum of local row `lr` (0..CR-1) of the staged chunk: entry k of row 32*ls+lane at
+  // ls*32*K + 32*k + lane, in stored order; the column is absolute or row-relative
+  template<typename V, typename S>
+  __device__ __forceinline__ typename ValueTraits<V>::acc staged_row_sum(const V* sv, const int16_t* sd,
+    const uint32_t* sc, uint32_t K, uint32_t lr, uint32_t row, const S* __restrict__ x)
+  {
+    typedef typename ValueTraits<V>::acc A;
+    constexpr uint32_t U = 9;
+    const uint32_t base = (lr >> 5) * 32u * K + (lr & 31u);
+    A sum = A(0);
+    for(uint32_t k0 = 0; k0 < K; k0 += U)
+    {
+      A xv[U];
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        if(k0 + u < K)
+        {
+          const uint32_t e = base + (k0 + u) * 32u;
+          const uint32_t c = sd ? uint32_t(int32_t(row) + int32_t(sd[e])) : sc[e];
+          xv[u] = A(__ldg(x + c));
+        }
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        if(k0 + u < K)
+          sum = add(sum, mul(to_acc(sv[base + (k0 + u) * 32u]), xv[u]));
+    }
+    return sum;
+  }
+
+  // Shared memory bytes of one stage for a matrix of width K.
+  template<typename V>
+  __host__ __device__ __forceinline__ uint32_t tma_stage_bytes(uint32_t K, bool narrow)
+  {
+    return uint32_t(TMA_NT) * K * uint32_t(sizeof(V) + (narrow ? 2u : 4u));
+  }
+
+  // Generic persistent pass: for every row i < A.rows, op(i, sum_i, op.pre(i)) with
+  // sum_i = (A x)_i; op returns the row's contribution to an optional grid reduction, finished by
+  // op.finish(total) in thread 0 of the last block.  padded_rows = the ELL storage rows (a
+  // multiple of 32).
+  template<typename V, typename S, class Op>
+  __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
+    Op op, RedSlot slot, int* err)
+  {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    __shared__ __align__(8) uint64_t bar[TMA_STAGES];
+    __shared__ double sh[32];
+    if(op.closed())
+      return;
+    const uint32_t K = A.kw;
+    const bool narrow = A.dcol != nullptr;
+    const uint32_t sb = tma_stage_bytes<V>(K, narrow);
+    const uint32_t nch = (padded_rows + TMA_NT - 1) / TMA_NT;
+    auto issue = [&](uint32_t c, int s)
+    {
+      const uint32_t r0 = c * TMA_NT;
+      const uint32_t rows = min(uint32_t(TMA_NT), padded_rows - r0);
+      const uint32_t vb = rows * K * uint32_t(sizeof(V));
+      const uint32_t cb = rows * K * (narrow ? 2u : 4u);
+      unsigned char* st = tma_smem + size_t(s) * sb;
+      mbar_expect_tx(&bar[s], vb + cb);
+      bulk_g2s(st, A.val + size_t(r0) * K, vb, &bar[s]);
+      if(narrow)
+        bulk_g2s(st + size_t(TMA_NT) * K * sizeof(V), A.dcol + size_t(r0) * K, cb, &bar[s]);
+      else
+        bulk_g2s(st + size_t(TMA_NT) * K * sizeof(V), A.col + size_t(r0) * K, cb, &bar[s]);
+    };
+    if(threadIdx.x == 0)
+    {
+      for(int s = 0; s < TMA_STAGES; ++s)
+        mbar_init(&bar[s], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if(threadIdx.x == 0)
+      for(int s = 0; s < TMA_STAGES; ++s)
+      {
+        const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
+        if(c < nch)
+          issue(c, s);
+      }
+    double part = 0.0;
+    bool failed = false;
+    uint32_t it = 0;
+    for(uint32_t c = blockIdx.x; c < nch; c += gridDim.x, ++it)
+    {
+      const int s = int(it % TMA_STAGES);
+      const uint32_t par = (it / TMA_STAGES) & 1u;
+      const bool ok = mbar_wait(&bar[s], par);
+      if(__syncthreads_or(!ok))   // the whole block leaves together
+      {
+        failed = true;
+        break;
+      }
+      const unsigned char* st = tma_smem + size_t(s) * sb;
+      const V* sv = reinterpret_cast<const V*>(st);
+      const void* scol = st + size_t(TMA_NT) * K * sizeof(V);
+      const uint32_t i = c * TMA_NT + threadIdx.x;
+      if(i < A.rows)
+      {
+        // the row's own vector entries are loaded first; they do not depend on the gathers
+        const typename Op::Pre pre = op.pre(i);
+        const auto sum = staged_row_sum<V, S>(sv, narrow ? reinterpret_cast<const int16_t*>(scol) : nullptr,
+          narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), K, threadIdx.x, i, x);
+        part += op(i, sum, pre);
+      }
+      __syncthreads();   // every thread is done with stage s
+      if(threadIdx.x == 0)
+      {
+        const uint32_t c2 = c + uint32_t(TMA_STAGES) * gridDim.x;
+        if(c2 < nch)
+        {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue(c2, s);
+        }
+      }
+    }
+    if(failed)
+    {
+      // record the expiry, then wait (bounded) for this block's copies still in flight; the block
+      // still takes part in the grid reduction below so that its arrival counter completes
+      if(threadIdx.x == 0)
+      {
+        atomicOr(err, 1);
+        for(uint32_t k = 0; k < uint32_t(TMA_STAGES); ++k)
+        {
+          const uint32_t jt = it + k;
+          const uint32_t c = blockIdx.x + jt * gridDim.x;
+          if(c < nch)
+            mbar_wait(&bar[jt % TMA_STAGES], (jt / TMA_STAGES) & 1u);
+        }
+      }
+      __syncthreads();
+    }
+    if(!Op::REDUCES)
+      return;
+    double total;
+    if(grid_sum_last<TMA_NT>(part, slot, sh, total))
+      op.finish(total);
+  }
+} // namespace fb

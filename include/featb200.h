@@ -188,10 +188,13 @@ typedef struct
   int rows_per_block;   /* CSR kernel rows per block, 0 = autotuned */
   int tail_rows;        /* levels (below the finest) with at most this many rows, down to the
                            coarsest, run in one single-block kernel per V-cycle; 0 = off */
+  int tma_rows;         /* uniform-width levels with at least this many rows use the TMA-staged
+                           persistent passes (bulk copies into shared memory); 0 = off */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
- * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks, tail below 4096 rows. */
+ * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks, tail below 4096 rows,
+ * TMA-staged passes from 32768 rows. */
 void fb_solver_config_default(fb_solver_config* cfg);
 
 typedef struct

@@ -147,3 +147,39 @@ def test_device_entry_point_and_launch_count(featlib, cuda):
     assert s.correct_device(sol, rhs) == fb.Status.success
     assert fb.launch_count() - c0 >= s.info.kernel_launches > 0
     assert rel_err(sol.cpu().numpy(), g["sol"]) <= PARITY
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_tma_staged_passes_match(featlib, cuda, name, precision):
+    """The TMA-staged passes (bulk copies of matrix chunks into shared memory) forced onto every
+    uniform-width level give the same results as the per-row kernels: bitwise V-cycles in FP64,
+    identical iterations, solutions within rounding of the dot products."""
+    fb = featlib
+    g = load_golden(name)
+    lv = to_lafem_levels(g["levels"])
+    s_tma, x_tma, st1 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=32, tail_rows=0)
+    s_ref, x_ref, st2 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=0, tail_rows=0)
+    assert st1 == st2 == fb.Status.success
+    assert s_tma.get_num_iter() == s_ref.get_num_iter()
+    z1 = s_tma.apply_precond(fb.DenseVector(g["rhs"])).elements
+    z2 = s_ref.apply_precond(fb.DenseVector(g["rhs"])).elements
+    assert np.array_equal(z1, z2)
+    assert rel_err(x_tma, x_ref) <= (1e-12 if precision == "f64" else 1e-7)
+    if precision == "f64":
+        assert np.array_equal(z1, g["vcycle"])
+        assert rel_err(x_tma, g["sol"]) <= PARITY
+
+
+def test_tma_full_size(featlib, cuda, oracle_lib):
+    """Level 10 with the default thresholds (TMA on the large levels): bitwise V-cycle against the
+    C oracle, solution within 1e-12."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(10, 2, rhs="gauss", gauss=AS.gauss_params(3, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    s, x, st = _solve(fb, levels, b, ordering="native")
+    assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, mg.vcycle(b))
+    assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+    assert rel_err(x, x_ref) <= PARITY
