@@ -1670,6 +1670,33 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def)
   return FB_OK;
 }
 
+} // extern "C"
+
+namespace fb
+{
+  template<typename V, typename S>
+  static void time_one(fb_solver* s, int which, cudaStream_t st)
+  {
+    Launcher<V, S> l{s, st, false};
+    const DevLevel& t = s->lv[0];
+    const DevMat& A64 = s->cfg.precision == FB_PREC_F64 ? t.A : t.A64;
+    if(which == FB_KERNEL_PCG_SPMV)
+    {
+      if(l.use_tma_f64(A64))
+        l.template tma<double, double>(A64, s->p, OpPcgQ{s->p, s->q, t.dm, s->sc});
+      else
+        k_pcg_q<<<blocks(t.n), NT, A64.smem, st>>>(view<double>(A64), s->p, s->q, t.dm, s->slot, s->sc);
+    }
+    else if(l.use_tma(t.A))
+      l.template tma<V, S>(t.A, t.x, OpDefect<V, S>{(const S*)t.b, (S*)t.d, t.dm, s->sc});
+    else
+      k_defect<V, S><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.b, (const S*)t.x, (S*)t.d, t.dm,
+        s->sc);
+  }
+} // namespace fb
+
+extern "C" {
+
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
   double* bytes_per_launch)
 {
@@ -1698,17 +1725,13 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
     if(flush_l2)
       FB_CUDA(cudaMemsetAsync(s->flush, k & 0xff, flush_bytes, st));
     FB_CUDA(cudaEventRecord(s->ev0, st));
-    if(which == FB_KERNEL_PCG_SPMV)
-      k_pcg_q<<<blocks(t.n), NT, A64.smem, st>>>(view<double>(A64), s->p, s->q, t.dm, s->slot, s->sc);
-    else if(s->cfg.precision == FB_PREC_F64)
-      k_defect<double, double><<<blocks(t.n), NT, t.A.smem, st>>>(view<double>(t.A), (const double*)t.b,
-        (const double*)t.x, (double*)t.d, t.dm, s->sc);
+    // the kernel the solve itself launches for this matrix: TMA-staged pass or per-row kernel
+    if(s->cfg.precision == FB_PREC_F64)
+      time_one<double, double>(s, which, st);
     else if(s->cfg.precision == FB_PREC_F32)
-      k_defect<float, float><<<blocks(t.n), NT, t.A.smem, st>>>(view<float>(t.A), (const float*)t.b,
-        (const float*)t.x, (float*)t.d, t.dm, s->sc);
+      time_one<float, float>(s, which, st);
     else
-      k_defect<bf16_t, float><<<blocks(t.n), NT, t.A.smem, st>>>(view<bf16_t>(t.A), (const float*)t.b,
-        (const float*)t.x, (float*)t.d, t.dm, s->sc);
+      time_one<bf16_t, float>(s, which, st);
     FB_LAUNCHED(1);
     FB_CUDA(cudaEventRecord(s->ev1, st));
     FB_CUDA(cudaEventSynchronize(s->ev1));
