@@ -245,6 +245,54 @@ namespace fb
     __device__ void finish(double) const {}
   };
 
+  // restriction: b_c = F_c(R d), sol1_c = F_c(D_c .* b_c) (xc != null), ||b_c|| -> the coarse
+  // level's pre-smoothing skip flag (restrict_row)
+  template<typename V, typename S>
+  struct OpRestrict
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac di; bool d; };
+    static constexpr bool REDUCES = true;
+    S* bc; S* xc; const S* dinvc; const uint8_t* dmc; int* skip; const Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t j) const { return Pre{xc ? Ac(__ldg(dinvc + j)) : Ac(0), __ldg(dmc + j) != 0}; }
+    __device__ double operator()(uint32_t j, Ac sum, const Pre& p) const
+    {
+      const Ac v = p.d ? Ac(0) : add(sum, Ac(0));
+      bc[j] = S(v);
+      if(xc)
+      {
+        const Ac c = p.d ? Ac(0) : mul(p.di, v);
+        xc[j] = S(add(Ac(0), c));
+      }
+      return double(v) * double(v);
+    }
+    __device__ void finish(double total) const
+    {
+      if(xc)
+        *skip = skip_from_norm<S>(sqrt(total));
+    }
+  };
+
+  // prolongation: x += F(P xc) (prolong_row); the pass gathers xc
+  template<typename V, typename S>
+  struct OpProlong
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac x; bool d; };
+    static constexpr bool REDUCES = false;
+    S* x; const uint8_t* dm; const Scalars* sc;
+    __device__ bool closed() const { return gate_closed(sc); }
+    __device__ Pre pre(uint32_t i) const { return Pre{Ac(x[i]), __ldg(dm + i) != 0}; }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      const Ac c = p.d ? Ac(0) : add(sum, Ac(0));
+      x[i] = S(add(p.x, c));
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
   template<typename V, typename S>
   struct OpDefect
   {
@@ -347,21 +395,29 @@ namespace fb
   // ------------------------------------------------------------------ coarse-level tail
   // The bottom of the V-cycle (levels whose row count is at most the tail threshold, down to the
   // coarsest) in ONE block of TAIL_NT threads: block-stride loops separated by __syncthreads
-  // replace one kernel launch per pass.  Vectors are read with coherent loads (they are written
-  // inside this kernel); the row bodies are the grid kernels' own.
+  // replace one kernel launch per pass.  The tail's vectors live in shared memory (levels the host
+  // placed there; the tail's top level is copied in and its solution copied out), and its
+  // matrices, diagonals and masks are bulk-prefetched into L2 when the block starts, so the passes
+  // wait on shared memory and L1/L2 instead of DRAM.  The row bodies are the grid kernels' own.
   constexpr int TAIL_NT = 512;
   constexpr int MAX_TAIL = 12;
+  constexpr int MAX_TAIL_PF = 96;
+  constexpr uint32_t TAIL_PF_CHUNK = 32768;
+  constexpr size_t TAIL_SMEM_MAX = 200 * 1024;
 
   template<typename V, typename S>
   struct TailLevel
   {
     DCsr<V> A, P, R;       // P: this <- next coarser, R: next coarser <- this
-    S *b, *x, *x2, *d, *c, *c2;
+    S *b, *x, *x2, *d, *c, *c2;   // global vectors (used when the level is not in shared memory)
     const S* dinv;
     const uint8_t* dm;
     int* skip_pre;
     int* skip_post;
     uint32_t n;
+    uint32_t soff;         // shared-memory offset of the level's six vectors (elements of S)
+    uint32_t np;           // padded length of one shared vector
+    int in_smem;
   };
 
   template<typename V, typename S>
@@ -373,86 +429,154 @@ namespace fb
     const uint32_t* free_dofs;
     const double* inv;
     uint32_t m;
+    int npf;               // L2 prefetch ranges (16-byte aligned, multiples of 16 bytes)
+    const void* pf_ptr[MAX_TAIL_PF];
+    uint32_t pf_bytes[MAX_TAIL_PF];
   };
+
+  // vector k (0 b, 1 x, 2 x2, 3 d, 4 c, 5 c2) of tail level t
+  template<typename V, typename S>
+  __device__ __forceinline__ S* tail_vec(const TailParams<V, S>& tp, S* sbase, int t, int k)
+  {
+    const TailLevel<V, S>& l = tp.lv[t];
+    if(l.in_smem)
+      return sbase + l.soff + uint32_t(k) * l.np;
+    switch(k)
+    {
+      case 0: return l.b;
+      case 1: return l.x;
+      case 2: return l.x2;
+      case 3: return l.d;
+      case 4: return l.c;
+      default: return l.c2;
+    }
+  }
 
   template<typename V, typename S>
   __global__ void __launch_bounds__(TAIL_NT) k_tail(const __grid_constant__ TailParams<V, S> tp, const Scalars* __restrict__ sc)
   {
     typedef typename ValueTraits<V>::acc Ac;
+    extern __shared__ __align__(16) unsigned char tail_smem[];
     __shared__ double sh[32];
+    __shared__ int skip_pre_sh[MAX_TAIL];
+    __shared__ int skip_post_sh;
     if(gate_closed(sc))
       return;
-    S* xcur[MAX_TAIL];
+    S* sbase = reinterpret_cast<S*>(tail_smem);
+    // matrix data of all tail levels towards L2, asynchronously
+    {
+      // thread j issues chunks j, j + TAIL_NT, ... of the flattened chunk list
+      uint32_t g = 0;
+      for(int r = 0; r < tp.npf; ++r)
+      {
+        const uint32_t nb = tp.pf_bytes[r];
+        for(uint32_t off = 0; off < nb; off += TAIL_PF_CHUNK, ++g)
+          if(g % TAIL_NT == threadIdx.x)
+          {
+            const uint32_t sz = min(TAIL_PF_CHUNK, nb - off);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(static_cast<const unsigned char*>(tp.pf_ptr[r]) + off), "r"(sz) : "memory");
+          }
+      }
+    }
     const int cnt = tp.count;
+    const int steps = tp.steps;
+    // the top level's input: b and sol1 = F(D .* b) written by the restriction above
+    if(tp.lv[0].in_smem)
+    {
+      S* b0 = tail_vec(tp, sbase, 0, 0);
+      S* x0 = tail_vec(tp, sbase, 0, 1);
+      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      {
+        b0[i] = tp.lv[0].b[i];
+        x0[i] = tp.lv[0].x[i];
+      }
+    }
+    if(threadIdx.x == 0)
+      skip_pre_sh[0] = *(volatile int*)tp.lv[0].skip_pre;
+    __syncthreads();
+    int xsel[MAX_TAIL];   // 1 or 2: which x buffer holds level t's iterate after pre-smoothing
     for(int t = 0; t + 1 < cnt; ++t)
     {
       const TailLevel<V, S>& f = tp.lv[t];
       const TailLevel<V, S>& c = tp.lv[t + 1];
-      S* xa = f.x;
-      S* xb = f.x2;
-      for(int k = 1; k < tp.steps; ++k)
+      const S* fb = tail_vec(tp, sbase, t, 0);
+      S* xa = tail_vec(tp, sbase, t, 1);
+      S* xb = tail_vec(tp, sbase, t, 2);
+      int sel = 1;
+      const bool skipped = skip_pre_sh[t] != 0;
+      for(int k = 1; k < steps; ++k)
       {
-        const bool skipped = *(volatile int*)f.skip_pre != 0;
         for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
-          xb[i] = smooth_row<V, S, false>(f.A, f.b, xa, f.dinv, f.dm, skipped, i);
+          xb[i] = smooth_row<V, S, false>(f.A, fb, xa, f.dinv, f.dm, skipped, i);
         __syncthreads();
         S* tmp = xa;
         xa = xb;
         xb = tmp;
+        sel = 3 - sel;
       }
-      xcur[t] = xa;
+      xsel[t] = sel;
+      S* fd = tail_vec(tp, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
-        f.d[i] = defect_row<V, S, false>(f.A, f.b, xa, f.dm, i);
+        fd[i] = defect_row<V, S, false>(f.A, fb, xa, f.dm, i);
       __syncthreads();
       const bool coarsest = (t + 2 == cnt);
+      S* cbv = tail_vec(tp, sbase, t + 1, 0);
+      S* cxv = coarsest ? (S*)nullptr : tail_vec(tp, sbase, t + 1, 1);
       double sq = 0.0;
       for(uint32_t j = threadIdx.x; j < c.n; j += TAIL_NT)
-        sq += restrict_row<V, S, false>(f.R, f.d, c.b, coarsest ? (S*)nullptr : c.x, c.dinv, c.dm, j);
+        sq += restrict_row<V, S, false>(f.R, fd, cbv, cxv, c.dinv, c.dm, j);
       const double tot = block_sum<TAIL_NT>(sq, sh);
       if(threadIdx.x == 0 && !coarsest)
-        *(volatile int*)c.skip_pre = skip_from_norm<S>(sqrt(tot));
+      {
+        const int sk = skip_from_norm<S>(sqrt(tot));
+        skip_pre_sh[t + 1] = sk;
+        *(volatile int*)c.skip_pre = sk;
+      }
       __syncthreads();
     }
     {
       const TailLevel<V, S>& c = tp.lv[cnt - 1];
-      coarse_block<S, TAIL_NT>(c.b, c.x, c.n, tp.free_dofs, tp.inv, tp.m);
-      xcur[cnt - 1] = c.x;
+      coarse_block<S, TAIL_NT>(tail_vec(tp, sbase, cnt - 1, 0), tail_vec(tp, sbase, cnt - 1, 1), c.n, tp.free_dofs,
+        tp.inv, tp.m);
+      xsel[cnt - 1] = 1;
       __syncthreads();
     }
     for(int t = cnt - 2; t >= 0; --t)
     {
       const TailLevel<V, S>& f = tp.lv[t];
-      S* xf = xcur[t];
-      const S* xc = xcur[t + 1];
+      S* xf = tail_vec(tp, sbase, t, xsel[t]);
+      const S* xc = tail_vec(tp, sbase, t + 1, xsel[t + 1]);
+      const S* fb = tail_vec(tp, sbase, t, 0);
+      S* fd = tail_vec(tp, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
       __syncthreads();
+      S* ca = tail_vec(tp, sbase, t, 4);
+      S* cb = tail_vec(tp, sbase, t, 5);
       double sq = 0.0;
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
-        sq += post1_row<V, S, false>(f.A, f.b, xf, f.d, f.c, f.dinv, f.dm, i);
+        sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
       const double tot = block_sum<TAIL_NT>(sq, sh);
-      __shared__ int skipped_sh;
       if(threadIdx.x == 0)
       {
-        skipped_sh = skip_from_norm<S>(sqrt(tot));
-        *(volatile int*)f.skip_post = skipped_sh;
+        skip_post_sh = skip_from_norm<S>(sqrt(tot));
+        *(volatile int*)f.skip_post = skip_post_sh;
       }
       __syncthreads();
-      const bool skipped = skipped_sh != 0;
-      S* ca = f.c;
-      S* cb = f.c2;
-      if(tp.steps == 1)
+      const bool skipped = skip_post_sh != 0;
+      if(steps == 1)
       {
         for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
           xf[i] = S(add(Ac(xf[i]), skipped ? Ac(0) : Ac(ca[i])));
         __syncthreads();
       }
-      for(int k = 2; k <= tp.steps; ++k)
+      for(int k = 2; k <= steps; ++k)
       {
-        const bool last = (k == tp.steps);
+        const bool last = (k == steps);
         for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         {
-          const Ac cn = post2_row<V, S, false>(f.A, f.d, ca, f.dinv, f.dm, skipped, i);
+          const Ac cn = post2_row<V, S, false>(f.A, fd, ca, f.dinv, f.dm, skipped, i);
           if(last)
             xf[i] = S(add(Ac(xf[i]), cn));
           else
@@ -463,6 +587,14 @@ namespace fb
         ca = cb;
         cb = tmp;
       }
+    }
+    // the top level's solution goes to the global buffer the prolongation above reads
+    if(tp.lv[0].in_smem)
+    {
+      const S* xs = tail_vec(tp, sbase, 0, xsel[0]);
+      S* xg = xsel[0] == 1 ? tp.lv[0].x : tp.lv[0].x2;
+      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+        xg[i] = xs[i];
     }
   }
 
@@ -694,6 +826,7 @@ namespace fb
     size_t smem = 0;
     double bytes = 0;                       // matrix bytes one sweep reads
     uint32_t kw = 0;                        // uniform width (ELL), 0 = sliced
+    uint32_t kmax = 0;                      // widest slice's entries per row
   };
 
   template<typename V> DCsr<V> view(const DevMat& m)
@@ -733,6 +866,9 @@ struct fb_solver
   void* flush = nullptr;   // L2 flush buffer of fb_solver_time_kernel (allocated on first use)
   uint32_t* perm0 = nullptr;
   double* hist = nullptr;
+  // fb_solver_update_matrix: per level, the device slot of every caller CSR entry (UINT32_MAX =
+  // not stored) and the caller entry of every device row's diagonal; built on first use
+  std::vector<uint32_t*> upd_slot, upd_diag;
   fb::Scalars* sc = nullptr;
   fb::RedSlot slot{nullptr, nullptr};
   cudaStream_t stream = nullptr;
@@ -797,6 +933,9 @@ namespace fb
     d.nnz = uint32_t(H.nnz);
     d.entries = H.entries;
     d.kw = H.kw;
+    d.kmax = H.kw;
+    for(uint32_t sl = 0; sl < ns; ++sl)
+      d.kmax = std::max(d.kmax, (H.soff[sl + 1] - H.soff[sl]) / 32u);
     const size_t vb = valsize_of(prec);
     const size_t cb = H.narrow ? 2 : 4;
     d.bytes = double(H.entries) * double(vb + cb) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
@@ -857,29 +996,29 @@ namespace fb
 
     bool use_tma_f64(const DevMat& m) const
     {
-      if(s->cfg.tma_rows <= 0 || !m.kw || m.rows < uint32_t(s->cfg.tma_rows))
+      if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kw, m.dcol != nullptr) <= 100u * 1024u;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= 100u * 1024u;
     }
 
-    // the TMA-staged pass serves uniform-width matrices of at least tma_rows rows whose stages fit
+    // the TMA-staged pass serves matrices of at least tma_rows rows whose stages fit
     bool use_tma(const DevMat& m) const
     {
-      if(s->cfg.tma_rows <= 0 || !m.kw || m.rows < uint32_t(s->cfg.tma_rows))
+      if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kw, m.dcol != nullptr) <= 100u * 1024u;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= 100u * 1024u;
     }
     template<typename VV, typename XS, class Op>
     void tma(const DevMat& m, const void* x, const Op& op)
     {
-      const uint32_t sb = tma_stage_bytes<VV>(m.kw, m.dcol != nullptr);
+      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr);
       const size_t smem = size_t(TMA_STAGES) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
       const uint32_t bps = std::max(1u, std::min(8u, uint32_t((200u * 1024u) / (smem + 2048u))));
       const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
-      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, op, s->slot,
-                                                        s->err);
+      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax, op,
+                                                        s->slot, s->err);
     }
     uint64_t launches = 0;
     double bytes = 0;
@@ -891,6 +1030,60 @@ namespace fb
     double csr_bytes(const DevMat& m, double vec_in, double vec_out)
     {
       return m.bytes + double(m.cols) * sizeof(S) + double(m.rows) * sizeof(S) * (vec_in + vec_out);
+    }
+
+    // Shared-memory placement of the tail's vectors (coarsest level first, while the levels fit)
+    // and the L2 prefetch list of its matrices, diagonals and masks; returns the dynamic shared
+    // memory size.
+    size_t tail_layout(TailParams<V, S>& tp, int lt)
+    {
+      const int nl = s->nlev;
+      uint32_t used = 0;
+      for(int l = nl - 1; l >= lt; --l)
+      {
+        TailLevel<V, S>& t = tp.lv[l - lt];
+        const uint32_t np = (t.n + 7u) & ~7u;
+        if(size_t(used) + 6ull * np * sizeof(S) > TAIL_SMEM_MAX)
+          break;
+        t.in_smem = 1;
+        t.soff = used / uint32_t(sizeof(S));
+        t.np = np;
+        used += 6u * np * uint32_t(sizeof(S));
+      }
+      auto pf = [&](const void* p, uint64_t nb)
+      {
+        if(!p || tp.npf >= MAX_TAIL_PF)
+          return;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+        const uintptr_t a16 = (a + 15) & ~uintptr_t(15);
+        if(nb < (a16 - a) + 16)
+          return;
+        nb = (nb - (a16 - a)) & ~uint64_t(15);
+        tp.pf_ptr[tp.npf] = reinterpret_cast<const void*>(a16);
+        tp.pf_bytes[tp.npf] = uint32_t(std::min<uint64_t>(nb, 0xfffffff0ull));
+        ++tp.npf;
+      };
+      auto add_mat = [&](const DevMat& m)
+      {
+        pf(m.val, m.entries * sizeof(V));
+        pf(m.dcol, m.entries * sizeof(int16_t));
+        pf(m.col, m.entries * sizeof(uint32_t));
+        if(!m.kw && m.soff)
+          pf(m.soff, (uint64_t((m.rows + 31) / 32) + 1) * sizeof(uint32_t));
+      };
+      for(int l = nl - 1; l >= lt; --l)
+      {
+        const DevLevel& f = L(l);
+        add_mat(f.A);
+        if(l + 1 < nl)
+        {
+          add_mat(f.R);
+          add_mat(f.P);
+        }
+        pf(f.dinv, uint64_t(f.n) * sizeof(S));
+        pf(f.dm, f.n);
+      }
+      return used;
     }
 
     // V-cycle from the top level; the top level's b and sol1 and skip_pre are in place.
@@ -932,8 +1125,14 @@ namespace fb
         ++launches;
         bytes += csr_bytes(f.A, 1, 1) + f.n;
         const bool coarsest = (l + 2 == nl);
-        if(!dry) k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
-          coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
+        if(dry)
+          ;
+        else if(use_tma(f.R))
+          tma<V, S>(f.R, f.d, OpRestrict<V, S>{(S*)c.b, coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm,
+            c.skip_pre, s->sc});
+        else
+          k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
+            coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
         ++launches;
         bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
       }
@@ -971,8 +1170,9 @@ namespace fb
           if(l + 1 < nl)
             bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
         }
+        const size_t smem = tail_layout(tp, lt);
         bytes += double(s->nfree) * s->nfree * 8.0;
-        if(!dry) k_tail<V, S><<<1, TAIL_NT, 0, st>>>(tp, s->sc);
+        if(!dry) k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
         ++launches;
       }
       else
@@ -989,7 +1189,13 @@ namespace fb
           continue;
         DevLevel& f = L(l);
         void* xf = xcur[size_t(l)];
-        if(!dry) k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
+        if(dry)
+          ;
+        else if(use_tma(f.P))
+          tma<V, S>(f.P, xcur[size_t(l + 1)], OpProlong<V, S>{(S*)xf, f.dm, s->sc});
+        else
+          k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm,
+            s->sc);
         ++launches;
         bytes += csr_bytes(f.P, 1, 1) + f.n;
         if(dry)
@@ -1107,7 +1313,10 @@ namespace fb
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, false, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpRestrict<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpProlong<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tail<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     return FB_OK;
   }
 
@@ -1674,6 +1883,20 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def)
 
 namespace fb
 {
+  // reads n16 16-byte words (L2 fills with clean lines); the sink is written only on a value the
+  // data never has, so the loads stay
+  __global__ void k_read_sweep(const uint4* __restrict__ p, size_t n16, unsigned int* sink)
+  {
+    uint32_t acc = 0;
+    for(size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n16; i += size_t(gridDim.x) * blockDim.x)
+    {
+      const uint4 v = p[i];
+      acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if(acc == 0x9e3779b9u)
+      atomicAdd(sink, 1u);
+  }
+
   template<typename V, typename S>
   static void time_one(fb_solver* s, int which, cudaStream_t st)
   {
@@ -1708,9 +1931,15 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   cudaStream_t st = s->stream;
   const DevLevel& t = s->lv[0];
   const bool f64 = s->cfg.precision == FB_PREC_F64;
+  // flush: overwrite one 256 MiB half, then read the other (zeroed once) so that the L2 holds clean
+  // lines of neither the matrix nor the vectors when the timed launch starts (a write-only flush
+  // would leave dirty lines whose write-back lands inside the timed interval)
   const size_t flush_bytes = size_t(256) << 20;
   if(flush_l2 && !s->flush)
-    FB_TRY(dalloc(s, &s->flush, flush_bytes));
+  {
+    FB_TRY(dalloc(s, &s->flush, 2 * flush_bytes + 256));
+    FB_CUDA(cudaMemsetAsync(s->flush, 0, 2 * flush_bytes + 256, st));
+  }
   const DevMat& A64 = f64 ? t.A : t.A64;
   const double sv = double(vsize_of(s->cfg.precision));
   if(which == FB_KERNEL_PCG_SPMV)
@@ -1723,7 +1952,13 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   for(int k = 0; k < reps; ++k)
   {
     if(flush_l2)
-      FB_CUDA(cudaMemsetAsync(s->flush, k & 0xff, flush_bytes, st));
+    {
+      unsigned char* f = static_cast<unsigned char*>(s->flush);
+      FB_CUDA(cudaMemsetAsync(f, (k + 1) & 0xff, flush_bytes, st));
+      k_read_sweep<<<s->nsm * 4, 512, 0, st>>>(reinterpret_cast<const uint4*>(f + flush_bytes), flush_bytes / 16,
+        reinterpret_cast<unsigned int*>(f + 2 * flush_bytes));
+      FB_LAUNCHED(1);
+    }
     FB_CUDA(cudaEventRecord(s->ev0, st));
     // the kernel the solve itself launches for this matrix: TMA-staged pass or per-row kernel
     if(s->cfg.precision == FB_PREC_F64)
@@ -1759,6 +1994,150 @@ fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out)
     out[3 * l + 1] = s->lv[size_t(l)].A.nnz;
     out[3 * l + 2] = s->lv[size_t(l)].P.nnz;
   }
+  return FB_OK;
+}
+
+} // extern "C"
+
+namespace fb
+{
+  template<typename V> __device__ __forceinline__ V from_f64(double v);
+  template<> __device__ __forceinline__ double from_f64<double>(double v) { return v; }
+  template<> __device__ __forceinline__ float from_f64<float>(double v) { return __double2float_rn(v); }
+  template<> __device__ __forceinline__ bf16_t from_f64<bf16_t>(double v)
+  {
+    // FP64 -> FP32 (nearest) -> BF16 (nearest even), as the host upload rounds
+    const float f = __double2float_rn(v);
+    uint32_t u = __float_as_uint(f);
+    bf16_t b;
+    if((u & 0x7f800000u) == 0x7f800000u)
+      b.bits = uint16_t(u >> 16) | ((u & 0xffffu) ? 0x40u : 0u);
+    else
+      b.bits = uint16_t((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+    return b;
+  }
+
+  template<typename V>
+  __global__ void k_scatter_values(const double* __restrict__ vals, const uint32_t* __restrict__ slot, uint64_t nnz,
+    V* __restrict__ dst)
+  {
+    const uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(j >= nnz)
+      return;
+    const uint32_t e = slot[j];
+    if(e != 0xffffffffu)
+      dst[e] = from_f64<V>(vals[j]);
+  }
+
+  // inv_diag = omega / a_ii in FP64, stored in the V-cycle's precision (inv_diagonal + upload_vec)
+  template<typename S>
+  __global__ void k_update_dinv(const double* __restrict__ vals, const uint32_t* __restrict__ diag, uint32_t n,
+    double omega, S* __restrict__ dinv)
+  {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if(k >= n)
+      return;
+    const uint32_t j = diag[k];
+    const double a = j == 0xffffffffu ? 0.0 : vals[j];
+    dinv[k] = S(omega / a);
+  }
+
+  // slot and diagonal maps of level l (see fb_solver::upd_slot)
+  static fb_status build_update_maps(fb_solver* s, int l)
+  {
+    const HostLevel& H = s->h->levels[size_t(l)];
+    const std::vector<uint32_t>& pf = s->perms[size_t(l)];
+    const std::vector<uint32_t> inv = pf.empty() ? std::vector<uint32_t>() : inverse_perm(pf);
+    const HostCsr& A = H.A;
+    std::vector<uint8_t> dm(A.rows);
+    for(uint32_t k = 0; k < A.rows; ++k)
+      dm[k] = H.dmask[pf.empty() ? k : pf[k]];
+    const HostSell S = build_sell(permute(A, pf, inv), &dm);
+    std::vector<uint32_t> slot(std::max<size_t>(1, A.col.size()), 0xffffffffu);
+    std::vector<uint32_t> diag(std::max<uint32_t>(1, A.rows), 0xffffffffu);
+    for(uint32_t r = 0; r < A.rows; ++r)
+    {
+      const uint32_t k = inv.empty() ? r : inv[r];
+      for(uint32_t j = A.rp[r]; j < A.rp[r + 1]; ++j)
+      {
+        if(A.col[j] == r && diag[k] == 0xffffffffu)
+          diag[k] = j;
+        if(!dm[k])
+          slot[j] = S.soff[k / 32u] + (j - A.rp[r]) * 32u + (k % 32u);
+      }
+    }
+    uint32_t* ds = nullptr;
+    uint32_t* dd = nullptr;
+    FB_TRY(dalloc(s, (void**)&ds, sizeof(uint32_t) * slot.size()));
+    FB_TRY(dalloc(s, (void**)&dd, sizeof(uint32_t) * diag.size()));
+    FB_CUDA(cudaMemcpy(ds, slot.data(), sizeof(uint32_t) * slot.size(), cudaMemcpyHostToDevice));
+    FB_CUDA(cudaMemcpy(dd, diag.data(), sizeof(uint32_t) * diag.size(), cudaMemcpyHostToDevice));
+    s->upd_slot[size_t(l)] = ds;
+    s->upd_diag[size_t(l)] = dd;
+    return FB_OK;
+  }
+
+  template<typename V, typename S>
+  static fb_status update_level(fb_solver* s, int l, const double* vals, cudaStream_t st)
+  {
+    DevLevel& D = s->lv[size_t(l)];
+    const uint64_t nnz = s->h->levels[size_t(l)].A.col.size();
+    const uint32_t* slot = s->upd_slot[size_t(l)];
+    if(nnz)
+    {
+      const unsigned g = unsigned((nnz + 255) / 256);
+      k_scatter_values<V><<<g, 256, 0, st>>>(vals, slot, nnz, static_cast<V*>(D.A.val));
+      if(D.A64.val)
+        k_scatter_values<double><<<g, 256, 0, st>>>(vals, slot, nnz, static_cast<double*>(D.A64.val));
+    }
+    k_update_dinv<S><<<(D.n + 255) / 256, 256, 0, st>>>(vals, s->upd_diag[size_t(l)], D.n, s->cfg.omega,
+      static_cast<S*>(D.dinv));
+    FB_LAUNCHED(nnz ? (D.A64.val ? 3 : 2) : 1);
+    return FB_OK;
+  }
+} // namespace fb
+
+extern "C" {
+
+fb_status fb_solver_update_matrix(fb_solver* s, int level, const double* values, void* stream)
+{
+  if(!s || level < 0 || level >= s->nlev || (!values && !s->h->levels[size_t(level)].A.col.empty()))
+  {
+    set_error("solver_update_matrix: bad arguments");
+    return FB_ERR_ARG;
+  }
+  if(s->upd_slot.empty())
+  {
+    s->upd_slot.assign(size_t(s->nlev), nullptr);
+    s->upd_diag.assign(size_t(s->nlev), nullptr);
+  }
+  if(!s->upd_slot[size_t(level)])
+    FB_TRY(build_update_maps(s, level));
+  cudaStream_t st = as_stream(stream);
+  fb_status e;
+  if(s->cfg.precision == FB_PREC_F64)
+    e = update_level<double, double>(s, level, values, st);
+  else if(s->cfg.precision == FB_PREC_F32)
+    e = update_level<float, float>(s, level, values, st);
+  else
+    e = update_level<bf16_t, float>(s, level, values, st);
+  if(e != FB_OK)
+    return e;
+  if(level == s->nlev - 1)
+  {
+    // the exact coarse inverse from the new values (host Gauss-Jordan, as at creation)
+    HostCsr A = s->h->levels[size_t(level)].A;
+    if(!A.val.empty())
+      FB_CUDA(cudaMemcpyAsync(A.val.data(), values, sizeof(double) * A.val.size(), cudaMemcpyDeviceToHost, st));
+    FB_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint32_t> fr;
+    std::vector<double> inv;
+    coarse_inverse(A, s->h->levels[size_t(level)].dmask, fr, inv);
+    if(!inv.empty())
+      FB_CUDA(cudaMemcpy(s->cinv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice));
+  }
+  else
+    FB_CUDA(cudaStreamSynchronize(st));
   return FB_OK;
 }
 

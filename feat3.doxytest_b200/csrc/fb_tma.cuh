@@ -1,7 +1,8 @@
-// TMA-staged row passes for uniform-width (ELL) matrices.
+// TMA-staged row passes over sliced-ELL / ELL matrices.
 //
-// A persistent block walks over chunks of CR consecutive rows.  The chunk's values and column
-// offsets (contiguous in ELL storage) are copied into shared memory by the bulk-copy engine
+// A persistent block walks over chunks of TMA_NT consecutive rows (TMA_NT/32 slices).  The chunk's
+// values and column indices (contiguous in both layouts) are copied into shared memory by the
+// bulk-copy engine
 // (cp.async.bulk ... mbarrier::complete_tx), NSTAGE chunks ahead of the threads, so the matrix
 // stream occupies no registers and stays in flight while the threads gather x from L1/L2 and
 // apply the pass's row epilogue.  Every mbarrier wait is bounded: on expiry the kernel records the
@@ -54,15 +55,14 @@ namespace fb
     return false;
   }
 
-  // row sum of local row `lr` (0..CR-1) of the staged chunk: entry k of row 32*ls+lane at
-  // ls*32*K + 32*k + lane, in stored order; the column is absolute or row-relative
+  // row sum of a staged row with K entries, entry k at base + 32*k, in stored order; the column
+  // is absolute or row-relative
   template<typename V, typename S>
   __device__ __forceinline__ typename ValueTraits<V>::acc staged_row_sum(const V* sv, const int16_t* sd,
-    const uint32_t* sc, uint32_t K, uint32_t lr, uint32_t row, const S* __restrict__ x)
+    const uint32_t* sc, uint32_t K, uint32_t base, uint32_t row, const S* __restrict__ x)
   {
     typedef typename ValueTraits<V>::acc A;
     constexpr uint32_t U = 9;
-    const uint32_t base = (lr >> 5) * 32u * K + (lr & 31u);
     A sum = A(0);
     for(uint32_t k0 = 0; k0 < K; k0 += U)
     {
@@ -83,7 +83,7 @@ namespace fb
     return sum;
   }
 
-  // Shared memory bytes of one stage for a matrix of width K.
+  // Shared memory bytes of one stage for a matrix of (maximum) width K.
   template<typename V>
   __host__ __device__ __forceinline__ uint32_t tma_stage_bytes(uint32_t K, bool narrow)
   {
@@ -92,34 +92,48 @@ namespace fb
 
   // Generic persistent pass: for every row i < A.rows, op(i, sum_i, op.pre(i)) with
   // sum_i = (A x)_i; op returns the row's contribution to an optional grid reduction, finished by
-  // op.finish(total) in thread 0 of the last block.  padded_rows = the ELL storage rows (a
-  // multiple of 32).
+  // op.finish(total) in thread 0 of the last block.  padded_rows = the storage rows (a multiple of
+  // 32); kst = the widest slice's entries per row (= A.kw for ELL), which sizes the stages.
   template<typename V, typename S, class Op>
   __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
-    Op op, RedSlot slot, int* err)
+    uint32_t kst, Op op, RedSlot slot, int* err)
   {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
     __shared__ double sh[32];
     if(op.closed())
       return;
+    constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
-    const uint32_t sb = tma_stage_bytes<V>(K, narrow);
+    const uint32_t sb = tma_stage_bytes<V>(kst, narrow);
+    const uint32_t nsl = padded_rows / 32u;
     const uint32_t nch = (padded_rows + TMA_NT - 1) / TMA_NT;
     auto issue = [&](uint32_t c, int s)
     {
-      const uint32_t r0 = c * TMA_NT;
-      const uint32_t rows = min(uint32_t(TMA_NT), padded_rows - r0);
-      const uint32_t vb = rows * K * uint32_t(sizeof(V));
-      const uint32_t cb = rows * K * (narrow ? 2u : 4u);
+      uint32_t e0, ne;
+      if(K)
+      {
+        const uint32_t r0 = c * TMA_NT;
+        e0 = r0 * K;
+        ne = min(uint32_t(TMA_NT), padded_rows - r0) * K;
+      }
+      else
+      {
+        e0 = __ldg(A.soff + c * SPC);
+        ne = __ldg(A.soff + min(c * SPC + SPC, nsl)) - e0;
+      }
+      const uint32_t vb = ne * uint32_t(sizeof(V));
+      const uint32_t cb = ne * (narrow ? 2u : 4u);
       unsigned char* st = tma_smem + size_t(s) * sb;
       mbar_expect_tx(&bar[s], vb + cb);
-      bulk_g2s(st, A.val + size_t(r0) * K, vb, &bar[s]);
+      if(ne == 0)
+        return;   // every row of the chunk is empty: the arrival alone completes the phase
+      bulk_g2s(st, A.val + e0, vb, &bar[s]);
       if(narrow)
-        bulk_g2s(st + size_t(TMA_NT) * K * sizeof(V), A.dcol + size_t(r0) * K, cb, &bar[s]);
+        bulk_g2s(st + size_t(TMA_NT) * kst * sizeof(V), A.dcol + e0, cb, &bar[s]);
       else
-        bulk_g2s(st + size_t(TMA_NT) * K * sizeof(V), A.col + size_t(r0) * K, cb, &bar[s]);
+        bulk_g2s(st + size_t(TMA_NT) * kst * sizeof(V), A.col + e0, cb, &bar[s]);
     };
     if(threadIdx.x == 0)
     {
@@ -150,14 +164,27 @@ namespace fb
       }
       const unsigned char* st = tma_smem + size_t(s) * sb;
       const V* sv = reinterpret_cast<const V*>(st);
-      const void* scol = st + size_t(TMA_NT) * K * sizeof(V);
+      const void* scol = st + size_t(TMA_NT) * kst * sizeof(V);
       const uint32_t i = c * TMA_NT + threadIdx.x;
       if(i < A.rows)
       {
         // the row's own vector entries are loaded first; they do not depend on the gathers
         const typename Op::Pre pre = op.pre(i);
+        uint32_t kr, base;
+        if(K)
+        {
+          kr = K;
+          base = (threadIdx.x >> 5) * 32u * K + (threadIdx.x & 31u);
+        }
+        else
+        {
+          const uint32_t sl = i >> 5;
+          const uint32_t o = __ldg(A.soff + sl);
+          kr = (__ldg(A.soff + sl + 1) - o) >> 5;
+          base = o - __ldg(A.soff + c * SPC) + (threadIdx.x & 31u);
+        }
         const auto sum = staged_row_sum<V, S>(sv, narrow ? reinterpret_cast<const int16_t*>(scol) : nullptr,
-          narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), K, threadIdx.x, i, x);
+          narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), kr, base, i, x);
         part += op(i, sum, pre);
       }
       __syncthreads();   // every thread is done with stage s

@@ -86,6 +86,19 @@ _PROTOS = {
     "fb_solver_solve_device": (I, [P, P, P, P, C.POINTER(SolveInfo)]),
     "fb_solver_vcycle": (I, [P, P, P]),
     "fb_solver_level_info": (I, [P, P]),
+    "fb_solver_update_matrix": (I, [P, I, P, P]),
+    "fb_q1_pattern_2d": (I, [I, P, P, P]),
+    "fb_q1_assemble_2d": (I, [I, I, P, P, D, I, P, P, P, P, P]),
+    "fb_unet_create": (I, [C.POINTER(P), I, I]),
+    "fb_unet_destroy": (None, [P]),
+    "fb_unet_num_params": (I, [P, C.POINTER(C.c_uint64)]),
+    "fb_unet_set_params": (I, [P, P]),
+    "fb_unet_get_params": (I, [P, P]),
+    "fb_unet_get_grads": (I, [P, P]),
+    "fb_unet_forward": (I, [P, P, P, I, P]),
+    "fb_unet_backward": (I, [P, P, I, I, P]),
+    "fb_unet_adam": (I, [P, C.c_float, C.c_float, C.c_float, C.c_float, I, P]),
+    "fb_unet_mse": (I, [P, P, P, C.c_uint64, P, P, P]),
     "fb_solver_time_kernel": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
     "fb_msolver_create": (I, [C.POINTER(P), P, C.POINTER(SolverConfig), I]),
     "fb_msolver_destroy": (None, [P]),

@@ -254,6 +254,18 @@ class PCG:
                    "fb_solver_solve_device")
         return Status(self.info.status)
 
+    def update_matrix(self, level, values, stream=None):
+        """New values for the system matrix of `level` (0 = finest) in the pattern and entry order
+        it was pushed with: a CUDA float64 tensor of nnz entries.  Refreshes the level's Jacobi
+        diagonal and, on the coarsest level, the exact coarse inverse -- what the reference's
+        init_numeric() does after the matrix values changed (kernel/solver/multigrid.hpp:776-790,
+        kernel/solver/jacobi_precond.hpp:136-165)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream()
+        _lib.check(_lib.lib().fb_solver_update_matrix(self._s, int(level), C.c_void_p(values.data_ptr()),
+                                                      C.c_void_p(stream.cuda_stream)), "fb_solver_update_matrix")
+
     def apply_precond(self, vec_def: DenseVector):
         """One V-cycle: MultiGrid::apply (kernel/solver/multigrid.hpp:1270)."""
         out = DenseVector(vec_def.size())

@@ -233,8 +233,9 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
 #define FB_KERNEL_MG_DEFECT 1  /* d = F(b - A x), finest level, in the V-cycle's precision */
 
 /* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
- * on that stream; with flush_l2 != 0 a 256 MiB buffer is overwritten before each launch (outside
- * the timed interval) so every launch starts with a cold L2.  Returns the mean launch time and the
+ * on that stream; with flush_l2 != 0 a 256 MiB buffer is overwritten and another 256 MiB buffer read
+ * before each launch (outside the timed interval), so every launch starts with an L2 that holds
+ * none of its data and no dirty lines.  Returns the mean launch time and the
  * kernel's algorithmic bytes per launch (matrix values + indices + row pointers + vector reads and
  * writes).  No counterpart in the reference: a measurement aid for the SpMV roofline. */
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
@@ -243,6 +244,17 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
 /* Per-level sizes after upload: rows, nnz of A, nnz of P (as stored on the device, explicit zeros
  * removed).  `out` holds 3 * num_levels entries. */
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
+
+/* New values for the system matrix of `level` (0 = finest): `values` is a DEVICE array of the
+ * level's used_elements doubles in the pattern and entry order passed to fb_hierarchy_set_level
+ * (the pattern must not change).  Rewrites the stored values (and the FP64 copy of the finest level
+ * in FB_PREC_F32* modes), recomputes the level's Jacobi inverse diagonal omega / a_ii on the device
+ * and, for the coarsest level, the exact coarse inverse on the host.  Ordered on `stream`; returns
+ * after it completed.  Counterpart of re-running init_numeric() of the hierarchy after the
+ * matrices' values changed (kernel/solver/multigrid.hpp:776-790, JacobiPrecond::init_numeric
+ * kernel/solver/jacobi_precond.hpp:136-165).  The host copies in the fb_hierarchy keep the old
+ * values. */
+fb_status fb_solver_update_matrix(fb_solver* s, int level, const double* values, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* 3. Solver level, many right-hand sides: K = 32 or 64 systems with one hierarchy              */
@@ -284,6 +296,63 @@ fb_status fb_batch_sizes(const fb_batch* b, uint64_t* top_rows);
 fb_status fb_batch_solve(fb_batch* b, double* sol, const double* rhs, fb_solve_info* info);
 /* As fb_batch_solve with DEVICE packed arrays, ordered on `stream`. */
 fb_status fb_batch_solve_device(fb_batch* b, double* sol, const double* rhs, void* stream, fb_solve_info* info);
+
+/* ------------------------------------------------------------------------------------------ */
+/* 5. Set-up on the device: Q1 assembly on the uniformly refined unit square                    */
+/* ------------------------------------------------------------------------------------------ */
+
+/* The step before the solve path.  Vertices of level L are numbered lexicographically (x fastest),
+ * (2^L+1)^2 of them; the reference assembles the same operators on the host
+ * (assemble_bilinear_operator_matrix_1 with a LaplaceOperator / kappa-weighted operator,
+ * kernel/assembly/domain_assembler_helpers.hpp, common_operators.hpp:36, the load vector
+ * int f phi_i of common_functionals.hpp:33; cubature "auto-degree:5" = 3x3 Gauss). */
+
+/* The row-sorted 9-point CSR pattern of level L (HOST arrays; row_ptr (2^L+1)^2+1 entries, col_ind
+ * nnz entries).  Pass NULL arrays to query nnz first.  0 <= level <= 13. */
+fb_status fb_q1_pattern_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind);
+
+/* Stiffness values of -div(kappa grad u) in that pattern and/or the load vector (Dirichlet
+ * boundary entries set to 0), DEVICE arrays, ordered on `stream`, synchronous on return.
+ * kappa = exp(g), g(x,y) = s sum_{i,j<K} (xi[i*K+j] cos t + eta[i*K+j] sin t) / (kx_i^2 + ky_j^2),
+ * t = 2 pi (kx_i x + ky_j y), kx_i = i - K/2, ky_j = j - K/2, the (0,0) mode left out; kmodes = 0
+ * gives kappa = 1 (xi, eta unused).  f = sum_g a_g exp(-|x - c_g|^2 / (2 w_g^2)) with
+ * gauss[4g..4g+3] = (c_x, c_y, w, a) (DEVICE array).  row_ptr: DEVICE copy of the pattern's row
+ * pointer (needed with values).  values or rhs may be NULL. */
+fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
+                            const double* gauss, const uint64_t* row_ptr, double* values, double* rhs,
+                            void* stream);
+
+/* ------------------------------------------------------------------------------------------ */
+/* 6. Learned warm start: a convolutional U-Net on vertex grids (no counterpart in the reference) */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Maps (f, log kappa) sampled on a G x G vertex grid (G = 2^k + 1, k >= 3) to an approximation of
+ * u on the same grid; the solve path prolongates it to the finest level as the PCG initial guess.
+ * 8 convolutions (channels 16/32/64/64, 3x3, zero padding): three injection subsamplings on the way
+ * down, bilinear vertex upsampling + concatenation with the encoder activations on the way up, ReLU
+ * everywhere but the last layer.  BF16 activations and GEMM operands, FP32 accumulation (tensor
+ * cores), FP32 master parameters with Adam.  Parameter order: per layer W[co][tap][ci]
+ * (tap = (dy+1)*3 + dx+1, dy along the slow grid axis), then b[co]. */
+typedef struct fb_unet fb_unet;
+
+fb_status fb_unet_create(fb_unet** out, int grid, int max_batch);
+void fb_unet_destroy(fb_unet* u);
+fb_status fb_unet_num_params(const fb_unet* u, uint64_t* n);
+/* HOST arrays of num_params floats; set_params also resets the Adam moments */
+fb_status fb_unet_set_params(fb_unet* u, const float* params);
+fb_status fb_unet_get_params(const fb_unet* u, float* params);
+fb_status fb_unet_get_grads(const fb_unet* u, float* grads);
+/* in: DEVICE [batch][2][G][G] FP32 (channel 0 = f, 1 = log kappa, caller-scaled);
+ * out: DEVICE [batch][G][G] FP32.  Keeps the activations for fb_unet_backward. */
+fb_status fb_unet_forward(fb_unet* u, const float* in, float* out, int batch, void* stream);
+/* dout: DEVICE [batch][G][G] FP32 = d loss / d out of the last forward (same batch); writes (or,
+ * with accumulate != 0, adds) the parameter gradients. */
+fb_status fb_unet_backward(fb_unet* u, const float* dout, int batch, int accumulate, void* stream);
+/* One Adam step (t = 1, 2, ...) with the stored gradients. */
+fb_status fb_unet_adam(fb_unet* u, float lr, float beta1, float beta2, float eps, int t, void* stream);
+/* loss (DEVICE double) = mean (y - t)^2 over n entries; grad (DEVICE, or NULL) = 2 (y - t) / n */
+fb_status fb_unet_mse(fb_unet* u, const float* y, const float* t, uint64_t n, float* grad, double* loss,
+                      void* stream);
 
 #ifdef __cplusplus
 }
