@@ -20,7 +20,7 @@ LIB = os.path.join(OUT_DIR, "libfeatb200.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["fb_arch.cu", "fb_mg.cu", "fb_mrhs.cu", "fb_noalloc.cu", "fb_batch.cu", "fb_unet.cu"]
+CU_SOURCES = ["fb_arch.cu", "fb_mg.cu", "fb_mrhs.cu", "fb_noalloc.cu", "fb_batch.cu", "fb_assemble.cu", "fb_unet.cu"]
 CPP_SOURCES = ["fb_setup.cpp"]
 
 

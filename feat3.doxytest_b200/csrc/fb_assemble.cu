@@ -1,0 +1,249 @@
+// Q1 assembly on the uniformly refined unit square, on the device: the set-up step before the
+// solve path (the reference assembles on the host: kernel/assembly/domain_assembler_helpers.hpp,
+// kernel/assembly/common_operators.hpp:36, common_functionals.hpp:33, with the 3x3 Gauss rule that
+// "auto-degree:5" selects).  Vertices are numbered lexicographically ((2^L+1)^2 of them); the
+// stiffness values are written in the row-sorted 9-point CSR pattern of fb_q1_pattern_2d.
+//
+// kappa = exp(g), g(x, y) = s * sum_{i,j} (xi_ij cos t + eta_ij sin t) / (kx_i^2 + ky_j^2),
+// t = 2 pi (kx_i x + ky_j y), kx = ky = -K/2 .. K/2-1 (the (0,0) mode excluded); f = sum of
+// Gaussians a * exp(-|x - c|^2 / (2 w^2)).  Pass 1 computes every cell's 4x4 element matrix and
+// 4 load contributions (one thread per cell); pass 2 sums them per matrix entry / vertex (one
+// thread per vertex, cells in ascending index order), so no atomics are needed and the result is
+// deterministic.
+#include "fb_common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace fb
+{
+namespace as
+{
+  struct Ref
+  {
+    double xq[3], wq[3];
+    double val[9][4];       // phi_v at quad point q
+    double gg[9][4][4];     // grad phi_u . grad phi_v at q (reference element)
+  };
+  __constant__ Ref c_ref;
+
+  // g at (x, y) by the separable sum: h_i = sum_j c_ij e^{2 pi i ky_j y}, g = s sum_i Re(h_i e^{2 pi i kx_i x})
+  __device__ double field(double x, double y, int K, const double* __restrict__ xi, const double* __restrict__ eta,
+    double s)
+  {
+    const double tp = 6.283185307179586476925286766559;
+    double acc = 0.0;
+    for(int i = 0; i < K; ++i)
+    {
+      const double kx = double(i - K / 2);
+      double hr = 0.0, hi = 0.0;
+      for(int j = 0; j < K; ++j)
+      {
+        const double ky = double(j - K / 2);
+        const double den = kx * kx + ky * ky;
+        if(den == 0.0)
+          continue;
+        double sy, cy;
+        sincos(tp * ky * y, &sy, &cy);
+        const double a = __ldg(xi + i * K + j) / den, b = __ldg(eta + i * K + j) / den;
+        hr += a * cy + b * sy;
+        hi += a * sy - b * cy;
+      }
+      double sx, cx;
+      sincos(tp * kx * x, &sx, &cx);
+      acc += hr * cx - hi * sx;
+    }
+    return s * acc;
+  }
+
+  // per cell: the 4x4 element matrix (kappa-weighted) and the 4 load-vector contributions
+  __global__ void k_cells(int N, double h, int K, const double* __restrict__ xi, const double* __restrict__ eta,
+    double s, int ng, const double* __restrict__ gauss, double* __restrict__ ke, double* __restrict__ fe)
+  {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= N * N)
+      return;
+    const int cx = c % N, cy = c / N;
+    double kq[9], fq[9];
+    for(int qy = 0; qy < 3; ++qy)
+      for(int qx = 0; qx < 3; ++qx)
+      {
+        const int q = qx * 3 + qy;   // reference order: x index slowest (meshgrid "ij" over (x, y))
+        const double x = (double(cx) + (1.0 + c_ref.xq[qx]) / 2.0) * h;
+        const double y = (double(cy) + (1.0 + c_ref.xq[qy]) / 2.0) * h;
+        kq[q] = (K > 0 && ke) ? exp(field(x, y, K, xi, eta, s)) : 1.0;
+        double f = 0.0;
+        for(int g = 0; g < ng && fe; ++g)
+        {
+          const double dx = x - gauss[4 * g + 0], dy = y - gauss[4 * g + 1], w = gauss[4 * g + 2];
+          f += gauss[4 * g + 3] * exp(-(dx * dx + dy * dy) / (2.0 * w * w));
+        }
+        fq[q] = f;
+      }
+    if(ke)
+      for(int a = 0; a < 4; ++a)
+        for(int b = 0; b < 4; ++b)
+        {
+          double v = 0.0;
+          for(int q = 0; q < 9; ++q)
+            v += kq[q] * (c_ref.wq[q / 3] * c_ref.wq[q % 3]) * c_ref.gg[q][a][b];
+          ke[size_t(c) * 16 + a * 4 + b] = v;
+        }
+    if(fe)
+      for(int a = 0; a < 4; ++a)
+      {
+        double v = 0.0;
+        for(int q = 0; q < 9; ++q)
+          v += fq[q] * (c_ref.wq[q / 3] * c_ref.wq[q % 3]) * c_ref.val[q][a];
+        fe[size_t(c) * 4 + a] = (h / 2.0) * (h / 2.0) * v;
+      }
+  }
+
+  // per vertex: stiffness row (sorted neighbours) and load entry, summing cells in ascending order
+  __global__ void k_vertices(int N, const double* __restrict__ ke, const double* __restrict__ fe,
+    const uint64_t* __restrict__ rp, double* __restrict__ vals, double* __restrict__ rhs)
+  {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n1 = N + 1;
+    if(v >= n1 * n1)
+      return;
+    const int ix = v % n1, iy = v / n1;
+    if(vals)
+    {
+      uint64_t pos = rp[v];
+      for(int dy = -1; dy <= 1; ++dy)
+        for(int dx = -1; dx <= 1; ++dx)
+        {
+          const int jx = ix + dx, jy = iy + dy;
+          if(jx < 0 || jy < 0 || jx > N || jy > N)
+            continue;
+          double s = 0.0;
+          for(int cy = max(max(iy, jy) - 1, 0); cy <= min(min(iy, jy), N - 1); ++cy)
+            for(int cx = max(max(ix, jx) - 1, 0); cx <= min(min(ix, jx), N - 1); ++cx)
+            {
+              const int a = (ix - cx) + 2 * (iy - cy);
+              const int b = (jx - cx) + 2 * (jy - cy);
+              s += ke[(size_t(cy) * N + cx) * 16 + a * 4 + b];
+            }
+          vals[pos++] = s;
+        }
+    }
+    if(rhs)
+    {
+      double s = 0.0;
+      for(int cy = max(iy - 1, 0); cy <= min(iy, N - 1); ++cy)
+        for(int cx = max(ix - 1, 0); cx <= min(ix, N - 1); ++cx)
+          s += fe[(size_t(cy) * N + cx) * 4 + (ix - cx) + 2 * (iy - cy)];
+      const bool boundary = ix == 0 || iy == 0 || ix == N || iy == N;
+      rhs[v] = boundary ? 0.0 : s;
+    }
+  }
+
+  static bool ref_ready[64] = {};
+  static fb_status upload_ref()
+  {
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    if(dev >= 0 && dev < 64 && ref_ready[dev])
+      return FB_OK;
+    Ref r;
+    const double g = std::sqrt(3.0 / 5.0);
+    const double xs[3] = {-g, 0.0, g}, ws[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    for(int k = 0; k < 3; ++k)
+    {
+      r.xq[k] = xs[k];
+      r.wq[k] = ws[k];
+    }
+    for(int qx = 0; qx < 3; ++qx)
+      for(int qy = 0; qy < 3; ++qy)
+      {
+        const int q = qx * 3 + qy;
+        double gr[4][2];
+        for(int v = 0; v < 4; ++v)
+        {
+          const double sx = (v & 1) ? 1.0 : -1.0, sy = (v & 2) ? 1.0 : -1.0;
+          const double fx = 1.0 + xs[qx] * sx, fy = 1.0 + xs[qy] * sy;
+          r.val[q][v] = fx * fy / 4.0;
+          gr[v][0] = sx * fy / 4.0;
+          gr[v][1] = sy * fx / 4.0;
+        }
+        for(int a = 0; a < 4; ++a)
+          for(int b = 0; b < 4; ++b)
+            r.gg[q][a][b] = gr[a][0] * gr[b][0] + gr[a][1] * gr[b][1];
+      }
+    FB_CUDA(cudaMemcpyToSymbol(c_ref, &r, sizeof(Ref)));
+    if(dev >= 0 && dev < 64)
+      ref_ready[dev] = true;
+    return FB_OK;
+  }
+} // namespace as
+} // namespace fb
+
+using namespace fb;
+
+extern "C" {
+
+fb_status fb_q1_pattern_2d(int level, uint64_t* nnz_out, uint64_t* row_ptr, uint64_t* col_ind)
+{
+  if(level < 0 || level > 13 || !nnz_out)
+  {
+    set_error("q1_pattern_2d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const int N = 1 << level, n1 = N + 1;
+  uint64_t pos = 0;
+  if(row_ptr)
+    row_ptr[0] = 0;
+  for(int iy = 0; iy <= N; ++iy)
+    for(int ix = 0; ix <= N; ++ix)
+    {
+      for(int dy = -1; dy <= 1; ++dy)
+        for(int dx = -1; dx <= 1; ++dx)
+        {
+          const int jx = ix + dx, jy = iy + dy;
+          if(jx < 0 || jy < 0 || jx > N || jy > N)
+            continue;
+          if(col_ind)
+            col_ind[pos] = uint64_t(jy) * n1 + jx;
+          ++pos;
+        }
+      if(row_ptr)
+        row_ptr[uint64_t(iy) * n1 + ix + 1] = pos;
+    }
+  *nnz_out = pos;
+  return FB_OK;
+}
+
+fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
+  const double* gauss, const uint64_t* row_ptr, double* values, double* rhs, void* stream)
+{
+  if(level < 0 || level > 13 || kmodes < 0 || kmodes > 64 || (kmodes && (!xi || !eta)) ||
+     (ngauss && !gauss) || (values && !row_ptr) || (!values && !rhs))
+  {
+    set_error("q1_assemble_2d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  fb_status e = as::upload_ref();
+  if(e != FB_OK)
+    return e;
+  const int N = 1 << level;
+  const double h = 1.0 / N;
+  cudaStream_t st = as_stream(stream);
+  double *ke = nullptr, *fe = nullptr;
+  if(values)
+    FB_CUDA(cudaMallocAsync((void**)&ke, sizeof(double) * 16 * size_t(N) * N, st));
+  if(rhs)
+    FB_CUDA(cudaMallocAsync((void**)&fe, sizeof(double) * 4 * size_t(N) * N, st));
+  const int cells = N * N, verts = (N + 1) * (N + 1);
+  as::k_cells<<<(cells + 127) / 128, 128, 0, st>>>(N, h, kmodes, xi, eta, s, rhs ? ngauss : 0, gauss, ke, fe);
+  as::k_vertices<<<(verts + 255) / 256, 256, 0, st>>>(N, ke, fe, row_ptr, values, rhs);
+  FB_LAUNCHED(2);
+  if(ke)
+    FB_CUDA(cudaFreeAsync(ke, st));
+  if(fe)
+    FB_CUDA(cudaFreeAsync(fe, st));
+  FB_CUDA(cudaStreamSynchronize(st));
+  return FB_OK;
+}
+
+} // extern "C"
