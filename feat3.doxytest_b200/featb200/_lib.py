@@ -87,8 +87,10 @@ _PROTOS = {
     "fb_solver_vcycle": (I, [P, P, P]),
     "fb_solver_level_info": (I, [P, P]),
     "fb_solver_update_matrix": (I, [P, I, P, P]),
+    "fb_solver_set_tolerances": (I, [P, D, D]),
     "fb_q1_pattern_2d": (I, [I, P, P, P]),
     "fb_q1_assemble_2d": (I, [I, I, P, P, D, I, P, P, P, P, P]),
+    "fb_q1_sample_2d": (I, [I, I, P, P, D, I, P, P, P, P]),
     "fb_unet_create": (I, [C.POINTER(P), I, I]),
     "fb_unet_destroy": (None, [P]),
     "fb_unet_num_params": (I, [P, C.POINTER(C.c_uint64)]),

@@ -245,6 +245,10 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
  * removed).  `out` holds 3 * num_levels entries. */
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
 
+/* New stopping tolerances for the following solves (IterativeSolver::set_tol_rel/set_tol_abs,
+ * kernel/solver/iterative.hpp): converged when ||d|| <= tol_abs and ||d|| <= tol_rel * ||d_0||. */
+fb_status fb_solver_set_tolerances(fb_solver* s, double tol_rel, double tol_abs);
+
 /* New values for the system matrix of `level` (0 = finest): `values` is a DEVICE array of the
  * level's used_elements doubles in the pattern and entry order passed to fb_hierarchy_set_level
  * (the pattern must not change).  Rewrites the stored values (and the FP64 copy of the finest level
@@ -321,6 +325,11 @@ fb_status fb_q1_pattern_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t
 fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
                             const double* gauss, const uint64_t* row_ptr, double* values, double* rhs,
                             void* stream);
+
+/* f (sum of Gaussians, as above) and g = log kappa at the vertices of level L (DEVICE arrays of
+ * (2^L+1)^2 doubles, lexicographic; either may be NULL): the inputs of the learned warm start. */
+fb_status fb_q1_sample_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
+                          const double* gauss, double* f, double* g, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* 6. Learned warm start: a convolutional U-Net on vertex grids (no counterpart in the reference) */
