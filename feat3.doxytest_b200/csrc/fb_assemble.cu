@@ -139,6 +139,30 @@ namespace as
     }
   }
 
+  // f and g (= log kappa) at the vertices of level L (lexicographic, x fastest)
+  __global__ void k_sample(int N, int K, const double* __restrict__ xi, const double* __restrict__ eta, double s,
+    int ng, const double* __restrict__ gauss, double* __restrict__ fv, double* __restrict__ gv)
+  {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n1 = N + 1;
+    if(v >= n1 * n1)
+      return;
+    const double h = 1.0 / N;
+    const double x = double(v % n1) * h, y = double(v / n1) * h;
+    if(gv)
+      gv[v] = K > 0 ? field(x, y, K, xi, eta, s) : 0.0;
+    if(fv)
+    {
+      double f = 0.0;
+      for(int g = 0; g < ng; ++g)
+      {
+        const double dx = x - gauss[4 * g + 0], dy = y - gauss[4 * g + 1], w = gauss[4 * g + 2];
+        f += gauss[4 * g + 3] * exp(-(dx * dx + dy * dy) / (2.0 * w * w));
+      }
+      fv[v] = f;
+    }
+  }
+
   static bool ref_ready[64] = {};
   static fb_status upload_ref()
   {
@@ -242,6 +266,23 @@ fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const doubl
     FB_CUDA(cudaFreeAsync(ke, st));
   if(fe)
     FB_CUDA(cudaFreeAsync(fe, st));
+  FB_CUDA(cudaStreamSynchronize(st));
+  return FB_OK;
+}
+
+fb_status fb_q1_sample_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
+  const double* gauss, double* f, double* g, void* stream)
+{
+  if(level < 0 || level > 13 || kmodes < 0 || kmodes > 64 || (kmodes && g && (!xi || !eta)) ||
+     (ngauss && f && !gauss) || (!f && !g))
+  {
+    set_error("q1_sample_2d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const int N = 1 << level, verts = (N + 1) * (N + 1);
+  cudaStream_t st = as_stream(stream);
+  as::k_sample<<<(verts + 255) / 256, 256, 0, st>>>(N, kmodes, xi, eta, s, f ? ngauss : 0, gauss, f, g);
+  FB_LAUNCHED(1);
   FB_CUDA(cudaStreamSynchronize(st));
   return FB_OK;
 }

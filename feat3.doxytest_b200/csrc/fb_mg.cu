@@ -31,6 +31,7 @@
 #include "fb_rows.cuh"
 #include "fb_tma.cuh"
 #include "fb_setup.h"
+#include <cstddef>
 
 #include <algorithm>
 #include <cmath>
@@ -2098,6 +2099,23 @@ namespace fb
 } // namespace fb
 
 extern "C" {
+
+fb_status fb_solver_set_tolerances(fb_solver* s, double tol_rel, double tol_abs)
+{
+  if(!s || !(tol_rel >= 0.0) || !(tol_abs >= 0.0))
+  {
+    set_error("solver_set_tolerances: bad arguments");
+    return FB_ERR_ARG;
+  }
+  FB_CUDA(cudaStreamSynchronize(s->stream));
+  s->cfg.tol_rel = tol_rel;
+  s->cfg.tol_abs = tol_abs;
+  const double t[2] = {tol_rel, tol_abs};
+  static_assert(offsetof(Scalars, tol_abs) == offsetof(Scalars, tol_rel) + sizeof(double), "Scalars layout");
+  FB_CUDA(cudaMemcpy(reinterpret_cast<char*>(s->sc) + offsetof(Scalars, tol_rel), t, sizeof(t),
+                     cudaMemcpyHostToDevice));
+  return FB_OK;
+}
 
 fb_status fb_solver_update_matrix(fb_solver* s, int level, const double* values, void* stream)
 {

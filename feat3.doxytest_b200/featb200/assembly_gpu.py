@@ -84,3 +84,38 @@ class Q1Assembler2D:
                                                 ptr(self.row_ptr_d), ptr(vals), ptr(b) if rhs else None,
                                                 C.c_void_p(stream.cuda_stream)), "fb_q1_assemble_2d")
         return vals, b
+
+
+def sample_2d(level, field=None, gauss=None, stream=None, device="cuda"):
+    """(f, g) at the vertices of level `level` as CUDA float64 tensors of (2^level+1)^2 entries:
+    f = sum of the Gaussians (zeros without), g = log kappa of the field (zeros without)."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    n = (2 ** level + 1) ** 2
+    f = torch.zeros(n, dtype=torch.float64, device=device)
+    g = torch.zeros(n, dtype=torch.float64, device=device)
+    k = 0
+    s = 0.0
+    xi_d = eta_d = g_d = None
+    if field is not None:
+        kx, ky, xi, eta, s = field
+        k = int(len(kx))
+        if not (np.array_equal(np.asarray(kx), np.arange(k) - k // 2) and np.array_equal(np.asarray(ky), np.asarray(kx))):
+            raise ValueError("wave numbers must be -K/2 .. K/2-1 in both directions")
+        xi_d = torch.tensor(np.ascontiguousarray(xi), dtype=torch.float64, device=device)
+        eta_d = torch.tensor(np.ascontiguousarray(eta), dtype=torch.float64, device=device)
+    ng = 0
+    if gauss is not None:
+        g_d = torch.tensor(np.ascontiguousarray(gauss, dtype=np.float64), device=device)
+        ng = int(g_d.shape[0])
+    if k == 0 and ng == 0:
+        return f, g
+
+    def ptr(t):
+        return C.c_void_p(t.data_ptr()) if t is not None else None
+
+    _lib.check(_lib.lib().fb_q1_sample_2d(int(level), k, ptr(xi_d), ptr(eta_d), float(s), ng, ptr(g_d),
+                                          ptr(f) if ng else None, ptr(g) if k else None,
+                                          C.c_void_p(stream.cuda_stream)), "fb_q1_sample_2d")
+    return f, g

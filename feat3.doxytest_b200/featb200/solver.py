@@ -31,7 +31,7 @@ from . import _lib
 from .lafem import DenseVector, SparseMatrixCSR, Transfer, UnitFilter
 
 
-class Status(enum.Enum):
+class Status(enum.IntEnum):
     undefined = 0
     progress = 1
     success = 2
@@ -253,6 +253,11 @@ class PCG:
                                                      C.c_void_p(stream.cuda_stream), C.byref(self.info)),
                    "fb_solver_solve_device")
         return Status(self.info.status)
+
+    def set_tolerances(self, tol_rel, tol_abs):
+        """Stopping test of the following solves: ||d|| <= tol_abs and ||d|| <= tol_rel ||d_0||."""
+        _lib.check(_lib.lib().fb_solver_set_tolerances(self._s, float(tol_rel), float(tol_abs)),
+                   "fb_solver_set_tolerances")
 
     def update_matrix(self, level, values, stream=None):
         """New values for the system matrix of `level` (0 = finest) in the pattern and entry order
