@@ -334,6 +334,8 @@ def main():
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
+    ap.add_argument("--tma-window", type=int, choices=[0, 1], default=1,
+                    help="stage each chunk's window of the gathered vector with the matrix (TMA passes)")
     ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
                     help="device DOF ordering (the generated problems are numbered lexicographically)")
     args = ap.parse_args()
@@ -360,7 +362,7 @@ def main():
     n = b.size
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
-                                    use_graph=not args.profile_solves)
+                                    use_graph=not args.profile_solves, tma_window=args.tma_window)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
@@ -428,7 +430,7 @@ def main():
 
     extra = {}
     if not args.no_plain and precision != "f64":
-        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering)
+        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush()

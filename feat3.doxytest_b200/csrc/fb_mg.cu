@@ -828,6 +828,10 @@ namespace fb
     double bytes = 0;                       // matrix bytes one sweep reads
     uint32_t kw = 0;                        // uniform width (ELL), 0 = sliced
     uint32_t kmax = 0;                      // widest slice's entries per row
+    // x windows of the TMA-staged pass: chunk c (TMA_NT rows) reads x[xlo[c] .. xlo[c] + xwin)
+    // only; xwin = 0: no window (gathers from global memory)
+    uint32_t* xlo = nullptr;
+    uint32_t xwin = 0;
   };
 
   template<typename V> DCsr<V> view(const DevMat& m)
@@ -940,6 +944,53 @@ namespace fb
     const size_t vb = valsize_of(prec);
     const size_t cb = H.narrow ? 2 : 4;
     d.bytes = double(H.entries) * double(vb + cb) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
+    {
+      // column window of every TMA chunk (real entries; narrow padding reads the row itself),
+      // start rounded down to 4 entries (16-byte copies for FP32 and FP64 vectors)
+      const uint32_t spc = uint32_t(TMA_NT) / 32u;
+      const uint32_t nch = (ns + spc - 1) / spc;
+      std::vector<uint32_t> lo(std::max<uint32_t>(1, nch), 0u);
+      uint32_t wmax = 0;
+      for(uint32_t c = 0; c < nch; ++c)
+      {
+        uint32_t mn = UINT32_MAX, mx = 0;
+        for(uint32_t sl = c * spc; sl < std::min(ns, c * spc + spc); ++sl)
+        {
+          const uint32_t K = (H.soff[sl + 1] - H.soff[sl]) / 32u;
+          for(uint32_t lane = 0; lane < 32u; ++lane)
+          {
+            const uint32_t r = sl * 32u + lane;
+            if(r >= H.rows)
+              break;
+            for(uint32_t k = 0; k < K; ++k)
+            {
+              const uint64_t e = H.soff[sl] + uint64_t(k) * 32u + lane;
+              uint32_t col;
+              if(H.narrow)
+                col = uint32_t(int64_t(r) + H.dcol[e]);
+              else if(H.col[e] == H.cols)
+                continue;
+              else
+                col = H.col[e];
+              mn = std::min(mn, col);
+              mx = std::max(mx, col);
+            }
+          }
+        }
+        if(mn == UINT32_MAX)
+          mn = mx = 0;
+        lo[c] = mn & ~3u;
+        wmax = std::max(wmax, mx + 1 - lo[c]);
+      }
+      d.xwin = (wmax + 3u) & ~3u;
+      if(d.xwin > TMA_XWIN_MAX)
+        d.xwin = 0;
+      else
+      {
+        FB_TRY(dalloc(s, (void**)&d.xlo, sizeof(uint32_t) * lo.size()));
+        FB_CUDA(cudaMemcpy(d.xlo, lo.data(), sizeof(uint32_t) * lo.size(), cudaMemcpyHostToDevice));
+      }
+    }
     FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * H.soff.size()));
     FB_CUDA(cudaMemcpy(d.soff, H.soff.data(), sizeof(uint32_t) * H.soff.size(), cudaMemcpyHostToDevice));
     const size_t ne = std::max<size_t>(1, size_t(H.entries));
@@ -999,7 +1050,7 @@ namespace fb
     {
       if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= 100u * 1024u;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
     }
 
     // the TMA-staged pass serves matrices of at least tma_rows rows whose stages fit
@@ -1007,19 +1058,26 @@ namespace fb
     {
       if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= 100u * 1024u;
+      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
     }
     template<typename VV, typename XS, class Op>
     void tma(const DevMat& m, const void* x, const Op& op)
     {
-      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr);
+      // the x window rides along when the stages still fit
+      uint32_t xw = s->cfg.tma_window ? m.xwin : 0u;
+      if(xw && uint64_t(TMA_STAGES) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
+                 TMA_SMEM_MAX)
+        xw = 0;
+      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + xw * uint32_t(sizeof(XS));
       const size_t smem = size_t(TMA_STAGES) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
-      const uint32_t bps = std::max(1u, std::min(8u, uint32_t((200u * 1024u) / (smem + 2048u))));
+      const uint32_t bps = std::max(1u, std::min(8u, uint32_t((227u * 1024u) / (smem + 1536u))));
       const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
-      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax, op,
-                                                        s->slot, s->err);
+      // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
+      const uint32_t nxa = (m.cols + 8u) & ~3u;
+      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
+                                                        xw ? m.xlo : nullptr, xw, nxa, op, s->slot, s->err);
     }
     uint64_t launches = 0;
     double bytes = 0;
@@ -1307,7 +1365,7 @@ namespace fb
   template<typename V, typename S>
   static fb_status set_tma_attrs()
   {
-    const int mx = 160 * 1024;
+    const int mx = int(TMA_SMEM_MAX) + 8 * 1024;
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpSmooth<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpDefect<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost1<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -1451,6 +1509,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->rows_per_block = 0;
   c->tail_rows = 4096;
   c->tma_rows = 32768;
+  c->tma_window = 1;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)

@@ -16,6 +16,8 @@ namespace fb
   constexpr int TMA_NT = 256;          // threads = rows per chunk
   constexpr int TMA_STAGES = 3;
   constexpr uint32_t TMA_SPIN = 1u << 22;
+  constexpr uint32_t TMA_XWIN_MAX = 8192;              // entries of a staged x window
+  constexpr uint64_t TMA_SMEM_MAX = 128u * 1024u;      // dynamic shared memory of all stages
 
   __device__ __forceinline__ uint32_t smem_u32(const void* p)
   {
@@ -56,10 +58,12 @@ namespace fb
   }
 
   // row sum of a staged row with K entries, entry k at base + 32*k, in stored order; the column
-  // is absolute or row-relative
+  // is absolute or row-relative.  With a staged window sx of x[x0 .. x0 + xl), the gathers read
+  // shared memory; a column outside the window is the zero slot of a padding entry (x = 0).
   template<typename V, typename S>
   __device__ __forceinline__ typename ValueTraits<V>::acc staged_row_sum(const V* sv, const int16_t* sd,
-    const uint32_t* sc, uint32_t K, uint32_t base, uint32_t row, const S* __restrict__ x)
+    const uint32_t* sc, uint32_t K, uint32_t base, uint32_t row, const S* __restrict__ x, const S* sx,
+    uint32_t x0, uint32_t xl)
   {
     typedef typename ValueTraits<V>::acc A;
     constexpr uint32_t U = 9;
@@ -73,7 +77,13 @@ namespace fb
         {
           const uint32_t e = base + (k0 + u) * 32u;
           const uint32_t c = sd ? uint32_t(int32_t(row) + int32_t(sd[e])) : sc[e];
-          xv[u] = A(__ldg(x + c));
+          if(sx)
+          {
+            const uint32_t o = c - x0;
+            xv[u] = o < xl ? A(sx[o]) : A(0);
+          }
+          else
+            xv[u] = A(__ldg(x + c));
         }
       #pragma unroll
       for(uint32_t u = 0; u < U; ++u)
@@ -94,9 +104,11 @@ namespace fb
   // sum_i = (A x)_i; op returns the row's contribution to an optional grid reduction, finished by
   // op.finish(total) in thread 0 of the last block.  padded_rows = the storage rows (a multiple of
   // 32); kst = the widest slice's entries per row (= A.kw for ELL), which sizes the stages.
+  // xlo != null: chunk c also stages x[xlo[c] .. xlo[c] + xw) (xw a multiple of 4 entries; the copy
+  // ends at nxa, the entries the vector's allocation holds, at the latest).
   template<typename V, typename S, class Op>
   __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
-    uint32_t kst, Op op, RedSlot slot, int* err)
+    uint32_t kst, const uint32_t* __restrict__ xlo, uint32_t xw, uint32_t nxa, Op op, RedSlot slot, int* err)
   {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
@@ -106,7 +118,8 @@ namespace fb
     constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
-    const uint32_t sb = tma_stage_bytes<V>(kst, narrow);
+    const uint32_t mb = tma_stage_bytes<V>(kst, narrow);
+    const uint32_t sb = mb + (xlo ? xw * uint32_t(sizeof(S)) : 0u);
     const uint32_t nsl = padded_rows / 32u;
     const uint32_t nch = (padded_rows + TMA_NT - 1) / TMA_NT;
     auto issue = [&](uint32_t c, int s)
@@ -126,9 +139,17 @@ namespace fb
       const uint32_t vb = ne * uint32_t(sizeof(V));
       const uint32_t cb = ne * (narrow ? 2u : 4u);
       unsigned char* st = tma_smem + size_t(s) * sb;
-      mbar_expect_tx(&bar[s], vb + cb);
+      uint32_t x0 = 0, xb = 0;
+      if(xlo && ne)
+      {
+        x0 = __ldg(xlo + c);
+        xb = min(xw, nxa - x0) * uint32_t(sizeof(S));
+      }
+      mbar_expect_tx(&bar[s], vb + cb + xb);
       if(ne == 0)
         return;   // every row of the chunk is empty: the arrival alone completes the phase
+      if(xb)
+        bulk_g2s(st + mb, x + x0, xb, &bar[s]);
       bulk_g2s(st, A.val + e0, vb, &bar[s]);
       if(narrow)
         bulk_g2s(st + size_t(TMA_NT) * kst * sizeof(V), A.dcol + e0, cb, &bar[s]);
@@ -183,8 +204,16 @@ namespace fb
           kr = (__ldg(A.soff + sl + 1) - o) >> 5;
           base = o - __ldg(A.soff + c * SPC) + (threadIdx.x & 31u);
         }
+        const S* sx = nullptr;
+        uint32_t x0 = 0, xl = 0;
+        if(xlo)
+        {
+          sx = reinterpret_cast<const S*>(st + mb);
+          x0 = __ldg(xlo + c);
+          xl = min(xw, nxa - x0);
+        }
         const auto sum = staged_row_sum<V, S>(sv, narrow ? reinterpret_cast<const int16_t*>(scol) : nullptr,
-          narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), kr, base, i, x);
+          narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), kr, base, i, x, sx, x0, xl);
         part += op(i, sum, pre);
       }
       __syncthreads();   // every thread is done with stage s

@@ -31,7 +31,8 @@ class SolverConfig(C.Structure):
     _fields_ = [("precision", C.c_int), ("ordering", C.c_int), ("omega", C.c_double),
                 ("smooth_steps", C.c_int), ("tol_rel", C.c_double), ("tol_abs", C.c_double),
                 ("max_iter", C.c_int), ("min_iter", C.c_int), ("use_graph", C.c_int),
-                ("rows_per_block", C.c_int), ("tail_rows", C.c_int), ("tma_rows", C.c_int)]
+                ("rows_per_block", C.c_int), ("tail_rows", C.c_int), ("tma_rows", C.c_int),
+                ("tma_window", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -91,6 +92,7 @@ _PROTOS = {
     "fb_q1_pattern_2d": (I, [I, P, P, P]),
     "fb_q1_assemble_2d": (I, [I, I, P, P, D, I, P, P, P, P, P]),
     "fb_q1_sample_2d": (I, [I, I, P, P, D, I, P, P, P, P]),
+    "fb_q1_prolongation_2d": (I, [I, C.POINTER(C.c_uint64), P, P, P, P]),
     "fb_unet_create": (I, [C.POINTER(P), I, I]),
     "fb_unet_destroy": (None, [P]),
     "fb_unet_num_params": (I, [P, C.POINTER(C.c_uint64)]),

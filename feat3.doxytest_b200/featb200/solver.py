@@ -206,6 +206,10 @@ class PCG:
         """Uniform-width levels with at least `rows` rows use the TMA-staged passes (0 = off)."""
         self.cfg.tma_rows = int(rows)
 
+    def set_tma_window(self, flag):
+        """TMA-staged passes also stage each chunk's window of the gathered vector (default on)."""
+        self.cfg.tma_window = 1 if flag else 0
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -315,7 +319,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
-                        ordering="native", use_graph=True, tail_rows=None, tma_rows=None):
+                        ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -337,6 +341,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_tail_rows(tail_rows)
     if tma_rows is not None:
         s.set_tma_rows(tma_rows)
+    if tma_window is not None:
+        s.set_tma_window(tma_window)
     h.init()
     s.init()
     return s

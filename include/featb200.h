@@ -188,8 +188,11 @@ typedef struct
   int rows_per_block;   /* CSR kernel rows per block, 0 = autotuned */
   int tail_rows;        /* levels (below the finest) with at most this many rows, down to the
                            coarsest, run in one single-block kernel per V-cycle; 0 = off */
-  int tma_rows;         /* uniform-width levels with at least this many rows use the TMA-staged
-                           persistent passes (bulk copies into shared memory); 0 = off */
+  int tma_rows;         /* levels with at least this many rows use the TMA-staged persistent
+                           passes (bulk copies into shared memory); 0 = off */
+  int tma_window;       /* 1: the TMA-staged passes also stage each chunk's window of the gathered
+                           vector, so the row sums gather from shared memory; 0 = gather from
+                           global memory */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
@@ -325,6 +328,14 @@ fb_status fb_q1_pattern_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t
 fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,
                             const double* gauss, const uint64_t* row_ptr, double* values, double* rhs,
                             void* stream);
+
+/* The Q1 prolongation from level-1 to `level` (1 <= level <= 13) on the lexicographic vertices
+ * (weights 1, 1/2, 1/4; entries in ascending coarse index), written into DEVICE arrays (row_ptr
+ * (2^level+1)^2+1, col_ind and values nnz entries); with all three NULL only nnz is returned.  The
+ * reference assembles it on the host (assemble_prolongation_direct,
+ * kernel/assembly/grid_transfer.hpp:353-430); R = P^T. */
+fb_status fb_q1_prolongation_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind, double* values,
+                                void* stream);
 
 /* f (sum of Gaussians, as above) and g = log kappa at the vertices of level L (DEVICE arrays of
  * (2^L+1)^2 doubles, lexicographic; either may be NULL): the inputs of the learned warm start. */

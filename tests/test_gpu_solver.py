@@ -151,15 +151,18 @@ def test_device_entry_point_and_launch_count(featlib, cuda):
 
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-def test_tma_staged_passes_match(featlib, cuda, name, precision):
-    """The TMA-staged passes (bulk copies of matrix chunks into shared memory) forced onto every
-    uniform-width level give the same results as the per-row kernels: bitwise V-cycles in FP64,
-    identical iterations, solutions within rounding of the dot products."""
+@pytest.mark.parametrize("window,ordering", [(1, "native"), (0, "native"), (1, "rcm")])
+def test_tma_staged_passes_match(featlib, cuda, name, precision, window, ordering):
+    """The TMA-staged passes (bulk copies of matrix chunks, and with window=1 of each chunk's window
+    of the gathered vector, into shared memory) forced onto every level give the same results as
+    the per-row kernels: bitwise V-cycles in FP64, identical iterations, solutions within rounding
+    of the dot products."""
     fb = featlib
     g = load_golden(name)
     lv = to_lafem_levels(g["levels"])
-    s_tma, x_tma, st1 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=32, tail_rows=0)
-    s_ref, x_ref, st2 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=0, tail_rows=0)
+    s_tma, x_tma, st1 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=32, tail_rows=0,
+                               tma_window=window, ordering=ordering)
+    s_ref, x_ref, st2 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=0, tail_rows=0, ordering=ordering)
     assert st1 == st2 == fb.Status.success
     assert s_tma.get_num_iter() == s_ref.get_num_iter()
     z1 = s_tma.apply_precond(fb.DenseVector(g["rhs"])).elements
@@ -171,15 +174,16 @@ def test_tma_staged_passes_match(featlib, cuda, name, precision):
         assert rel_err(x_tma, g["sol"]) <= PARITY
 
 
-def test_tma_full_size(featlib, cuda, oracle_lib):
-    """Level 10 with the default thresholds (TMA on the large levels): bitwise V-cycle against the
-    C oracle, solution within 1e-12."""
+@pytest.mark.parametrize("ordering", ["native", "rcm"])
+def test_tma_full_size(featlib, cuda, oracle_lib, ordering):
+    """Level 10 with the default thresholds (TMA with staged vector windows on the large levels):
+    bitwise V-cycle against the C oracle, solution within 1e-12."""
     from featb200 import assembly as AS
     fb = featlib
     levels, b = AS.poisson_hierarchy(10, 2, rhs="gauss", gauss=AS.gauss_params(3, 2))
     mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
     x_ref, info = mg.solve(b)
-    s, x, st = _solve(fb, levels, b, ordering="native")
+    s, x, st = _solve(fb, levels, b, ordering=ordering)
     assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, mg.vcycle(b))
     assert st == fb.Status.success and s.get_num_iter() == info["iters"]
     assert rel_err(x, x_ref) <= PARITY
