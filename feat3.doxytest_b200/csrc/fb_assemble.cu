@@ -56,8 +56,41 @@ namespace as
     return s * acc;
   }
 
+  // Separable tables of the field at the quadrature coordinates (3 per cell and direction, index
+  // 3*cell + q): ex[t][i] = e^{2 pi i kx_i x_t} and hy[t][i] = sum_j c_ij e^{2 pi i ky_j y_t}, so that
+  // g(x_t, y_u) = s * sum_i Re(ex[t][i] * hy[u][i]): K complex products per point instead of K^2
+  // sine/cosine pairs.
+  __global__ void k_field_tables(int N, double h, int K, const double* __restrict__ xi,
+    const double* __restrict__ eta, double2* __restrict__ ex, double2* __restrict__ hy)
+  {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if(e >= 3 * N * K)
+      return;
+    const double tp = 6.283185307179586476925286766559;
+    const int i = e % K, t = e / K;
+    const double c = (double(t / 3) + (1.0 + c_ref.xq[t % 3]) / 2.0) * h;   // x_t = y_t
+    const double kx = double(i - K / 2);
+    double sx, cx;
+    sincos(tp * kx * c, &sx, &cx);
+    ex[e] = make_double2(cx, sx);
+    double hr = 0.0, hi = 0.0;
+    for(int j = 0; j < K; ++j)
+    {
+      const double ky = double(j - K / 2);
+      const double den = kx * kx + ky * ky;
+      if(den == 0.0)
+        continue;
+      double sy, cy;
+      sincos(tp * ky * c, &sy, &cy);
+      const double a = __ldg(xi + i * K + j) / den, b = __ldg(eta + i * K + j) / den;
+      hr += a * cy + b * sy;
+      hi += a * sy - b * cy;
+    }
+    hy[e] = make_double2(hr, hi);
+  }
+
   // per cell: the 4x4 element matrix (kappa-weighted) and the 4 load-vector contributions
-  __global__ void k_cells(int N, double h, int K, const double* __restrict__ xi, const double* __restrict__ eta,
+  __global__ void k_cells(int N, double h, int K, const double2* __restrict__ ex, const double2* __restrict__ hy,
     double s, int ng, const double* __restrict__ gauss, double* __restrict__ ke, double* __restrict__ fe)
   {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,7 +104,20 @@ namespace as
         const int q = qx * 3 + qy;   // reference order: x index slowest (meshgrid "ij" over (x, y))
         const double x = (double(cx) + (1.0 + c_ref.xq[qx]) / 2.0) * h;
         const double y = (double(cy) + (1.0 + c_ref.xq[qy]) / 2.0) * h;
-        kq[q] = (K > 0 && ke) ? exp(field(x, y, K, xi, eta, s)) : 1.0;
+        double kv = 1.0;
+        if(K > 0 && ke)
+        {
+          const double2* exr = ex + size_t(cx * 3 + qx) * K;
+          const double2* hyr = hy + size_t(cy * 3 + qy) * K;
+          double g = 0.0;
+          for(int i = 0; i < K; ++i)
+          {
+            const double2 a = __ldg(exr + i), b = __ldg(hyr + i);
+            g += b.x * a.x - b.y * a.y;
+          }
+          kv = exp(s * g);
+        }
+        kq[q] = kv;
         double f = 0.0;
         for(int g = 0; g < ng && fe; ++g)
         {
@@ -161,6 +207,35 @@ namespace as
       }
       fv[v] = f;
     }
+  }
+
+  // Q1 prolongation level-1 -> level on the lexicographic vertices: fine vertex (ix, iy) takes
+  // coarse (ix/2, iy/2) with weight 1 per even coordinate and the two neighbours (i-1)/2, (i+1)/2
+  // with 1/2 each per odd coordinate; entries in ascending coarse index.  The row pointer is in
+  // closed form: cnt(i) = 1 + (i odd), sum_{j<i} cnt(j) = i + i/2.
+  __global__ void k_prolongation(int Nf, uint64_t* __restrict__ rp, uint64_t* __restrict__ col,
+    double* __restrict__ val)
+  {
+    const int n1 = Nf + 1, nc1 = Nf / 2 + 1;
+    const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(v >= uint64_t(n1) * n1)
+      return;
+    const int ix = int(v % n1), iy = int(v / n1);
+    const uint64_t W = uint64_t(n1 + Nf / 2);
+    const int cx = 1 + (ix & 1), cy = 1 + (iy & 1);
+    const uint64_t off = uint64_t(iy + iy / 2) * W + uint64_t(cy) * uint64_t(ix + ix / 2);
+    rp[v] = off;
+    if(v + 1 == uint64_t(n1) * n1)
+      rp[v + 1] = off + uint64_t(cx) * cy;
+    const int x0 = ix / 2, y0 = iy / 2;   // odd i: (i-1)/2 and (i+1)/2 = x0, x0 + 1
+    uint64_t e = off;
+    for(int b = 0; b < cy; ++b)
+      for(int a = 0; a < cx; ++a)
+      {
+        col[e] = uint64_t(y0 + b) * nc1 + uint64_t(x0 + a);
+        val[e] = (cx == 2 ? 0.5 : 1.0) * (cy == 2 ? 0.5 : 1.0);
+        ++e;
+      }
   }
 
   static bool ref_ready[64] = {};
@@ -254,18 +329,56 @@ fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const doubl
   const double h = 1.0 / N;
   cudaStream_t st = as_stream(stream);
   double *ke = nullptr, *fe = nullptr;
+  double2 *ex = nullptr, *hy = nullptr;
+  const int K = values ? kmodes : 0;
   if(values)
     FB_CUDA(cudaMallocAsync((void**)&ke, sizeof(double) * 16 * size_t(N) * N, st));
   if(rhs)
     FB_CUDA(cudaMallocAsync((void**)&fe, sizeof(double) * 4 * size_t(N) * N, st));
+  if(K)
+  {
+    FB_CUDA(cudaMallocAsync((void**)&ex, sizeof(double2) * 3 * size_t(N) * K, st));
+    FB_CUDA(cudaMallocAsync((void**)&hy, sizeof(double2) * 3 * size_t(N) * K, st));
+    as::k_field_tables<<<(3 * N * K + 127) / 128, 128, 0, st>>>(N, h, K, xi, eta, ex, hy);
+    FB_LAUNCHED(1);
+  }
   const int cells = N * N, verts = (N + 1) * (N + 1);
-  as::k_cells<<<(cells + 127) / 128, 128, 0, st>>>(N, h, kmodes, xi, eta, s, rhs ? ngauss : 0, gauss, ke, fe);
+  as::k_cells<<<(cells + 127) / 128, 128, 0, st>>>(N, h, K, ex, hy, s, rhs ? ngauss : 0, gauss, ke, fe);
   as::k_vertices<<<(verts + 255) / 256, 256, 0, st>>>(N, ke, fe, row_ptr, values, rhs);
   FB_LAUNCHED(2);
   if(ke)
     FB_CUDA(cudaFreeAsync(ke, st));
   if(fe)
     FB_CUDA(cudaFreeAsync(fe, st));
+  if(ex)
+    FB_CUDA(cudaFreeAsync(ex, st));
+  if(hy)
+    FB_CUDA(cudaFreeAsync(hy, st));
+  FB_CUDA(cudaStreamSynchronize(st));
+  return FB_OK;
+}
+
+fb_status fb_q1_prolongation_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind, double* values,
+  void* stream)
+{
+  if(level < 1 || level > 13 || !nnz)
+  {
+    set_error("q1_prolongation_2d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const uint64_t Nf = uint64_t(1) << level, n1 = Nf + 1;
+  const uint64_t cnt = n1 + Nf / 2;   // x-entries per fine row
+  *nnz = cnt * cnt;
+  if(!row_ptr && !col_ind && !values)
+    return FB_OK;
+  if(!row_ptr || !col_ind || !values)
+  {
+    set_error("q1_prolongation_2d: row_ptr, col_ind and values are all needed");
+    return FB_ERR_ARG;
+  }
+  cudaStream_t st = as_stream(stream);
+  as::k_prolongation<<<unsigned((n1 * n1 + 255) / 256), 256, 0, st>>>(int(Nf), row_ptr, col_ind, values);
+  FB_LAUNCHED(1);
   FB_CUDA(cudaStreamSynchronize(st));
   return FB_OK;
 }

@@ -119,3 +119,22 @@ def sample_2d(level, field=None, gauss=None, stream=None, device="cuda"):
                                           ptr(f) if ng else None, ptr(g) if k else None,
                                           C.c_void_p(stream.cuda_stream)), "fb_q1_sample_2d")
     return f, g
+
+
+def q1_prolongation_2d(level, device="cuda", stream=None):
+    """(row_ptr, col_ind, values) of the Q1 prolongation level-1 -> level as CUDA tensors
+    (int64, int64, float64)."""
+    import torch
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    nnz = C.c_uint64(0)
+    _lib.check(_lib.lib().fb_q1_prolongation_2d(int(level), C.byref(nnz), None, None, None, None),
+               "fb_q1_prolongation_2d")
+    n = (2 ** level + 1) ** 2
+    rp = torch.empty(n + 1, dtype=torch.int64, device=device)
+    ci = torch.empty(int(nnz.value), dtype=torch.int64, device=device)
+    v = torch.empty(int(nnz.value), dtype=torch.float64, device=device)
+    _lib.check(_lib.lib().fb_q1_prolongation_2d(int(level), C.byref(nnz), C.c_void_p(rp.data_ptr()),
+                                                C.c_void_p(ci.data_ptr()), C.c_void_p(v.data_ptr()),
+                                                C.c_void_p(stream.cuda_stream)), "fb_q1_prolongation_2d")
+    return rp, ci, v

@@ -127,3 +127,16 @@ def test_update_matrix_rejects_bad_level(featlib, cuda):
         s.update_matrix(len(lv0), v)
     with pytest.raises(fb.FeatB200Error):
         s.update_matrix(-1, v)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [1, 2, 5, 8])
+def test_prolongation_matches_host(featlib, cuda, level):
+    from featb200.assembly_gpu import q1_prolongation_2d
+    rp, ci, v = q1_prolongation_2d(level)
+    cuda.cuda.synchronize()
+    P = AS.prolongation(level, 2).tocsr()
+    P.sort_indices()
+    assert np.array_equal(rp.cpu().numpy(), P.indptr.astype(np.int64))
+    assert np.array_equal(ci.cpu().numpy(), P.indices.astype(np.int64))
+    assert np.array_equal(v.cpu().numpy(), P.data)
