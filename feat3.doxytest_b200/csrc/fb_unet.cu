@@ -6,7 +6,9 @@
 //   L1 conv 2->16 @G1, ReLU = e1;  S = injection (every other vertex)
 //   L2 conv 16->32 @G2 on S(e1), ReLU = e2
 //   L3 conv 32->64 @G3 on S(e2), ReLU = e3
-//   L4 conv 64->64 @G4 on S(e3), ReLU = e4
+//   L4 conv 64->64 @G4 on S(e3), then two more 64->64 convolutions @G4 with dilation 2 and 4
+//      (ReLU after each) = e4: the bottleneck sees 15 x 15 of its 17 x 17 points (for G1 = 129), so
+//      the prediction can couple the whole domain as the solution operator does
 //   L5 conv 128->64 @G3 on [U(e4), e3], ReLU = d3;  U = bilinear vertex upsampling (the Q1
 //      prolongation stencil: coincident vertex 1, edge midpoints 1/2 + 1/2, cell centres 4 x 1/4)
 //   L6 conv 96->32 @G2 on [U(d3), e2], ReLU = d2
@@ -36,12 +38,12 @@ namespace un
   __device__ __forceinline__ float bf2f(bf v) { return __uint_as_float(uint32_t(v) << 16); }
   __device__ __forceinline__ bf f2bf(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 
-  constexpr int NLAYER = 8;
-  struct LayerDef { int cin, cout, level; bool relu; };
-  // real channel counts; level = resolution index (0 = finest grid)
+  constexpr int NLAYER = 10;
+  struct LayerDef { int cin, cout, level; bool relu; int dil; };
+  // real channel counts; level = resolution index (0 = finest grid); dil = tap spacing
   constexpr LayerDef LAYERS[NLAYER] = {
-    {2, 16, 0, true}, {16, 32, 1, true}, {32, 64, 2, true}, {64, 64, 3, true},
-    {128, 64, 2, true}, {96, 32, 1, true}, {48, 16, 0, true}, {16, 1, 0, false}};
+    {2, 16, 0, true, 1}, {16, 32, 1, true, 1}, {32, 64, 2, true, 1}, {64, 64, 3, true, 1}, {64, 64, 3, true, 2},
+    {64, 64, 3, true, 4}, {128, 64, 2, true, 1}, {96, 32, 1, true, 1}, {48, 16, 0, true, 1}, {16, 1, 0, false, 1}};
 
   __host__ __device__ inline int pad8(int c) { return (c + 7) & ~7; }
 
@@ -95,7 +97,7 @@ namespace un
     const float* bias;     // nb entries (columns >= nb get no bias)
     void* y;
     int cin, kpad, n, n_ld, nb;
-    int B, H, W;
+    int B, H, W, dil;
     int y_ld, y_off;
     int relu, out_bf16;
   };
@@ -138,7 +140,7 @@ namespace un
         if(prow && k < K9)
         {
           const int tap = k / a.cin, ci = k - tap * a.cin;
-          const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+          const int yy = py + (tap / 3 - 1) * a.dil, xx = px + (tap % 3 - 1) * a.dil;
           if(yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
           {
             src = a.x + ((size_t(pb) * a.H + yy) * a.W + xx) * a.cin + ci;
@@ -266,7 +268,7 @@ namespace un
     const bf* x;         // [P][cin]
     float* part;         // [splits][m][n] (m < m_real, n < 9*cin)
     int m_ld, m_real, cin;
-    int B, H, W;
+    int B, H, W, dil;
     int pix_per_split;
   };
 
@@ -315,7 +317,7 @@ namespace un
           const int tap = j / a.cin, ci = j - tap * a.cin;
           const int px = p % a.W, t = p / a.W;
           const int py = t % a.H, pb = t / a.H;
-          const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+          const int yy = py + (tap / 3 - 1) * a.dil, xx = px + (tap % 3 - 1) * a.dil;
           if(yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
           {
             src = a.x + ((size_t(pb) * a.H + yy) * a.W + xx) * a.cin + ci;
@@ -667,6 +669,7 @@ struct fb_unet
   bf* wd[NLAYER] = {};
   // activations (BF16 NHWC): x8 (input), e1..e4, s1..s3, c3, c2, c1, d3, d2, d1
   bf *x8 = nullptr, *e[4] = {}, *s[3] = {}, *c[3] = {}, *d[3] = {};
+  bf* b4[2] = {};              // bottleneck: outputs of the dilation-2 and dilation-4 convolutions
   float* yout = nullptr;       // [P1][8] FP32 pre-activation output of L8
   // backward scratch: BF16 output gradient and pre-activation gradient (one layer at a time);
   // FP32 data gradients of the concatenated inputs (dc1 @G1 48 ch, dc2 @G2 96, dc3 @G3 128) and of
@@ -731,6 +734,7 @@ namespace
     a.n_ld = u->cout_pad[l];
     a.nb = LAYERS[l].cout;
     a.B = B;
+    a.dil = LAYERS[l].dil;
     a.H = G;
     a.W = G;
     a.y_ld = y_ld;
@@ -765,6 +769,7 @@ namespace
     a.n_ld = u->cin_pad[l];
     a.nb = 0;
     a.B = B;
+    a.dil = LAYERS[l].dil;
     a.H = G;
     a.W = G;
     a.y_ld = u->cin_pad[l];
@@ -812,6 +817,7 @@ namespace
     a.B = B;
     a.H = G;
     a.W = G;
+    a.dil = L.dil;
     a.pix_per_split = pps;
     dim3 grid(ntile, splits);
     const int bm = u->cout_pad[l] <= 16 ? 16 : (u->cout_pad[l] <= 32 ? 32 : 64);
@@ -892,6 +898,8 @@ fb_status fb_unet_create(fb_unet** out, int grid, int max_batch)
     UN_A(p->e[i], sizeof(bf) * pix(i) * ech[i]);
   for(int i = 0; i < 3; ++i)
     UN_A(p->s[i], sizeof(bf) * pix(i + 1) * ech[i]);
+  for(int i = 0; i < 2; ++i)
+    UN_A(p->b4[i], sizeof(bf) * pix(3) * 64);
   // c[0] = [U(d2), e1] @G1 (48), c[1] = [U(d3), e2] @G2 (96), c[2] = [U(e4), e3] @G3 (128)
   UN_A(p->c[0], sizeof(bf) * pix(0) * 48);
   UN_A(p->c[1], sizeof(bf) * pix(1) * 96);
@@ -1002,21 +1010,24 @@ fb_status fb_unet_forward(fb_unet* u, const float* in, float* out, int batch, vo
     FB_LAUNCHED(1);
     UN_TRY(conv_fwd(u, i + 1, u->s[i], B, G[i + 1], u->e[i + 1], ech[i + 1], true, true, st));
   }
+  // bottleneck: dilation 2 and 4
+  UN_TRY(conv_fwd(u, 4, u->e[3], B, G[3], u->b4[0], 64, true, true, st));
+  UN_TRY(conv_fwd(u, 5, u->b4[0], B, G[3], u->b4[1], 64, true, true, st));
   // decoder
   {
     const size_t n3 = size_t(B) * G[2] * G[2] * 128;
-    k_upsample_cat<<<grid_for(n3), 256, 0, st>>>(u->e[3], 64, u->e[2], 64, B, G[2], u->c[2]);
+    k_upsample_cat<<<grid_for(n3), 256, 0, st>>>(u->b4[1], 64, u->e[2], 64, B, G[2], u->c[2]);
     FB_LAUNCHED(1);
-    UN_TRY(conv_fwd(u, 4, u->c[2], B, G[2], u->d[2], 64, true, true, st));
+    UN_TRY(conv_fwd(u, 6, u->c[2], B, G[2], u->d[2], 64, true, true, st));
     const size_t n2 = size_t(B) * G[1] * G[1] * 96;
     k_upsample_cat<<<grid_for(n2), 256, 0, st>>>(u->d[2], 64, u->e[1], 32, B, G[1], u->c[1]);
     FB_LAUNCHED(1);
-    UN_TRY(conv_fwd(u, 5, u->c[1], B, G[1], u->d[1], 32, true, true, st));
+    UN_TRY(conv_fwd(u, 7, u->c[1], B, G[1], u->d[1], 32, true, true, st));
     const size_t n1 = size_t(B) * G[0] * G[0] * 48;
     k_upsample_cat<<<grid_for(n1), 256, 0, st>>>(u->d[1], 32, u->e[0], 16, B, G[0], u->c[0]);
     FB_LAUNCHED(1);
-    UN_TRY(conv_fwd(u, 6, u->c[0], B, G[0], u->d[0], 16, true, true, st));
-    UN_TRY(conv_fwd(u, 7, u->d[0], B, G[0], u->yout, 8, false, false, st));
+    UN_TRY(conv_fwd(u, 8, u->c[0], B, G[0], u->d[0], 16, true, true, st));
+    UN_TRY(conv_fwd(u, 9, u->d[0], B, G[0], u->yout, 8, false, false, st));
   }
   k_unpack_out<<<grid_for(P0), 256, 0, st>>>(u->yout, P0, out);
   FB_LAUNCHED(1);
@@ -1041,25 +1052,35 @@ fb_status fb_unet_backward(fb_unet* u, const float* dout, int batch, int accumul
   // L8 (input d1): dy8 = dout
   k_pack_dout<<<grid_for(P0), 256, 0, st>>>(dout, P0, u->dy8);
   FB_LAUNCHED(1);
-  UN_TRY(conv_bwd_weight(u, 7, u->dy8, u->d[0], B, G[0], acc, st));
-  UN_TRY(conv_bwd_data(u, 7, u->dy8, B, G[0], u->gs, st));                       // d1 grad [P0][16]
+  UN_TRY(conv_bwd_weight(u, 9, u->dy8, u->d[0], B, G[0], acc, st));
+  UN_TRY(conv_bwd_data(u, 9, u->dy8, B, G[0], u->gs, st));                       // d1 grad [P0][16]
   // L7 (input c1 = [U(d2), e1]): dpre = mask(d1) * gs
   k_grad_mask<<<grid_for(n_at(0, 16)), 256, 0, st>>>(u->d[0], 16, B, G[0], u->gs, 16, 0, nullptr, 0, u->dpre);
   FB_LAUNCHED(1);
-  UN_TRY(conv_bwd_weight(u, 6, u->dpre, u->c[0], B, G[0], acc, st));
-  UN_TRY(conv_bwd_data(u, 6, u->dpre, B, G[0], u->dc[0], st));                   // dc1 [P0][48]
+  UN_TRY(conv_bwd_weight(u, 8, u->dpre, u->c[0], B, G[0], acc, st));
+  UN_TRY(conv_bwd_data(u, 8, u->dpre, B, G[0], u->dc[0], st));                   // dc1 [P0][48]
   // L6 (input c2 = [U(d3), e2]): dpre = mask(d2) * U^T(dc1[:, 0:32])
   k_upsample_bwd_mask<<<grid_for(n_at(1, 32)), 256, 0, st>>>(u->dc[0], 48, 0, 32, B, G[0], u->d[1], u->dpre);
   FB_LAUNCHED(1);
-  UN_TRY(conv_bwd_weight(u, 5, u->dpre, u->c[1], B, G[1], acc, st));
-  UN_TRY(conv_bwd_data(u, 5, u->dpre, B, G[1], u->dc[1], st));                   // dc2 [P1][96]
+  UN_TRY(conv_bwd_weight(u, 7, u->dpre, u->c[1], B, G[1], acc, st));
+  UN_TRY(conv_bwd_data(u, 7, u->dpre, B, G[1], u->dc[1], st));                   // dc2 [P1][96]
   // L5 (input c3 = [U(e4), e3]): dpre = mask(d3) * U^T(dc2[:, 0:64])
   k_upsample_bwd_mask<<<grid_for(n_at(2, 64)), 256, 0, st>>>(u->dc[1], 96, 0, 64, B, G[1], u->d[2], u->dpre);
   FB_LAUNCHED(1);
-  UN_TRY(conv_bwd_weight(u, 4, u->dpre, u->c[2], B, G[2], acc, st));
-  UN_TRY(conv_bwd_data(u, 4, u->dpre, B, G[2], u->dc[2], st));                   // dc3 [P2][128]
-  // L4 (input s3 = S(e3)): dpre = mask(e4) * U^T(dc3[:, 0:64])
-  k_upsample_bwd_mask<<<grid_for(n_at(3, 64)), 256, 0, st>>>(u->dc[2], 128, 0, 64, B, G[2], u->e[3], u->dpre);
+  UN_TRY(conv_bwd_weight(u, 6, u->dpre, u->c[2], B, G[2], acc, st));
+  UN_TRY(conv_bwd_data(u, 6, u->dpre, B, G[2], u->dc[2], st));                   // dc3 [P2][128]
+  // bottleneck, dilation 4 (input b4[0]): dpre = mask(e4) * U^T(dc3[:, 0:64])
+  k_upsample_bwd_mask<<<grid_for(n_at(3, 64)), 256, 0, st>>>(u->dc[2], 128, 0, 64, B, G[2], u->b4[1], u->dpre);
+  FB_LAUNCHED(1);
+  UN_TRY(conv_bwd_weight(u, 5, u->dpre, u->b4[0], B, G[3], acc, st));
+  UN_TRY(conv_bwd_data(u, 5, u->dpre, B, G[3], u->gs, st));                      // b4[0] grad [P3][64]
+  // bottleneck, dilation 2 (input e4a = e[3])
+  k_grad_mask<<<grid_for(n_at(3, 64)), 256, 0, st>>>(u->b4[0], 64, B, G[3], u->gs, 64, 0, nullptr, 0, u->dpre);
+  FB_LAUNCHED(1);
+  UN_TRY(conv_bwd_weight(u, 4, u->dpre, u->e[3], B, G[3], acc, st));
+  UN_TRY(conv_bwd_data(u, 4, u->dpre, B, G[3], u->gs, st));                      // e[3] grad [P3][64]
+  // L4 (input s3 = S(e3))
+  k_grad_mask<<<grid_for(n_at(3, 64)), 256, 0, st>>>(u->e[3], 64, B, G[3], u->gs, 64, 0, nullptr, 0, u->dpre);
   FB_LAUNCHED(1);
   UN_TRY(conv_bwd_weight(u, 3, u->dpre, u->s[2], B, G[3], acc, st));
   UN_TRY(conv_bwd_data(u, 3, u->dpre, B, G[3], u->gs, st));                      // s3 grad [P3][64]

@@ -12,8 +12,9 @@ import numpy as np
 
 from . import _lib
 
-# (cin, cout) of the eight convolutions, in parameter order
-LAYERS = [(2, 16), (16, 32), (32, 64), (64, 64), (128, 64), (96, 32), (48, 16), (16, 1)]
+# (cin, cout) of the ten convolutions, in parameter order (L1, L2, L3, L4, the two dilated
+# bottleneck convolutions, L5, L6, L7, L8)
+LAYERS = [(2, 16), (16, 32), (32, 64), (64, 64), (64, 64), (64, 64), (128, 64), (96, 32), (48, 16), (16, 1)]
 
 
 def num_params():
@@ -47,9 +48,12 @@ class UNet:
         self._loss = torch.zeros(1, dtype=torch.float64, device="cuda")
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            _lib.lib().fb_unet_destroy(self._h)
-            self._h = None
+        try:
+            if getattr(self, "_h", None):
+                _lib.lib().fb_unet_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
 
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)

@@ -20,20 +20,21 @@ from __future__ import annotations
 
 import numpy as np
 
-# (cin, cout, level, relu): L1..L8
-LAYERS = [(2, 16, 0, True), (16, 32, 1, True), (32, 64, 2, True), (64, 64, 3, True),
-          (128, 64, 2, True), (96, 32, 1, True), (48, 16, 0, True), (16, 1, 0, False)]
+# (cin, cout, level, relu, dilation): L1, L2, L3, L4 + two dilated bottleneck convolutions, L5..L8
+LAYERS = [(2, 16, 0, True, 1), (16, 32, 1, True, 1), (32, 64, 2, True, 1), (64, 64, 3, True, 1),
+          (64, 64, 3, True, 2), (64, 64, 3, True, 4), (128, 64, 2, True, 1), (96, 32, 1, True, 1),
+          (48, 16, 0, True, 1), (16, 1, 0, False, 1)]
 
 
 def num_params():
-    return sum(co * 9 * ci + co for ci, co, _, _ in LAYERS)
+    return sum(co * 9 * ci + co for ci, co, _, _, _ in LAYERS)
 
 
 def split_params(theta):
     """Flat vector -> [(W [co, 9, ci], b [co])] (views)."""
     out = []
     k = 0
-    for ci, co, _, _ in LAYERS:
+    for ci, co, _, _, _ in LAYERS:
         W = theta[k:k + co * 9 * ci].reshape(co, 9, ci)
         k += co * 9 * ci
         b = theta[k:k + co]
@@ -60,28 +61,29 @@ def _shift(x, dy, dx):
     s = np.zeros_like(x)
     ys0, ys1 = max(0, -dy), min(H, H - dy)
     xs0, xs1 = max(0, -dx), min(W, W - dx)
-    s[:, ys0:ys1, xs0:xs1] = x[:, ys0 + dy:ys1 + dy, xs0 + dx:xs1 + dx]
+    if ys0 < ys1 and xs0 < xs1:
+        s[:, ys0:ys1, xs0:xs1] = x[:, ys0 + dy:ys1 + dy, xs0 + dx:xs1 + dx]
     return s
 
 
-def _cols(x):
-    """im2col: [B, H, W, 9, C]."""
-    return np.stack([_shift(x, t // 3 - 1, t % 3 - 1) for t in range(9)], axis=3)
+def _cols(x, dil=1):
+    """im2col with tap spacing dil: [B, H, W, 9, C]."""
+    return np.stack([_shift(x, (t // 3 - 1) * dil, (t % 3 - 1) * dil) for t in range(9)], axis=3)
 
 
-def conv(x, W, b):
-    return np.einsum("bhwtc,otc->bhwo", _cols(x), W, optimize=True) + b
+def conv(x, W, b, dil=1):
+    return np.einsum("bhwtc,otc->bhwo", _cols(x, dil), W, optimize=True) + b
 
 
-def conv_bwd(x, W, dy):
-    """(dx, dW, db) of y = conv(x, W, b) for upstream gradient dy."""
-    cols = _cols(x)
+def conv_bwd(x, W, dy, dil=1):
+    """(dx, dW, db) of y = conv(x, W, b, dil) for upstream gradient dy."""
+    cols = _cols(x, dil)
     dW = np.einsum("bhwo,bhwtc->otc", dy, cols, optimize=True)
     db = dy.sum(axis=(0, 1, 2))
     dx = np.zeros_like(x)
     for t in range(9):
         T = np.einsum("bhwo,oc->bhwc", dy, W[:, t, :], optimize=True)
-        dx += _shift(T, -(t // 3 - 1), -(t % 3 - 1))
+        dx += _shift(T, -(t // 3 - 1) * dil, -(t % 3 - 1) * dil)
     return dx, dW, db
 
 
@@ -137,7 +139,7 @@ def forward(theta, inp, exact=True):
 
     def layer(l, a):
         W, b = P[l]
-        pre = conv(a, W, b)
+        pre = conv(a, W, b, LAYERS[l][4])
         return R(np.maximum(pre, 0.0)) if LAYERS[l][3] else pre
 
     e1 = layer(0, x)
@@ -146,18 +148,21 @@ def forward(theta, inp, exact=True):
     s2 = sub(e2)
     e3 = layer(2, s2)
     s3 = sub(e3)
-    e4 = layer(3, s3)
+    e4a = layer(3, s3)
+    e4b = layer(4, e4a)
+    e4 = layer(5, e4b)
     rup = None if exact else bf16
     c3 = np.concatenate([up(e4, rup), e3], axis=3)
-    d3 = layer(4, c3)
+    d3 = layer(6, c3)
     c2 = np.concatenate([up(d3, rup), e2], axis=3)
-    d2 = layer(5, c2)
+    d2 = layer(7, c2)
     c1 = np.concatenate([up(d2, rup), e1], axis=3)
-    d1 = layer(6, c1)
-    y = layer(7, d1)
+    d1 = layer(8, c1)
+    y = layer(9, d1)
     if not exact:
         y = f32(y)
-    cache.update(e1=e1, s1=s1, e2=e2, s2=s2, e3=e3, s3=s3, e4=e4, c3=c3, d3=d3, c2=c2, d2=d2, c1=c1, d1=d1)
+    cache.update(e1=e1, s1=s1, e2=e2, s2=s2, e3=e3, s3=s3, e4a=e4a, e4b=e4b, e4=e4, c3=c3, d3=d3, c2=c2, d2=d2,
+                 c1=c1, d1=d1)
     return y[..., 0], cache
 
 
@@ -166,11 +171,11 @@ def backward(cache, dout, exact=True):
     R = (lambda a: a) if exact else bf16
     F = (lambda a: a) if exact else f32
     P = cache["P"]
-    grads = [None] * 8
+    grads = [None] * len(LAYERS)
 
     def bwd(l, a_in, dpre):
         W, _ = P[l]
-        dx, dW, db = conv_bwd(a_in, W, dpre)
+        dx, dW, db = conv_bwd(a_in, W, dpre, LAYERS[l][4])
         grads[l] = (dW, db)
         return F(dx)
 
@@ -178,12 +183,14 @@ def backward(cache, dout, exact=True):
         return R(np.where(post > 0, g, 0.0))
 
     dy = R(np.asarray(dout, dtype=np.float64)[..., None])
-    g_d1 = bwd(7, cache["d1"], dy)
-    dc1 = bwd(6, cache["c1"], mask(cache["d1"], g_d1))
+    g_d1 = bwd(9, cache["d1"], dy)
+    dc1 = bwd(8, cache["c1"], mask(cache["d1"], g_d1))
     G1 = dc1.shape[1]
-    dc2 = bwd(5, cache["c2"], mask(cache["d2"], up_T(dc1[..., :32])))
-    dc3 = bwd(4, cache["c3"], mask(cache["d3"], up_T(dc2[..., :64])))
-    g_s3 = bwd(3, cache["s3"], mask(cache["e4"], up_T(dc3[..., :64])))
+    dc2 = bwd(7, cache["c2"], mask(cache["d2"], up_T(dc1[..., :32])))
+    dc3 = bwd(6, cache["c3"], mask(cache["d3"], up_T(dc2[..., :64])))
+    g_e4b = bwd(5, cache["e4b"], mask(cache["e4"], up_T(dc3[..., :64])))
+    g_e4a = bwd(4, cache["e4a"], mask(cache["e4b"], g_e4b))
+    g_s3 = bwd(3, cache["s3"], mask(cache["e4a"], g_e4a))
     G3 = dc3.shape[1]
     g_s2 = bwd(2, cache["s2"], mask(cache["e3"], dc3[..., 64:] + sub_T(g_s3, G3)))
     G2 = dc2.shape[1]

@@ -29,7 +29,7 @@ def _setup(torch, G, B, seed):
 def _layer_slices():
     out = []
     k = 0
-    for ci, co, _, _ in UO.LAYERS:
+    for ci, co, _, _, _ in UO.LAYERS:
         out.append(slice(k, k + co * 9 * ci))
         k += co * 9 * ci
         out.append(slice(k, k + co))

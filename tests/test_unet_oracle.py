@@ -31,7 +31,7 @@ def test_oracle_gradient_matches_finite_differences():
     # a few coordinates of every layer's weights and biases
     off = 0
     idx = []
-    for ci, co, _, _ in UO.LAYERS:
+    for ci, co, _, _, _ in UO.LAYERS:
         nw = co * 9 * ci
         idx += list(off + rng.choice(nw, 4, replace=False))
         idx += list(off + nw + rng.choice(co, min(co, 2), replace=False))
@@ -77,3 +77,26 @@ def test_bf16_rounding():
     assert r[0] == 1.0 and r[1] == 1.0          # tie -> even
     assert r[2] == 1.0 + 2 ** -7                 # above the tie -> up
     assert r[3] == -2.5 and r[4] == 0.0
+
+
+def test_dilated_conv_gradients():
+    """conv / conv_bwd with tap spacing 2 and 4 (the bottleneck layers): the data gradient is the
+    adjoint of the convolution, the weight gradient matches central differences."""
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((2, 11, 11, 3))
+    W = rng.standard_normal((4, 9, 3))
+    b = rng.standard_normal(4)
+    dy = rng.standard_normal((2, 11, 11, 4))
+    for dil in (1, 2, 4):
+        y = UO.conv(x, W, b, dil)
+        dx, dW, db = UO.conv_bwd(x, W, dy, dil)
+        # adjoint in x: <conv(x) - b, dy> = <x, dx>
+        assert np.isclose(np.sum((y - b) * dy), np.sum(x * dx))
+        assert np.allclose(db, dy.sum(axis=(0, 1, 2)))
+        for (o, t, c) in [(0, 0, 0), (3, 8, 2), (1, 4, 1), (2, 2, 0)]:
+            Wp = W.copy()
+            Wm = W.copy()
+            Wp[o, t, c] += 1e-6
+            Wm[o, t, c] -= 1e-6
+            fd = (np.sum(UO.conv(x, Wp, b, dil) * dy) - np.sum(UO.conv(x, Wm, b, dil) * dy)) / 2e-6
+            assert abs(fd - dW[o, t, c]) <= 1e-5 * max(1.0, abs(fd))
