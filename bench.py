@@ -44,6 +44,11 @@ WORKLOADS = {
     "poisson3d_l6_rhs64_mixed": (3, 6, "gauss64", "f32",
                                  "3D Poisson Q1 unit cube L6 (274,625 DOFs, 27-point), 64 right-hand sides of 8 "
                                  "Gaussians each (seeds 100..163), solved together, FP32 V(2,2) in FP64 PCG"),
+    "poisson2d_l9_warmstart": (2, 9, "family", "f32",
+                               "-div(kappa grad u)=f family at L9 (263,169 DOFs; kappa = exp(16x16-mode field), "
+                               "8-Gaussian f): U-Net on the 129^2 L7 grid trained on FP64-multigrid solutions, "
+                               "prediction prolongated as the PCG initial guess (zero-guess fallback), FP32 V(2,2) "
+                               "in FP64 PCG, stop at ||d|| <= 1e-8 ||b||; evaluated on unseen seeds"),
     "poisson2d_batch256_mixed": (2, 9, "batch", "f32",
                                  "256 independent -div(kappa grad u)=f instances, levels uniform in 5..9 (seed 7), "
                                  "kappa = exp(16x16-mode random field), 8-Gaussian RHS, one launch per V-cycle phase, "
@@ -179,6 +184,85 @@ class L2Flush:
         self.r.sum()
 
 
+def run_warmstart(args):
+    """Learned warm start (value = mean device ms per solve of the unseen instances, network
+    inference, prolongation and the fallback test included; assembly excluded).  Training data:
+    args.ws_train instances solved by the FP64 multigrid; evaluation: args.ws_eval unseen instances,
+    each solved from zero and from the network's start by the same mixed-precision solver."""
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    import featb200 as fb
+    from featb200.warmstart import ParametricFamily, WarmStart
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    t0 = time.time()
+    gen = ParametricFamily(level=9, net_level=7, precision="f64")
+    X, Y, its_train = gen.generate(range(0, args.ws_train))
+    t_gen = time.time() - t0
+    ws = WarmStart(gen, max_batch=32, seed=0)
+    t0 = time.time()
+    hist = ws.fit(X, Y, epochs=args.ws_epochs, batch=32, lr=3e-3)
+    torch.cuda.synchronize()
+    t_fit = time.time() - t0
+    del X, Y
+    fam = ParametricFamily(level=9, net_level=7, precision=precision)
+    ws.family = fam
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        out = fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        return out, ev0.elapsed_time(ev1)
+
+    ev = range(50_000, 50_000 + args.ws_eval)
+    # warm-up (untimed)
+    for k in range(40_000, 40_000 + args.warmup):
+        fam.setup(k)
+        fam.solve(torch.zeros(fam.n, dtype=torch.float64, device="cuda"))
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    wall0 = time.time()
+    l0 = fb.launch_count()
+    rows = []
+    for k in ev:
+        fam.setup(k)
+        x = torch.zeros(fam.n, dtype=torch.float64, device="cuda")
+        (st0, it0), ms0 = timed(lambda: fam.solve(x))
+
+        def warm():
+            x0, used, ratio = ws.initial_guess(k)
+            st, it = fam.solve(x0)
+            return x0, used, ratio, st, it
+        (x0, used, ratio, st1, it1), ms1 = timed(warm)
+        rows.append((it0, it1, ms0, ms1, used, float((x0 - x).norm() / x.norm()),
+                     st0 == fb.Status.success and st1 == fb.Status.success))
+    launches = fb.launch_count() - l0
+    wall1 = time.time()
+    time.sleep(0.3)
+    clk = clocks.stop(wall0, wall1)
+    a = np.array([r[:6] for r in rows], dtype=np.float64)
+    ms_warm = float(a[:, 3].mean())
+    print(json.dumps({"metric": METRIC, "value": ms_warm, "unit": "ms", "n_gpus": world, "steps": len(rows),
+                      "warmup": args.warmup, "ms_per_step": ms_warm, "higher_is_better": False, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f32+f64 (network bf16/f32)", "data": "synthetic",
+                      "config": {"workload": args.workload + ": " + desc, "dofs": fam.n, "train_instances": args.ws_train,
+                                 "epochs": args.ws_epochs, "eval_instances": len(rows), "network_grid": "129x129",
+                                 "l2": "not flushed (each step reassembles the instance first)"},
+                      "ms_zero_guess": float(a[:, 2].mean()), "iterations_zero": float(a[:, 0].mean()),
+                      "iterations_warm": float(a[:, 1].mean()), "network_used": float(a[:, 4].mean()),
+                      "max_rel_diff_warm_vs_zero": float(a[:, 5].max()), "all_success": all(r[6] for r in rows),
+                      "train_loss_last": float(hist[-1]), "generate_s": t_gen, "train_s": t_fit,
+                      "train_iterations_fp64": float(np.mean(its_train)),
+                      "gpu_launches": int(launches), "clocks": clk}))
+    return 0
+
+
 def run_multi(args, kind):
     """Secondary workloads: the 64-RHS 3D solve and the 256-instance batch (value = ms per solve of
     the whole set).  With N ranks the batch's instances are sharded by a longest-processing-time
@@ -278,7 +362,7 @@ def run_multi(args, kind):
     return 0
 
 
-def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900):
+def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900, field=None):
     """The reference's own CPU solver (oracle/_ref/feat_oracle, built from the reference's sources)
     on the same problem; returns its JSON summary with per-solve times (1 warm-up + reps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -287,12 +371,69 @@ def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900):
         return None
     from featb200 import assembly as AS
     with tempfile.TemporaryDirectory() as d:
-        params = None
+        params = kappa = None
         if gauss is not None:
             params = os.path.join(d, "gauss.txt")
             AS.write_params(params, gauss=gauss)
-        return O.feat_solve(d, dim=dim, level=level, rhs=rhs_kind, params=params, dump=False, time_reps=reps,
-                            timeout=timeout)
+        if field is not None:
+            kappa = os.path.join(d, "kappa.txt")
+            AS.write_params(kappa, field=field)
+        return O.feat_solve(d, dim=dim, level=level, rhs=rhs_kind, params=params, kappa=kappa, dump=False,
+                            time_reps=reps, timeout=timeout)
+
+
+def reference_sample(args):
+    """(ms per step, iterations, dofs, nnz, sample description) of the reference's CPU solver for
+    the workload, from a bounded sample (a few minutes at most)."""
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    from featb200 import assembly as AS
+    if rhs_kind in ("sine", "gauss"):
+        reps = max(1, min(args.warmup + args.steps, 40))
+        gauss = AS.gauss_params(1, dim) if rhs_kind == "gauss" else None
+        res = cpu_reference_times(dim, level, rhs_kind, gauss, reps)
+        if res is None:
+            return None
+        t = res["times_ms"]
+        return (float(np.mean(t)), res["iters"], res["dofs"], res["nnz"],
+                f"{len(t)} FP64 solves of the workload (after 1 warm-up) by the reference's generic "
+                "(single-threaded) backend, solve only")
+    if rhs_kind == "gauss64":
+        g = AS.gauss_params(100, 3, width=(0.03, 0.12))
+        res = cpu_reference_times(3, level, "gauss", g, 3)
+        if res is None:
+            return None
+        t = float(np.mean(res["times_ms"]))
+        return (64.0 * t, res["iters"], res["dofs"], res["nnz"],
+                "3 FP64 single right-hand-side solves of the 3D L6 problem (right-hand side 0 of the 64) by the "
+                "reference's generic backend, times 64 (the reference solves the columns one after the other)")
+    if rhs_kind == "batch":
+        levels = batch_levels(256)
+        per_level = {}
+        for L in sorted(set(levels)):
+            k = levels.index(L)
+            res = cpu_reference_times(2, L, "gauss", AS.gauss_params(10_000 + 2 * k, 2), 1,
+                                      field=AS.field_params(10_001 + 2 * k))
+            if res is None:
+                return None
+            per_level[L] = (float(res["times_ms"][-1]), res["iters"])
+        ms = float(sum(per_level[L][0] for L in levels))
+        return (ms, max(v[1] for v in per_level.values()), None, None,
+                "one instance per level 5..9 of the 256-instance batch solved by the reference's generic backend "
+                "(FP64, single-threaded, solve only); value = sum over the 256 instances of their level's time")
+    if rhs_kind == "family":
+        from featb200.warmstart import SEED_BASE
+        ts, its = [], []
+        for k in range(50_000, 50_004):
+            s0 = SEED_BASE + 2 * k
+            res = cpu_reference_times(2, level, "gauss", AS.gauss_params(s0, 2), 1, field=AS.field_params(s0 + 1))
+            if res is None:
+                return None
+            ts.append(float(res["times_ms"][-1]))
+            its.append(res["iters"])
+        return (float(np.mean(ts)), float(np.mean(its)), res["dofs"], res["nnz"],
+                "4 of the unseen instances solved from a zero guess by the reference's generic backend (FP64, "
+                "single-threaded, solve only; the reference has no learned start)")
+    return None
 
 
 def run_reference(args):
@@ -300,23 +441,18 @@ def run_reference(args):
     if rank != 0:
         return 0
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
-    from featb200 import assembly as AS
-    gauss = AS.gauss_params(1, dim) if rhs_kind == "gauss" else None
-    res = cpu_reference_times(dim, level, rhs_kind, gauss, args.warmup + args.steps)
+    res = reference_sample(args)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/feat_oracle (the reference built from "
                           "its sources) is missing; build it with `make -C oracle ref`"}))
         return 0
-    times = res["times_ms"][args.warmup:] if len(res["times_ms"]) > args.warmup else res["times_ms"]
-    ms = float(np.mean(times))
-    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": len(times),
+    ms, iters, dofs, nnz, sample = res
+    line = {"impl": "reference", "metric": METRIC, "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload + ": " + desc + " (the reference's CPU path is FP64 only)",
-                       "dofs": res["dofs"], "nnz": res["nnz"], "iterations": res["iters"]},
-            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference",
-                             "sample": f"{len(times)} FP64 solves of the workload by the reference's generic "
-                                       "(single-threaded) backend, solve only"},
+                       "dofs": dofs, "nnz": nnz, "iterations": iters},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -334,15 +470,20 @@ def main():
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
-    ap.add_argument("--tma-window", type=int, choices=[0, 1], default=1,
-                    help="stage each chunk's window of the gathered vector with the matrix (TMA passes)")
+    ap.add_argument("--tma-window", type=int, choices=[0, 1, 2], default=0,
+                    help="gathered-vector window of a TMA chunk: 2 prefetch into L2, 1 stage in shared memory, 0 none")
     ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
                     help="device DOF ordering (the generated problems are numbered lexicographically)")
+    ap.add_argument("--ws-train", type=int, default=20000, help="training instances (learned warm start)")
+    ap.add_argument("--ws-epochs", type=int, default=20)
+    ap.add_argument("--ws-eval", type=int, default=1000, help="unseen evaluation instances")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "poisson2d_l9_warmstart":
+        return run_warmstart(args)
     if args.workload in ("poisson2d_batch256_mixed", "poisson3d_l6_rhs64_mixed"):
         return run_multi(args, "batch" if "batch" in args.workload else "rhs64")
 

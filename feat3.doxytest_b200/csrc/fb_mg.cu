@@ -1063,12 +1063,15 @@ namespace fb
     template<typename VV, typename XS, class Op>
     void tma(const DevMat& m, const void* x, const Op& op)
     {
-      // the x window rides along when the stages still fit
+      // tma_window 1: the x window rides along in shared memory when the stages still fit;
+      // 2: it is bulk-prefetched into L2 three chunks ahead; 0: neither
       uint32_t xw = s->cfg.tma_window ? m.xwin : 0u;
-      if(xw && uint64_t(TMA_STAGES) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
-                 TMA_SMEM_MAX)
+      const int xstage = s->cfg.tma_window == 1 ? 1 : 0;
+      if(xw && xstage &&
+         uint64_t(TMA_STAGES) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
+           TMA_SMEM_MAX)
         xw = 0;
-      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + xw * uint32_t(sizeof(XS));
+      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + (xstage ? xw * uint32_t(sizeof(XS)) : 0u);
       const size_t smem = size_t(TMA_STAGES) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
@@ -1077,7 +1080,7 @@ namespace fb
       // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
       const uint32_t nxa = (m.cols + 8u) & ~3u;
       k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
-                                                        xw ? m.xlo : nullptr, xw, nxa, op, s->slot, s->err);
+                                                        xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
     }
     uint64_t launches = 0;
     double bytes = 0;
@@ -1509,7 +1512,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->rows_per_block = 0;
   c->tail_rows = 4096;
   c->tma_rows = 32768;
-  c->tma_window = 1;
+  c->tma_window = 0;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)

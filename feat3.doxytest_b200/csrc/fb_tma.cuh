@@ -104,11 +104,14 @@ namespace fb
   // sum_i = (A x)_i; op returns the row's contribution to an optional grid reduction, finished by
   // op.finish(total) in thread 0 of the last block.  padded_rows = the storage rows (a multiple of
   // 32); kst = the widest slice's entries per row (= A.kw for ELL), which sizes the stages.
-  // xlo != null: chunk c also stages x[xlo[c] .. xlo[c] + xw) (xw a multiple of 4 entries; the copy
-  // ends at nxa, the entries the vector's allocation holds, at the latest).
+  // xlo != null: chunk c reads only x[xlo[c] .. xlo[c] + xw) (xw a multiple of 4 entries; the range
+  // ends at nxa, the entries the vector's allocation holds, at the latest).  xstage != 0: that window
+  // is staged in shared memory with the chunk; xstage == 0: it is only bulk-prefetched into L2 when
+  // the chunk's copies are issued, so the gathers find it there.
   template<typename V, typename S, class Op>
   __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
-    uint32_t kst, const uint32_t* __restrict__ xlo, uint32_t xw, uint32_t nxa, Op op, RedSlot slot, int* err)
+    uint32_t kst, const uint32_t* __restrict__ xlo, uint32_t xw, uint32_t nxa, int xstage, Op op, RedSlot slot,
+    int* err)
   {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
@@ -119,7 +122,7 @@ namespace fb
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
     const uint32_t mb = tma_stage_bytes<V>(kst, narrow);
-    const uint32_t sb = mb + (xlo ? xw * uint32_t(sizeof(S)) : 0u);
+    const uint32_t sb = mb + (xlo && xstage ? xw * uint32_t(sizeof(S)) : 0u);
     const uint32_t nsl = padded_rows / 32u;
     const uint32_t nch = (padded_rows + TMA_NT - 1) / TMA_NT;
     auto issue = [&](uint32_t c, int s)
@@ -143,7 +146,14 @@ namespace fb
       if(xlo && ne)
       {
         x0 = __ldg(xlo + c);
-        xb = min(xw, nxa - x0) * uint32_t(sizeof(S));
+        const uint32_t bytes = min(xw, nxa - x0) * uint32_t(sizeof(S));
+        if(xstage)
+          xb = bytes;
+        else
+          for(uint32_t o = 0; o < bytes; o += 32768u)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(reinterpret_cast<const unsigned char*>(x + x0) + o), "r"(min(32768u, bytes - o))
+                         : "memory");
       }
       mbar_expect_tx(&bar[s], vb + cb + xb);
       if(ne == 0)
@@ -206,7 +216,7 @@ namespace fb
         }
         const S* sx = nullptr;
         uint32_t x0 = 0, xl = 0;
-        if(xlo)
+        if(xlo && xstage)
         {
           sx = reinterpret_cast<const S*>(st + mb);
           x0 = __ldg(xlo + c);

@@ -206,9 +206,10 @@ class PCG:
         """Uniform-width levels with at least `rows` rows use the TMA-staged passes (0 = off)."""
         self.cfg.tma_rows = int(rows)
 
-    def set_tma_window(self, flag):
-        """TMA-staged passes also stage each chunk's window of the gathered vector (default on)."""
-        self.cfg.tma_window = 1 if flag else 0
+    def set_tma_window(self, mode):
+        """Window of the gathered vector per TMA-staged chunk: 0 = neither (default), 1 = staged in
+        shared memory, 2 = prefetched into L2."""
+        self.cfg.tma_window = int(mode)
 
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""

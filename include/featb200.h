@@ -190,9 +190,10 @@ typedef struct
                            coarsest, run in one single-block kernel per V-cycle; 0 = off */
   int tma_rows;         /* levels with at least this many rows use the TMA-staged persistent
                            passes (bulk copies into shared memory); 0 = off */
-  int tma_window;       /* 1: the TMA-staged passes also stage each chunk's window of the gathered
-                           vector, so the row sums gather from shared memory; 0 = gather from
-                           global memory */
+  int tma_window;       /* the window of the gathered vector that a TMA-staged chunk reads:
+                           0 (default) = neither: the row sums gather from global memory;
+                           1 = staged in shared memory with the chunk; 2 = bulk-prefetched into L2
+                           when the chunk's copies are issued.  Both measured slower on B200 */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,

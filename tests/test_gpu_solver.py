@@ -151,10 +151,11 @@ def test_device_entry_point_and_launch_count(featlib, cuda):
 
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("precision", ["f64", "f32"])
-@pytest.mark.parametrize("window,ordering", [(1, "native"), (0, "native"), (1, "rcm")])
+@pytest.mark.parametrize("window,ordering", [(2, "native"), (1, "native"), (0, "native"), (1, "rcm"), (2, "rcm")])
 def test_tma_staged_passes_match(featlib, cuda, name, precision, window, ordering):
-    """The TMA-staged passes (bulk copies of matrix chunks, and with window=1 of each chunk's window
-    of the gathered vector, into shared memory) forced onto every level give the same results as
+    """The TMA-staged passes (bulk copies of matrix chunks into shared memory; window 1 also stages
+    each chunk's window of the gathered vector there, window 2 prefetches it into L2) forced onto
+    every level give the same results as
     the per-row kernels: bitwise V-cycles in FP64, identical iterations, solutions within rounding
     of the dot products."""
     fb = featlib
