@@ -27,7 +27,8 @@ namespace fb
 {
 namespace bt
 {
-  constexpr int BNT = 256;
+  constexpr int BNT = 256;       // block size of the PCG-space kernels
+  constexpr int BNT_MAX = 512;   // largest block size the autotuner may pick for the V-cycle passes
   constexpr int BW = BNT / 32;
   constexpr int MAXG = 16;
 
@@ -103,13 +104,13 @@ namespace bt
 
   // ---------------------------------------------------------------- V-cycle passes, level G
   template<typename V, typename S>
-  __global__ void __launch_bounds__(BNT) kb_smooth(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+  __global__ void __launch_bounds__(BNT_MAX) kb_smooth(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ xo, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ sinst,
     const int* __restrict__ skip, BScal sc)
   {
     if(closed(sc))
       return;
-    const uint32_t i = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= A.rows)
       return;
     const int j = __ldg(sinst + (i >> 5));
@@ -119,12 +120,12 @@ namespace bt
   }
 
   template<typename V, typename S>
-  __global__ void __launch_bounds__(BNT) kb_defect(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+  __global__ void __launch_bounds__(BNT_MAX) kb_defect(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ d, const uint8_t* __restrict__ dm, const int* __restrict__ sinst, BScal sc)
   {
     if(closed(sc))
       return;
-    const uint32_t i = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= A.rows)
       return;
     const int j = __ldg(sinst + (i >> 5));
@@ -135,13 +136,13 @@ namespace bt
 
   // coarse rows of level G-1: rows of instances whose top is G-1 are fed by their PCG: untouched
   template<typename V, typename S>
-  __global__ void __launch_bounds__(BNT) kb_restrict(DCsr<V> R, const S* __restrict__ d, S* __restrict__ bc,
+  __global__ void __launch_bounds__(BNT_MAX) kb_restrict(DCsr<V> R, const S* __restrict__ d, S* __restrict__ bc,
     S* __restrict__ xc, const S* __restrict__ dinvc, const uint8_t* __restrict__ dmc, const int* __restrict__ sinstc,
     int gc, int* __restrict__ skipc, BScal sc)
   {
     if(closed(sc))
       return;
-    const uint32_t jr = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t jr = blockIdx.x * blockDim.x + threadIdx.x;
     int inst = -1;
     double sq = 0.0;
     if(jr < R.rows || (jr & ~31u) < R.rows)
@@ -181,12 +182,12 @@ namespace bt
   }
 
   template<typename V, typename S>
-  __global__ void __launch_bounds__(BNT) kb_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ x,
+  __global__ void __launch_bounds__(BNT_MAX) kb_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ x,
     const uint8_t* __restrict__ dm, const int* __restrict__ sinst, BScal sc)
   {
     if(closed(sc))
       return;
-    const uint32_t i = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if(i >= P.rows)
       return;
     const int j = __ldg(sinst + (i >> 5));
@@ -196,13 +197,13 @@ namespace bt
   }
 
   template<typename V, typename S>
-  __global__ void __launch_bounds__(BNT) kb_post1(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
+  __global__ void __launch_bounds__(BNT_MAX) kb_post1(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ d, S* __restrict__ c, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
     const int* __restrict__ sinst, int* __restrict__ skip, BScal sc)
   {
     if(closed(sc))
       return;
-    const uint32_t i = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int inst = -1;
     double sq = 0.0;
     if((i & ~31u) < A.rows)
@@ -225,7 +226,7 @@ namespace bt
   // post-smoothing step k >= 2 at level g; LAST: instances whose top is g write z (PCG space) and
   // r.z -> gamma, beta; the others update x
   template<typename V, typename S, bool LAST>
-  __global__ void __launch_bounds__(BNT) kb_post2(DCsr<V> A, const S* __restrict__ d, const S* __restrict__ c,
+  __global__ void __launch_bounds__(BNT_MAX) kb_post2(DCsr<V> A, const S* __restrict__ d, const S* __restrict__ c,
     S* __restrict__ co, S* __restrict__ x, double* __restrict__ z, const double* __restrict__ r,
     const int* __restrict__ pcg_base, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
     const int* __restrict__ sinst, int g, const int* __restrict__ skip, BScal sc)
@@ -233,7 +234,7 @@ namespace bt
     typedef typename ValueTraits<V>::acc Ac;
     if(closed(sc))
       return;
-    const uint32_t i = blockIdx.x * BNT + threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int inst = -1;
     double rz = 0.0;
     if((i & ~31u) < A.rows)
@@ -545,6 +546,7 @@ struct fb_batch
     int* sinst = nullptr;
     int* pcg_base = nullptr;
     std::vector<uint32_t> off;   // per instance row offset (UINT32_MAX: absent)
+    int bs = 256;                // rows per block of this level's V-cycle passes (autotuned)
   };
   fb_solver_config cfg;
   int J = 0, NG = 0;
@@ -664,6 +666,7 @@ namespace bt
   }
 
   static unsigned int nblk(uint32_t n) { return std::max(1u, (n + BNT - 1) / BNT); }
+  static unsigned int nblk(uint32_t n, int bs) { return std::max(1u, (n + uint32_t(bs) - 1) / uint32_t(bs)); }
 
   template<typename V, typename S>
   struct BLaunch
@@ -708,7 +711,7 @@ namespace bt
         for(int k = 1; k < steps; ++k)
         {
           if(!dry)
-            kb_smooth<V, S><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+            kb_smooth<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
               (const S*)f.dinv, f.dm, f.sinst, skp, sc);
           ++launches;
           bytes += cb(f.A, 3, 1);
@@ -716,11 +719,11 @@ namespace bt
         }
         xcur[size_t(G)] = xa;
         if(!dry)
-          kb_defect<V, S><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm,
+          kb_defect<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm,
             f.sinst, sc);
         const bool coarsest = (G - 1 == 0);
         if(!dry)
-          kb_restrict<V, S><<<nblk(c.n), BNT, 0, st>>>(bview<V>(f.R), (const S*)f.d, (S*)c.b,
+          kb_restrict<V, S><<<nblk(c.n, c.bs), c.bs, 0, st>>>(bview<V>(f.R), (const S*)f.d, (S*)c.b,
             coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.sinst, G - 1,
             sc.skip_pre + size_t(G - 1) * sc.J, sc);
         launches += 2;
@@ -742,9 +745,9 @@ namespace bt
         int* skq = sc.skip_post + size_t(G) * sc.J;
         if(!dry)
         {
-          kb_prolong<V, S><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.P), (const S*)xcur[size_t(G - 1)], (S*)xf, f.dm,
+          kb_prolong<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.P), (const S*)xcur[size_t(G - 1)], (S*)xf, f.dm,
             f.sinst, sc);
-          kb_post1<V, S><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+          kb_post1<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
             (const S*)f.dinv, f.dm, f.sinst, skq, sc);
         }
         launches += 2;
@@ -757,10 +760,10 @@ namespace bt
           if(dry)
             ;
           else if(last)
-            kb_post2<V, S, true><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cbuf,
+            kb_post2<V, S, true><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cbuf,
               (S*)xf, s->z, s->r, f.pcg_base, (const S*)f.dinv, f.dm, f.sinst, G, skq, sc);
           else
-            kb_post2<V, S, false><<<nblk(f.n), BNT, 0, st>>>(bview<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cbuf,
+            kb_post2<V, S, false><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cbuf,
               (S*)xf, s->z, s->r, f.pcg_base, (const S*)f.dinv, f.dm, f.sinst, G, skq, sc);
           ++launches;
           bytes += cb(f.A, 3, 1);
@@ -802,10 +805,67 @@ namespace bt
     }
   };
 
+  // Autotuner: for every global level, the rows per block of its V-cycle passes (64 .. 512, i.e.
+  // 2 .. 16 warps of 32 rows) that runs the level's defect pass fastest over all instances present
+  // (median of 5 timed launches after 2 untimed ones; the pass writes only the level's defect
+  // buffer, which the solve overwrites).  Small levels favour small blocks (more SMs busy), large
+  // levels larger ones.
+  template<typename V, typename S>
+  static fb_status autotune(fb_batch* s)
+  {
+    cudaStream_t st = s->stream;
+    BScal sc = s->sc;
+    kb_open<<<4, 256, 0, st>>>(sc);
+    FB_LAUNCHED(1);
+    const int cand[4] = {64, 128, 256, 512};
+    for(int G = 1; G < s->NG; ++G)
+    {
+      fb_batch::GLevel& f = s->g[size_t(G)];
+      float best = 1e30f;
+      int pick = 256;
+      for(int bs : cand)
+      {
+        float t[5];
+        for(int r = 0; r < 7; ++r)
+        {
+          FB_CUDA(cudaEventRecord(s->ev0, st));
+          kb_defect<V, S><<<nblk(f.n, bs), bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)f.x, (S*)f.d, f.dm,
+            f.sinst, sc);
+          FB_CUDA(cudaEventRecord(s->ev1, st));
+          FB_CUDA(cudaEventSynchronize(s->ev1));
+          float ms = 0.f;
+          FB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+          if(r >= 2)
+            t[r - 2] = ms;
+        }
+        FB_LAUNCHED(7);
+        std::sort(t, t + 5);
+        if(t[2] < best * 0.97f)   // a candidate must win by 3% to replace a smaller block size
+        {
+          best = t[2];
+          pick = bs;
+        }
+      }
+      f.bs = pick;
+    }
+    s->g[0].bs = s->NG > 1 ? s->g[1].bs : 256;
+    FB_CUDA(cudaStreamSynchronize(st));
+    return FB_OK;
+  }
+
   template<typename V, typename S>
   static fb_status build(fb_batch* s)
   {
     cudaStream_t st = s->stream;
+    if(s->cfg.rows_per_block > 0)
+      for(auto& g : s->g)
+        g.bs = std::max(32, std::min(BNT_MAX, (s->cfg.rows_per_block + 31) / 32 * 32));
+    else
+    {
+      const fb_status e = autotune<V, S>(s);
+      if(e != FB_OK)
+        return e;
+    }
     {
       BLaunch<V, S> a{s, st, true};
       a.init();
@@ -915,6 +975,20 @@ void fb_batch_destroy(fb_batch* s)
   for(void* p : s->allocs)
     cudaFree(p);
   delete s;
+}
+
+fb_status fb_batch_rows_per_block(const fb_batch* b, int* rows_per_block, int* num_levels)
+{
+  if(!b || !num_levels)
+  {
+    set_error("batch_rows_per_block: bad arguments");
+    return FB_ERR_ARG;
+  }
+  *num_levels = b->NG;
+  if(rows_per_block)
+    for(int G = 0; G < b->NG; ++G)
+      rows_per_block[G] = b->g[size_t(b->NG - 1 - G)].bs;
+  return FB_OK;
 }
 
 fb_status fb_batch_create(fb_batch** out, int num, fb_hierarchy* const* hs, const fb_solver_config* cfg_in)

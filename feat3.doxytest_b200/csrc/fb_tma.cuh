@@ -187,11 +187,24 @@ namespace fb
     {
       const int s = int(it % TMA_STAGES);
       const uint32_t par = (it / TMA_STAGES) & 1u;
-      const bool ok = mbar_wait(&bar[s], par);
+      // one warp polls the barrier; the others wait in __syncthreads without taking issue slots
+      bool ok = true;
+      if(threadIdx.x < 32)
+        ok = mbar_wait(&bar[s], par);
       if(__syncthreads_or(!ok))   // the whole block leaves together
       {
         failed = true;
         break;
+      }
+      // every thread is past the previous chunk: refill its stage (TMA_STAGES - 1 chunks ahead)
+      if(threadIdx.x == 0 && it > 0)
+      {
+        const uint32_t c2 = c - gridDim.x + uint32_t(TMA_STAGES) * gridDim.x;
+        if(c2 < nch)
+        {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue(c2, int((it - 1) % TMA_STAGES));
+        }
       }
       const unsigned char* st = tma_smem + size_t(s) * sb;
       const V* sv = reinterpret_cast<const V*>(st);
@@ -226,16 +239,6 @@ namespace fb
           narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), kr, base, i, x, sx, x0, xl);
         part += op(i, sum, pre);
       }
-      __syncthreads();   // every thread is done with stage s
-      if(threadIdx.x == 0)
-      {
-        const uint32_t c2 = c + uint32_t(TMA_STAGES) * gridDim.x;
-        if(c2 < nch)
-        {
-          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue(c2, s);
-        }
-      }
     }
     if(failed)
     {
@@ -244,7 +247,9 @@ namespace fb
       if(threadIdx.x == 0)
       {
         atomicOr(err, 1);
-        for(uint32_t k = 0; k < uint32_t(TMA_STAGES); ++k)
+        // copies in flight: chunks it .. it + TMA_STAGES - 1 before the first refill, then one fewer
+        const uint32_t pending = it == 0 ? uint32_t(TMA_STAGES) : uint32_t(TMA_STAGES) - 1u;
+        for(uint32_t k = 0; k < pending; ++k)
         {
           const uint32_t jt = it + k;
           const uint32_t c = blockIdx.x + jt * gridDim.x;

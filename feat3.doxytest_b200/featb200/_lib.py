@@ -113,6 +113,7 @@ _PROTOS = {
     "fb_batch_sizes": (I, [P, P]),
     "fb_batch_solve": (I, [P, P, P, P]),
     "fb_batch_solve_device": (I, [P, P, P, P, P]),
+    "fb_batch_rows_per_block": (I, [P, P, C.POINTER(I)]),
 }
 
 _lib = None

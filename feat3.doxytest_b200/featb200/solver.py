@@ -429,7 +429,7 @@ class BatchPCG:
     packed: the instances' fine-level vectors concatenated in order."""
 
     def __init__(self, hierarchies, tol_rel=1e-8, max_iter=100, precision="f64", ordering="native",
-                 use_graph=True):
+                 use_graph=True, rows_per_block=0):
         omega, steps = hierarchies[0].smoother_params()
         for h in hierarchies:
             if h.smoother_params() != (omega, steps):
@@ -444,6 +444,7 @@ class BatchPCG:
         self.cfg.tol_rel, self.cfg.max_iter = float(tol_rel), int(max_iter)
         self.cfg.precision, self.cfg.ordering = _lib.PREC[precision], _lib.ORDER[ordering]
         self.cfg.use_graph = 1 if use_graph else 0
+        self.cfg.rows_per_block = int(rows_per_block)
         arr = (C.c_void_p * self.j)(*[h._h.value for h in self.hierarchies])
         s = C.c_void_p()
         _lib.check(_lib.lib().fb_batch_create(C.byref(s), self.j, arr, C.byref(self.cfg)), "fb_batch_create")
@@ -453,6 +454,16 @@ class BatchPCG:
         self.sizes = sizes.astype(np.int64)
         self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
         self.info = (_lib.SolveInfo * self.j)()
+
+    def rows_per_block(self):
+        """Rows per block of the V-cycle passes per global level, finest first (autotuned unless
+        given at construction)."""
+        n = C.c_int(0)
+        _lib.check(_lib.lib().fb_batch_rows_per_block(self._s, None, C.byref(n)), "fb_batch_rows_per_block")
+        out = np.zeros(n.value, dtype=np.int32)
+        _lib.check(_lib.lib().fb_batch_rows_per_block(self._s, out.ctypes.data_as(C.c_void_p), C.byref(n)),
+                   "fb_batch_rows_per_block")
+        return out
 
     def solve(self, sol, rhs):
         """sol (initial guesses, overwritten) and rhs: packed float64 arrays."""

@@ -116,3 +116,28 @@ class UNet:
         self.backward(g, stream=stream)
         self.adam(lr, stream=stream)
         return loss
+
+
+def _main():
+    """A few training steps on random data (for profiling the network kernels):
+    python -m featb200.unet --grid 129 --batch 32 --steps 5"""
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", type=int, default=129)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--steps", type=int, default=5)
+    a = ap.parse_args()
+    net = UNet(a.grid, a.batch, seed=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((a.batch, 2, a.grid, a.grid), device="cuda", generator=g)
+    t = torch.randn((a.batch, a.grid, a.grid), device="cuda", generator=g)
+    buf = torch.empty_like(t)
+    for _ in range(a.steps):
+        loss = net.train_step(x, t, 1e-3, buf)
+    torch.cuda.synchronize()
+    print({"loss": float(loss.item()), "steps": a.steps})
+
+
+if __name__ == "__main__":
+    _main()

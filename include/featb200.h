@@ -185,7 +185,8 @@ typedef struct
   int max_iter;         /* PCG max_iter (default 100) */
   int min_iter;         /* PCG min_iter (default 0) */
   int use_graph;        /* capture the whole solve in one CUDA graph (1) or launch per kernel (0) */
-  int rows_per_block;   /* CSR kernel rows per block, 0 = autotuned */
+  int rows_per_block;   /* batch solver: rows (threads) per block of the V-cycle passes, a multiple
+                           of 32 up to 512; 0 = picked per level by the autotuner at creation */
   int tail_rows;        /* levels (below the finest) with at most this many rows, down to the
                            coarsest, run in one single-block kernel per V-cycle; 0 = off */
   int tma_rows;         /* levels with at least this many rows use the TMA-staged persistent
@@ -304,6 +305,10 @@ fb_status fb_batch_sizes(const fb_batch* b, uint64_t* top_rows);
 fb_status fb_batch_solve(fb_batch* b, double* sol, const double* rhs, fb_solve_info* info);
 /* As fb_batch_solve with DEVICE packed arrays, ordered on `stream`. */
 fb_status fb_batch_solve_device(fb_batch* b, double* sol, const double* rhs, void* stream, fb_solve_info* info);
+/* Rows per block of the V-cycle passes per global level (finest first; rows_per_block may be NULL to
+ * query num_levels): the autotuner's choice at creation, or cfg.rows_per_block.  No counterpart in
+ * the reference. */
+fb_status fb_batch_rows_per_block(const fb_batch* b, int* rows_per_block, int* num_levels);
 
 /* ------------------------------------------------------------------------------------------ */
 /* 5. Set-up on the device: Q1 assembly on the uniformly refined unit square                    */

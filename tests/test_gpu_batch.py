@@ -80,3 +80,28 @@ def test_batch_converged_instances_stop(featlib, cuda):
     X = bat.split(bat.solve(np.zeros_like(rhs), rhs))
     assert bat.iterations()[0] == 0 and np.all(X[0] == 0)
     assert bat.statuses()[1] == fb.Status.success and bat.iterations()[1] > 0
+
+
+@pytest.mark.parametrize("rows_per_block", [0, 64, 512])
+def test_batch_rows_per_block(featlib, cuda, rows_per_block):
+    """The autotuner (0) picks a block size per level from 64..512; any choice gives the same
+    iterations and solutions as the single-system solves (block sizes change only which threads
+    run which rows)."""
+    fb = featlib
+    inst = _family([5, 7, 3, 6], seed0=500)
+    hs = [fb.build_hierarchy(lv) for lv, _ in inst]
+    bat = fb.BatchPCG(hs, rows_per_block=rows_per_block)
+    rpb = bat.rows_per_block()
+    assert len(rpb) == 7
+    if rows_per_block:
+        assert np.all(rpb == rows_per_block)
+    else:
+        assert set(rpb.tolist()) <= {64, 128, 256, 512}
+    rhs = np.concatenate([b for _, b in inst])
+    X = bat.split(bat.solve(np.zeros_like(rhs), rhs))
+    for k, (lv, b) in enumerate(inst):
+        s = fb.build_pcg_multigrid(lv)
+        x = fb.DenseVector(b.size)
+        assert fb.solve(s, x, fb.DenseVector(b)) == fb.Status.success
+        assert bat.iterations()[k] == s.get_num_iter()
+        assert rel_err(X[k], x.elements) <= 1e-12
