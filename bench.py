@@ -56,6 +56,10 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
 
+# DRAM bytes of one launch of the roofline kernel, from one ncu capture (summarised in profiles/):
+# (workload, ordering) -> bytes read + written
+MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.057856e6 + 4.222464e6}
+
 
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
@@ -632,7 +636,10 @@ def main():
                            "iterations": int(np.median(iters))},
                 "spmv_gbs": spmv_gbs, "rel_residual": rel_res,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None, "kernel": "k_pcg_q (FP64 CSR SpMV + q.p)",
+                             "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get((args.workload, args.ordering)),
+                             "traffic_source": "profiles/k_tma_pass_OpPcgQ_l10_f64.md (ncu dram__bytes_read.sum + "
+                                               "dram__bytes_write.sum of one launch)",
+                             "kernel": "k_tma_pass<OpPcgQ> (FP64 CSR SpMV + q.p, TMA-staged)",
                              "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": by_k,
                              "launch_ms": ms_k},
                 "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(2 * 8 * n),

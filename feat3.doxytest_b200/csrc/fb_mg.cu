@@ -1079,8 +1079,13 @@ namespace fb
       const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
       // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
       const uint32_t nxa = (m.cols + 8u) & ~3u;
-      k_tma_pass<VV, XS, Op><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
-                                                        xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
+      // the 2D Q1 stencil (ELL of width 9) runs the fully unrolled row sum
+      if(m.kw == 9)
+        k_tma_pass<VV, XS, Op, 9><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
+                                                             xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
+      else
+        k_tma_pass<VV, XS, Op, 0><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
+                                                             xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
     }
     uint64_t launches = 0;
     double bytes = 0;
@@ -1369,15 +1374,24 @@ namespace fb
   static fb_status set_tma_attrs()
   {
     const int mx = int(TMA_SMEM_MAX) + 8 * 1024;
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpSmooth<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpDefect<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost1<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, false, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, false>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, true>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpRestrict<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpProlong<V, S>>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpSmooth<V, S>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpSmooth<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpDefect<V, S>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpDefect<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost1<V, S>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost1<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, false, false>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, false, false>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, false>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, false>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, true>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpPost2<V, S, true, true>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpRestrict<V, S>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpRestrict<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpProlong<V, S>, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpProlong<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tail<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     return FB_OK;
   }

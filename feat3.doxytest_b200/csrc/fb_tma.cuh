@@ -60,12 +60,36 @@ namespace fb
   // row sum of a staged row with K entries, entry k at base + 32*k, in stored order; the column
   // is absolute or row-relative.  With a staged window sx of x[x0 .. x0 + xl), the gathers read
   // shared memory; a column outside the window is the zero slot of a padding entry (x = 0).
-  template<typename V, typename S>
+  // KC > 0: every row of the matrix has exactly KC slots (ELL of width KC), so the loop is fully
+  // unrolled without width tests.
+  template<typename V, typename S, int KC = 0>
   __device__ __forceinline__ typename ValueTraits<V>::acc staged_row_sum(const V* sv, const int16_t* sd,
     const uint32_t* sc, uint32_t K, uint32_t base, uint32_t row, const S* __restrict__ x, const S* sx,
     uint32_t x0, uint32_t xl)
   {
     typedef typename ValueTraits<V>::acc A;
+    if(KC > 0)
+    {
+      A xv[KC > 0 ? KC : 1];
+      #pragma unroll
+      for(int u = 0; u < KC; ++u)
+      {
+        const uint32_t e = base + uint32_t(u) * 32u;
+        const uint32_t c = sd ? uint32_t(int32_t(row) + int32_t(sd[e])) : sc[e];
+        if(sx)
+        {
+          const uint32_t o = c - x0;
+          xv[u] = o < xl ? A(sx[o]) : A(0);
+        }
+        else
+          xv[u] = A(__ldg(x + c));
+      }
+      A s = A(0);
+      #pragma unroll
+      for(int u = 0; u < KC; ++u)
+        s = add(s, mul(to_acc(sv[base + uint32_t(u) * 32u]), xv[u]));
+      return s;
+    }
     constexpr uint32_t U = 9;
     A sum = A(0);
     for(uint32_t k0 = 0; k0 < K; k0 += U)
@@ -108,7 +132,7 @@ namespace fb
   // ends at nxa, the entries the vector's allocation holds, at the latest).  xstage != 0: that window
   // is staged in shared memory with the chunk; xstage == 0: it is only bulk-prefetched into L2 when
   // the chunk's copies are issued, so the gathers find it there.
-  template<typename V, typename S, class Op>
+  template<typename V, typename S, class Op, int KC = 0>
   __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
     uint32_t kst, const uint32_t* __restrict__ xlo, uint32_t xw, uint32_t nxa, int xstage, Op op, RedSlot slot,
     int* err)
@@ -235,7 +259,7 @@ namespace fb
           x0 = __ldg(xlo + c);
           xl = min(xw, nxa - x0);
         }
-        const auto sum = staged_row_sum<V, S>(sv, narrow ? reinterpret_cast<const int16_t*>(scol) : nullptr,
+        const auto sum = staged_row_sum<V, S, KC>(sv, narrow ? reinterpret_cast<const int16_t*>(scol) : nullptr,
           narrow ? nullptr : reinterpret_cast<const uint32_t*>(scol), kr, base, i, x, sx, x0, xl);
         part += op(i, sum, pre);
       }
