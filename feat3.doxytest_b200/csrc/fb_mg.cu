@@ -599,6 +599,161 @@ namespace fb
     }
   }
 
+  // ------------------------------------------------------------------ cluster tail
+  // The same V-cycle bottom as k_tail, spread over a thread-block cluster of CT_CS blocks (one per
+  // SM) so that larger levels fit: rows are dealt out cluster-wide, the passes are separated by the
+  // cluster's hardware barrier (release/acquire at cluster scope, so every block sees the vectors
+  // the others wrote), and the skip-test norms are summed from per-block partials in block order
+  // (deterministic).  The vectors stay in global memory (L2).
+  constexpr int CT_NT = 512;
+  constexpr int CT_CS = 8;
+
+  __device__ __forceinline__ void cluster_sync_all()
+  {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
+  __device__ __forceinline__ uint32_t cluster_rank()
+  {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+  }
+
+  // cluster-wide sum of one value per thread; `slot` selects this reduction's partials in red[]
+  __device__ __forceinline__ double cluster_sum(double v, double* sh, double* __restrict__ red, int slot,
+    uint32_t rank)
+  {
+    const double b = block_sum<CT_NT>(v, sh);
+    if(threadIdx.x == 0)
+      red[slot * CT_CS + int(rank)] = b;
+    cluster_sync_all();
+    double t = 0.0;
+    #pragma unroll
+    for(int r = 0; r < CT_CS; ++r)
+      t += *(volatile double*)(red + slot * CT_CS + r);
+    return t;
+  }
+
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(CT_NT) k_ctail(const __grid_constant__ TailParams<V, S> tp,
+    const Scalars* __restrict__ sc, double* __restrict__ red)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    __shared__ int skip_pre_sh[MAX_TAIL];
+    if(gate_closed(sc))   // the same answer in every block: the gate changes between launches only
+      return;
+    const uint32_t rank = cluster_rank();
+    const uint32_t gt = rank * CT_NT + threadIdx.x;
+    constexpr uint32_t GT = uint32_t(CT_CS) * CT_NT;
+    // matrix data of all tail levels towards L2: chunk q of the flattened list by thread q % GT
+    {
+      uint32_t g = 0;
+      for(int r = 0; r < tp.npf; ++r)
+      {
+        const uint32_t nb = tp.pf_bytes[r];
+        for(uint32_t off = 0; off < nb; off += TAIL_PF_CHUNK, ++g)
+          if(g % GT == gt)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(static_cast<const unsigned char*>(tp.pf_ptr[r]) + off),
+                            "r"(min(TAIL_PF_CHUNK, nb - off)) : "memory");
+      }
+    }
+    const int cnt = tp.count;
+    const int steps = tp.steps;
+    if(threadIdx.x == 0)
+      skip_pre_sh[0] = *(volatile int*)tp.lv[0].skip_pre;
+    __syncthreads();
+    int xsel[MAX_TAIL];
+    int slot = 0;
+    for(int t = 0; t + 1 < cnt; ++t)
+    {
+      const TailLevel<V, S>& f = tp.lv[t];
+      const TailLevel<V, S>& c = tp.lv[t + 1];
+      const S* fb = f.b;
+      S* xa = f.x;
+      S* xb = f.x2;
+      int sel = 1;
+      const bool skipped = skip_pre_sh[t] != 0;
+      for(int k = 1; k < steps; ++k)
+      {
+        for(uint32_t i = gt; i < f.n; i += GT)
+          xb[i] = smooth_row<V, S, false>(f.A, fb, xa, f.dinv, f.dm, skipped, i);
+        cluster_sync_all();
+        S* tmp = xa;
+        xa = xb;
+        xb = tmp;
+        sel = 3 - sel;
+      }
+      xsel[t] = sel;
+      for(uint32_t i = gt; i < f.n; i += GT)
+        f.d[i] = defect_row<V, S, false>(f.A, fb, xa, f.dm, i);
+      cluster_sync_all();
+      const bool coarsest = (t + 2 == cnt);
+      double sq = 0.0;
+      for(uint32_t j = gt; j < c.n; j += GT)
+        sq += restrict_row<V, S, false>(f.R, f.d, c.b, coarsest ? (S*)nullptr : c.x, c.dinv, c.dm, j);
+      const double tot = cluster_sum(sq, sh, red, slot++, rank);
+      if(threadIdx.x == 0)
+      {
+        const int sk = skip_from_norm<S>(sqrt(tot));
+        skip_pre_sh[t + 1] = sk;
+        if(!coarsest && rank == 0)
+          *(volatile int*)c.skip_pre = sk;
+      }
+      __syncthreads();
+    }
+    {
+      const TailLevel<V, S>& c = tp.lv[cnt - 1];
+      if(rank == 0)
+        coarse_block<S, CT_NT>(c.b, c.x, c.n, tp.free_dofs, tp.inv, tp.m);
+      xsel[cnt - 1] = 1;
+      cluster_sync_all();
+    }
+    for(int t = cnt - 2; t >= 0; --t)
+    {
+      const TailLevel<V, S>& f = tp.lv[t];
+      S* xf = xsel[t] == 1 ? f.x : f.x2;
+      const TailLevel<V, S>& cl = tp.lv[t + 1];
+      const S* xc = xsel[t + 1] == 1 ? cl.x : cl.x2;
+      for(uint32_t i = gt; i < f.n; i += GT)
+        xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
+      cluster_sync_all();
+      S* ca = f.c;
+      S* cb = f.c2;
+      double sq = 0.0;
+      for(uint32_t i = gt; i < f.n; i += GT)
+        sq += post1_row<V, S, false>(f.A, f.b, xf, f.d, ca, f.dinv, f.dm, i);
+      const double tot = cluster_sum(sq, sh, red, slot++, rank);
+      const int sk = skip_from_norm<S>(sqrt(tot));
+      if(threadIdx.x == 0 && rank == 0)
+        *(volatile int*)f.skip_post = sk;
+      const bool skipped = sk != 0;
+      if(steps == 1)
+      {
+        for(uint32_t i = gt; i < f.n; i += GT)
+          xf[i] = S(add(Ac(xf[i]), skipped ? Ac(0) : Ac(ca[i])));
+        cluster_sync_all();
+      }
+      for(int k = 2; k <= steps; ++k)
+      {
+        const bool last = (k == steps);
+        for(uint32_t i = gt; i < f.n; i += GT)
+        {
+          const Ac cn = post2_row<V, S, false>(f.A, f.d, ca, f.dinv, f.dm, skipped, i);
+          if(last)
+            xf[i] = S(add(Ac(xf[i]), cn));
+          else
+            cb[i] = S(cn);
+        }
+        cluster_sync_all();
+        S* tmp = ca;
+        ca = cb;
+        cb = tmp;
+      }
+    }
+  }
+
   // ------------------------------------------------------------------ PCG passes (FP64)
   // writes the V-cycle input of the top level: b = S(r * scale) (FP32 modes) and
   // sol1 = F(D .* b); returns the scale used.
@@ -883,6 +1038,9 @@ struct fb_solver
   cudaGraphExec_t vexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
+  int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
+  double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
+  cudaError_t launch_err = cudaSuccess;
   int nsm = 148;          // streaming multiprocessors of the device
   int* err = nullptr;     // device error word (bounded waits that expired)
   uint64_t launches_init = 0, launches_body = 0, launches_vcycle = 0;
@@ -1102,11 +1260,11 @@ namespace fb
     // Shared-memory placement of the tail's vectors (coarsest level first, while the levels fit)
     // and the L2 prefetch list of its matrices, diagonals and masks; returns the dynamic shared
     // memory size.
-    size_t tail_layout(TailParams<V, S>& tp, int lt)
+    size_t tail_layout(TailParams<V, S>& tp, int lt, bool use_smem)
     {
       const int nl = s->nlev;
       uint32_t used = 0;
-      for(int l = nl - 1; l >= lt; --l)
+      for(int l = nl - 1; l >= lt && use_smem; --l)
       {
         TailLevel<V, S>& t = tp.lv[l - lt];
         const uint32_t np = (t.n + 7u) & ~7u;
@@ -1159,7 +1317,9 @@ namespace fb
     {
       const int nl = s->nlev;
       const int steps = std::max(1, s->cfg.smooth_steps);
-      const int lt = s->tail_first;   // first level of the single-block tail, -1 = none
+      // first level of the tail (cluster kernel or single-block kernel), -1 = none
+      const bool ctail = s->ctail_first >= 0;
+      const int lt = ctail ? s->ctail_first : s->tail_first;
       std::vector<void*> xcur(static_cast<size_t>(nl));
       for(int l = 0; l + 1 < nl; ++l)
       {
@@ -1237,9 +1397,30 @@ namespace fb
           if(l + 1 < nl)
             bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
         }
-        const size_t smem = tail_layout(tp, lt);
+        const size_t smem = tail_layout(tp, lt, !ctail);
         bytes += double(s->nfree) * s->nfree * 8.0;
-        if(!dry) k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
+        if(dry)
+          ;
+        else if(ctail)
+        {
+          cudaLaunchConfig_t lc = {};
+          lc.gridDim = dim3(CT_CS, 1, 1);
+          lc.blockDim = dim3(CT_NT, 1, 1);
+          lc.dynamicSmemBytes = 0;
+          lc.stream = st;
+          cudaLaunchAttribute at[1];
+          at[0].id = cudaLaunchAttributeClusterDimension;
+          at[0].val.clusterDim.x = CT_CS;
+          at[0].val.clusterDim.y = 1;
+          at[0].val.clusterDim.z = 1;
+          lc.attrs = at;
+          lc.numAttrs = 1;
+          const cudaError_t e = cudaLaunchKernelEx(&lc, k_ctail<V, S>, tp, (const Scalars*)s->sc, s->cred);
+          if(e != cudaSuccess && s->launch_err == cudaSuccess)
+            s->launch_err = e;
+        }
+        else
+          k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
         ++launches;
       }
       else
@@ -1525,6 +1706,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->use_graph = 1;
   c->rows_per_block = 0;
   c->tail_rows = 4096;
+  c->cluster_rows = 0;
   c->tma_rows = 32768;
   c->tma_window = 0;
 }
@@ -1744,7 +1926,17 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   // the tail starts at the first level (below the top) with at most tail_rows rows, if it has a
   // coarser level below it
   s->tail_first = -1;
-  if(cfg.tail_rows > 0)
+  s->ctail_first = -1;
+  if(cfg.cluster_rows > 0)
+    for(int l = 1; l + 1 < s->nlev; ++l)
+      if(s->lv[size_t(l)].n <= uint32_t(cfg.cluster_rows))
+      {
+        s->ctail_first = (s->nlev - l <= MAX_TAIL) ? l : -1;
+        break;
+      }
+  if(s->ctail_first >= 0)
+    FB_TRY(dalloc(s.get(), (void**)&s->cred, sizeof(double) * 2 * MAX_TAIL * CT_CS));
+  if(cfg.tail_rows > 0 && s->ctail_first < 0)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.tail_rows))
       {
@@ -1818,6 +2010,12 @@ static fb_status solve_common(fb_solver* s, fb_solve_info* info)
     e = solve_dispatch<bf16_t, float>(s);
   if(e != FB_OK)
     return e;
+  if(s->launch_err != cudaSuccess)
+  {
+    const cudaError_t le = s->launch_err;
+    s->launch_err = cudaSuccess;
+    return cuda_fail(le, "cluster tail launch");
+  }
   FB_CUDA(cudaEventRecord(s->ev1, st));
   Scalars h;
   int err = 0;

@@ -126,23 +126,37 @@ namespace fb
     return d ? S(0) : S(sub(bi, sum));
   }
 
+  // b_c = F_c(R d) and (with_x) sol1_c = F_c(D_c .* b_c), without stores
+  template<typename Ac>
+  struct RestrictOut { Ac v, x; };
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ RestrictOut<typename ValueTraits<V>::acc> restrict_calc(const DCsr<V>& R, const S* d,
+    bool with_x, const S* dinvc, const uint8_t* dmc, uint32_t j)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const bool dc = __ldg(dmc + j) != 0;
+    const Ac di = with_x ? Ac(__ldg(dinvc + j)) : Ac(0);
+    const Ac sum = row_sum<V, S, NC>(R, j, d);
+    const Ac v = dc ? Ac(0) : add(sum, Ac(0));
+    Ac x = Ac(0);
+    if(with_x)
+    {
+      const Ac c = dc ? Ac(0) : mul(di, v);
+      x = add(Ac(0), c);
+    }
+    return RestrictOut<Ac>{v, x};
+  }
+
   // b_c = F_c(R d) and (xc != null) sol1_c = F_c(D_c .* b_c); returns b_c^2
   template<typename V, typename S, bool NC>
   __device__ __forceinline__ double restrict_row(const DCsr<V>& R, const S* d, S* bc, S* xc, const S* dinvc,
     const uint8_t* dmc, uint32_t j)
   {
-    typedef typename ValueTraits<V>::acc Ac;
-    const bool dc = __ldg(dmc + j) != 0;
-    const Ac di = xc ? Ac(__ldg(dinvc + j)) : Ac(0);
-    const Ac sum = row_sum<V, S, NC>(R, j, d);
-    const Ac v = dc ? Ac(0) : add(sum, Ac(0));
-    bc[j] = S(v);
+    const auto o = restrict_calc<V, S, NC>(R, d, xc != nullptr, dinvc, dmc, j);
+    bc[j] = S(o.v);
     if(xc)
-    {
-      const Ac c = dc ? Ac(0) : mul(di, v);
-      xc[j] = S(add(Ac(0), c));
-    }
-    return double(v) * double(v);
+      xc[j] = S(o.x);
+    return double(o.v) * double(o.v);
   }
 
   // x + F(P xc)
@@ -157,20 +171,31 @@ namespace fb
     return S(add(xi, c));
   }
 
-  // d = F(b - A x), c = F(D .* d); returns d^2
+  // d = F(b - A x), c = F(D .* d), without stores
+  template<typename Ac>
+  struct Post1Out { Ac d, c; };
   template<typename V, typename S, bool NC>
-  __device__ __forceinline__ double post1_row(const DCsr<V>& A, const S* b, const S* x, S* d, S* c, const S* dinv,
-    const uint8_t* dm, uint32_t i)
+  __device__ __forceinline__ Post1Out<typename ValueTraits<V>::acc> post1_calc(const DCsr<V>& A, const S* b,
+    const S* x, const S* dinv, const uint8_t* dm, uint32_t i)
   {
     typedef typename ValueTraits<V>::acc Ac;
     const bool dd = __ldg(dm + i) != 0;
     const Ac bi = Ac(b[i]), di = Ac(__ldg(dinv + i));
     const Ac sum = row_sum<V, S, NC>(A, i, x);
     const Ac dv = dd ? Ac(0) : sub(bi, sum);
-    d[i] = S(dv);
     const Ac cv = dd ? Ac(0) : mul(di, dv);
-    c[i] = S(add(Ac(0), cv));
-    return double(dv) * double(dv);
+    return Post1Out<Ac>{dv, add(Ac(0), cv)};
+  }
+
+  // d = F(b - A x), c = F(D .* d); returns d^2
+  template<typename V, typename S, bool NC>
+  __device__ __forceinline__ double post1_row(const DCsr<V>& A, const S* b, const S* x, S* d, S* c, const S* dinv,
+    const uint8_t* dm, uint32_t i)
+  {
+    const auto o = post1_calc<V, S, NC>(A, b, x, dinv, dm, i);
+    d[i] = S(o.d);
+    c[i] = S(o.c);
+    return double(o.d) * double(o.d);
   }
 
   // post-smoothing step k >= 2: c + F(D .* F(d - A c)); skipped -> 0

@@ -211,6 +211,11 @@ class PCG:
         shared memory, 2 = prefetched into L2."""
         self.cfg.tma_window = int(mode)
 
+    def set_cluster_rows(self, rows):
+        """Levels with at most `rows` rows (below the finest) run in one kernel on a cluster of 8
+        thread blocks (0 = off; takes precedence over set_tail_rows)."""
+        self.cfg.cluster_rows = int(rows)
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -320,7 +325,8 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
-                        ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None):
+                        ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
+                        cluster_rows=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -344,6 +350,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_tma_rows(tma_rows)
     if tma_window is not None:
         s.set_tma_window(tma_window)
+    if cluster_rows is not None:
+        s.set_cluster_rows(cluster_rows)
     h.init()
     s.init()
     return s

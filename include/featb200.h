@@ -191,6 +191,11 @@ typedef struct
                            coarsest, run in one single-block kernel per V-cycle; 0 = off */
   int tma_rows;         /* levels with at least this many rows use the TMA-staged persistent
                            passes (bulk copies into shared memory); 0 = off */
+  int cluster_rows;     /* levels (below the finest) with at most this many rows, down to the
+                           coarsest, run in one kernel on a cluster of 8 thread blocks (8 SMs) per
+                           V-cycle, passes separated by the cluster barrier; takes precedence over
+                           tail_rows; 0 = off (default: measured slower than the single-block tail
+                           on B200 for every threshold) */
   int tma_window;       /* the window of the gathered vector that a TMA-staged chunk reads:
                            0 (default) = neither: the row sums gather from global memory;
                            1 = staged in shared memory with the chunk; 2 = bulk-prefetched into L2

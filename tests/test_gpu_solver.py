@@ -25,14 +25,17 @@ def _solve(fb, levels, rhs, **kw):
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("ordering,graph,tail", [("native", True, None), ("native", False, None), ("rcm", True, None),
-                                                 ("native", True, 0), ("rcm", False, 0)])
-def test_fp64_matches_reference(featlib, cuda, name, ordering, graph, tail):
-    """tail None: coarse levels in the single-block tail kernel (default); 0: one launch per pass."""
+@pytest.mark.parametrize("ordering,graph,tail,cluster", [("native", True, None, None), ("native", False, None, None),
+                                                         ("rcm", True, None, None), ("native", True, None, 32767),
+                                                         ("rcm", False, None, 32767), ("native", True, 0, 0),
+                                                         ("rcm", False, 0, 0)])
+def test_fp64_matches_reference(featlib, cuda, name, ordering, graph, tail, cluster):
+    """Defaults: the coarse levels run in the single-block tail kernel; cluster 32767: every level
+    below the finest in the cluster tail kernel; tail 0: one launch per pass."""
     fb = featlib
     g = load_golden(name)
     lv = to_lafem_levels(g["levels"])
-    s, x, st = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, tail_rows=tail)
+    s, x, st = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, tail_rows=tail, cluster_rows=cluster)
     z = s.apply_precond(fb.DenseVector(g["rhs"])).elements
     assert np.array_equal(z, g["vcycle"]), rel_err(z, g["vcycle"])
     assert st == fb.Status.success
@@ -42,7 +45,8 @@ def test_fp64_matches_reference(featlib, cuda, name, ordering, graph, tail):
     assert abs(s.get_def_final() - g["summary"]["def_final"]) <= 1e-9 * g["summary"]["def_final"]
     if ordering == "native" and graph:
         for k, xk_ref in enumerate(g["iterates"], start=1):
-            sk, xk, stk = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, max_iter=k, tail_rows=tail)
+            sk, xk, stk = _solve(fb, lv, g["rhs"], ordering=ordering, use_graph=graph, max_iter=k, tail_rows=tail,
+                                 cluster_rows=cluster)
             assert rel_err(xk, xk_ref) <= PARITY, k
             assert abs(sk.get_def_final() - g["defects"][k - 1]) <= 1e-9 * g["defects"][k - 1]
 
@@ -69,8 +73,9 @@ def test_fp64_matches_live_reference(featlib, cuda, level, dim):
         vc = np.load(os.path.join(tmp, "vcycle.npy"))
         it2 = np.load(os.path.join(tmp, "iterate_2.npy"))
     lv = conv(levels)
-    for ordering, tail in (("native", None), ("rcm", None), ("rcm", 0)):
-        s, x, st = _solve(fb, lv, rhs, ordering=ordering, tail_rows=tail)
+    for ordering, tail, cluster in (("native", None, None), ("rcm", None, 32767), ("native", None, 32767),
+                                    ("rcm", 0, 0)):
+        s, x, st = _solve(fb, lv, rhs, ordering=ordering, tail_rows=tail, cluster_rows=cluster)
         assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc)
         assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
         assert rel_err(x, sol) <= PARITY
@@ -161,9 +166,10 @@ def test_tma_staged_passes_match(featlib, cuda, name, precision, window, orderin
     fb = featlib
     g = load_golden(name)
     lv = to_lafem_levels(g["levels"])
-    s_tma, x_tma, st1 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=32, tail_rows=0,
+    s_tma, x_tma, st1 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=32, tail_rows=0, cluster_rows=0,
                                tma_window=window, ordering=ordering)
-    s_ref, x_ref, st2 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=0, tail_rows=0, ordering=ordering)
+    s_ref, x_ref, st2 = _solve(fb, lv, g["rhs"], precision=precision, tma_rows=0, tail_rows=0, cluster_rows=0,
+                               ordering=ordering)
     assert st1 == st2 == fb.Status.success
     assert s_tma.get_num_iter() == s_ref.get_num_iter()
     z1 = s_tma.apply_precond(fb.DenseVector(g["rhs"])).elements
@@ -185,6 +191,20 @@ def test_tma_full_size(featlib, cuda, oracle_lib, ordering):
     mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
     x_ref, info = mg.solve(b)
     s, x, st = _solve(fb, levels, b, ordering=ordering)
+    assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, mg.vcycle(b))
+    assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+    assert rel_err(x, x_ref) <= PARITY
+
+
+def test_cluster_tail_full_size(featlib, cuda, oracle_lib):
+    """Level 10 with levels 7..1 in the cluster tail kernel (8 blocks, cluster barriers): bitwise
+    V-cycle against the C oracle, same iterations, solution within 1e-12."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(10, 2, rhs="gauss", gauss=AS.gauss_params(3, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    s, x, st = _solve(fb, levels, b, ordering="rcm", cluster_rows=32767)
     assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, mg.vcycle(b))
     assert st == fb.Status.success and s.get_num_iter() == info["iters"]
     assert rel_err(x, x_ref) <= PARITY
