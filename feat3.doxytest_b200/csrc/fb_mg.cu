@@ -1208,7 +1208,7 @@ namespace fb
     {
       if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
+      return uint64_t(tma_stages<double>()) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
     }
 
     // the TMA-staged pass serves matrices of at least tma_rows rows whose stages fit
@@ -1216,7 +1216,7 @@ namespace fb
     {
       if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(TMA_STAGES) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
+      return uint64_t(tma_stages<V>()) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
     }
     template<typename VV, typename XS, class Op>
     void tma(const DevMat& m, const void* x, const Op& op)
@@ -1226,11 +1226,11 @@ namespace fb
       uint32_t xw = s->cfg.tma_window ? m.xwin : 0u;
       const int xstage = s->cfg.tma_window == 1 ? 1 : 0;
       if(xw && xstage &&
-         uint64_t(TMA_STAGES) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
+         uint64_t(tma_stages<VV>()) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
            TMA_SMEM_MAX)
         xw = 0;
       const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + (xstage ? xw * uint32_t(sizeof(XS)) : 0u);
-      const size_t smem = size_t(TMA_STAGES) * sb;
+      const size_t smem = size_t(tma_stages<VV>()) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
       const uint32_t bps = std::max(1u, std::min(8u, uint32_t((227u * 1024u) / (smem + 1536u))));

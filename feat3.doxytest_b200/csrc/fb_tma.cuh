@@ -14,7 +14,11 @@
 namespace fb
 {
   constexpr int TMA_NT = 256;          // threads = rows per chunk
-  constexpr int TMA_STAGES = 3;
+  constexpr int TMA_STAGES = 3;   // pipeline depth, at most
+  // Stages of a pass over values of type V: FP64 rows are wide, and two stages leave room for
+  // more blocks (rows in flight) per SM; measured faster for FP64 on B200, three for FP32/BF16.
+  template<typename V>
+  __host__ __device__ constexpr int tma_stages() { return sizeof(V) == 8 ? 2 : 3; }
   constexpr uint32_t TMA_SPIN = 1u << 22;
   constexpr uint32_t TMA_XWIN_MAX = 8192;              // entries of a staged x window
   constexpr uint64_t TMA_SMEM_MAX = 128u * 1024u;      // dynamic shared memory of all stages
@@ -142,6 +146,7 @@ namespace fb
     __shared__ double sh[32];
     if(op.closed())
       return;
+    constexpr int NS = tma_stages<V>();
     constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
@@ -192,13 +197,13 @@ namespace fb
     };
     if(threadIdx.x == 0)
     {
-      for(int s = 0; s < TMA_STAGES; ++s)
+      for(int s = 0; s < NS; ++s)
         mbar_init(&bar[s], 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     if(threadIdx.x == 0)
-      for(int s = 0; s < TMA_STAGES; ++s)
+      for(int s = 0; s < NS; ++s)
       {
         const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
         if(c < nch)
@@ -209,8 +214,8 @@ namespace fb
     uint32_t it = 0;
     for(uint32_t c = blockIdx.x; c < nch; c += gridDim.x, ++it)
     {
-      const int s = int(it % TMA_STAGES);
-      const uint32_t par = (it / TMA_STAGES) & 1u;
+      const int s = int(it % NS);
+      const uint32_t par = (it / NS) & 1u;
       // one warp polls the barrier; the others wait in __syncthreads without taking issue slots
       bool ok = true;
       if(threadIdx.x < 32)
@@ -220,14 +225,14 @@ namespace fb
         failed = true;
         break;
       }
-      // every thread is past the previous chunk: refill its stage (TMA_STAGES - 1 chunks ahead)
+      // every thread is past the previous chunk: refill its stage (NS - 1 chunks ahead)
       if(threadIdx.x == 0 && it > 0)
       {
-        const uint32_t c2 = c - gridDim.x + uint32_t(TMA_STAGES) * gridDim.x;
+        const uint32_t c2 = c - gridDim.x + uint32_t(NS) * gridDim.x;
         if(c2 < nch)
         {
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-          issue(c2, int((it - 1) % TMA_STAGES));
+          issue(c2, int((it - 1) % NS));
         }
       }
       const unsigned char* st = tma_smem + size_t(s) * sb;
@@ -271,14 +276,14 @@ namespace fb
       if(threadIdx.x == 0)
       {
         atomicOr(err, 1);
-        // copies in flight: chunks it .. it + TMA_STAGES - 1 before the first refill, then one fewer
-        const uint32_t pending = it == 0 ? uint32_t(TMA_STAGES) : uint32_t(TMA_STAGES) - 1u;
+        // copies in flight: chunks it .. it + NS - 1 before the first refill, then one fewer
+        const uint32_t pending = it == 0 ? uint32_t(NS) : uint32_t(NS) - 1u;
         for(uint32_t k = 0; k < pending; ++k)
         {
           const uint32_t jt = it + k;
           const uint32_t c = blockIdx.x + jt * gridDim.x;
           if(c < nch)
-            mbar_wait(&bar[jt % TMA_STAGES], (jt / TMA_STAGES) & 1u);
+            mbar_wait(&bar[jt % NS], (jt / NS) & 1u);
         }
       }
       __syncthreads();
