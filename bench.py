@@ -58,7 +58,7 @@ DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
 
 # DRAM bytes of one launch of the roofline kernel, from one ncu capture (summarised in profiles/):
 # (workload, ordering) -> bytes read + written
-MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.057856e6 + 4.222464e6}
+MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.055808e6 + 4.434432e6}
 
 
 def dist_env():
