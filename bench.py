@@ -474,6 +474,8 @@ def main():
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
+    ap.add_argument("--tma-rows", type=int, default=None,
+                    help="levels with at least this many rows use the TMA-staged passes")
     ap.add_argument("--cluster-rows", type=int, default=None,
                     help="levels with at most this many rows run in the cluster tail kernel (0 = off)")
     ap.add_argument("--tma-window", type=int, choices=[0, 1, 2], default=0,
@@ -510,7 +512,7 @@ def main():
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
-                                    cluster_rows=args.cluster_rows)
+                                    cluster_rows=args.cluster_rows, tma_rows=args.tma_rows)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()

@@ -1705,9 +1705,9 @@ void fb_solver_config_default(fb_solver_config* c)
   c->min_iter = 0;
   c->use_graph = 1;
   c->rows_per_block = 0;
-  c->tail_rows = 4096;
+  c->tail_rows = 300;
   c->cluster_rows = 0;
-  c->tma_rows = 32768;
+  c->tma_rows = 1000;
   c->tma_window = 0;
 }
 

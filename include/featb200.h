@@ -203,8 +203,8 @@ typedef struct
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
- * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks, tail below 4096 rows,
- * TMA-staged passes from 32768 rows. */
+ * tol_abs 1/eps^2, max_iter 100, min_iter 0, graph on, autotuned blocks, single-block tail for
+ * levels of at most 300 rows, TMA-staged passes from 1000 rows (both thresholds tuned on B200). */
 void fb_solver_config_default(fb_solver_config* cfg);
 
 typedef struct
