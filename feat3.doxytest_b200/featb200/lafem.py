@@ -40,6 +40,17 @@ class DenseVector:
     def norm2(self):
         return float(np.sqrt(np.dot(self.elements, self.elements)))
 
+    # DenseVector::read_from / write_out (kernel/lafem/dense_vector.hpp:600-720); mode "dv"/"binary",
+    # "mtx" or "exp" (featb200.fileio)
+    @staticmethod
+    def read_from(mode, filename):
+        from . import fileio
+        return DenseVector(fileio.read_dv(filename, mode))
+
+    def write_out(self, mode, filename):
+        from . import fileio
+        fileio.write_dv(filename, self.elements, mode)
+
 
 class SparseMatrixCSR:
     """SparseMatrixCSR<double, Index>: row_ptr[rows+1], col_ind[nnz] (u64), val[nnz] (f64)."""
@@ -84,6 +95,18 @@ class SparseMatrixCSR:
         import scipy.sparse as sp
         return sp.csr_matrix((self.val, self.col_ind.astype(np.int64), self.row_ptr.astype(np.int64)),
                              shape=self.shape)
+
+    # SparseMatrixCSR::read_from / write_out (kernel/lafem/sparse_matrix_csr.hpp:880-1125); mode
+    # "csr"/"binary" or "mtx" (featb200.fileio)
+    @staticmethod
+    def read_from(mode, filename):
+        from . import fileio
+        rows, cols, rp, ci, val = fileio.read_csr(filename, mode)
+        return SparseMatrixCSR(rp, ci, val, (rows, cols))
+
+    def write_out(self, mode, filename):
+        from . import fileio
+        fileio.write_csr(filename, self.shape[0], self.shape[1], self.row_ptr, self.col_ind, self.val, mode)
 
     def c_host(self):
         """The fb_csr_host view (the arrays must outlive the call)."""

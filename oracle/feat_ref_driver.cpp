@@ -652,6 +652,28 @@ namespace Oracle
       (unsigned long)d, (unsigned long)iters[0], (unsigned long)iters[1]);
     return 0;
   }
+  // Container I/O round trip through the reference's own readers and writers: reads a binary CSR
+  // matrix (fm_csr) and a binary dense vector (fm_dv), writes them back in the binary formats and
+  // as Matrix Market / exponential ASCII into DIR (rt.csr, rt.dv, rt_matrix.mtx, rt_vector.mtx,
+  // rt_vector.exp), and prints their sizes.
+  int run_io(const char* csr_in, const char* dv_in, const std::string& out)
+  {
+    typedef LAFEM::SparseMatrixCSR<double, Index> MatrixType;
+    typedef LAFEM::DenseVector<double, Index> VectorType;
+    MatrixType a;
+    a.read_from(LAFEM::FileMode::fm_csr, String(csr_in));
+    VectorType v;
+    v.read_from(LAFEM::FileMode::fm_dv, String(dv_in));
+    a.write_out(LAFEM::FileMode::fm_csr, String(out + "/rt.csr"));
+    v.write_out(LAFEM::FileMode::fm_dv, String(out + "/rt.dv"));
+    a.write_out(LAFEM::FileMode::fm_mtx, String(out + "/rt_matrix.mtx"));
+    v.write_out(LAFEM::FileMode::fm_mtx, String(out + "/rt_vector.mtx"));
+    v.write_out(LAFEM::FileMode::fm_exp, String(out + "/rt_vector.exp"));
+    std::printf("{\"rows\": %lu, \"columns\": %lu, \"used_elements\": %lu, \"size\": %lu}\n",
+      (unsigned long)a.rows(), (unsigned long)a.columns(), (unsigned long)a.used_elements(),
+      (unsigned long)v.size());
+    return 0;
+  }
 } // namespace Oracle
 
 int main(int argc, char* argv[])
@@ -660,6 +682,8 @@ int main(int argc, char* argv[])
   Oracle::Options opt;
   if(argc == 5 && std::strcmp(argv[1], "fd") == 0)
     return Oracle::run_fd(Index(std::stoul(argv[2])), Index(std::stoul(argv[3])), argv[4]);
+  if(argc == 5 && std::strcmp(argv[1], "io") == 0)
+    return Oracle::run_io(argv[2], argv[3], argv[4]);
   if(argc < 2 || std::strcmp(argv[1], "solve") != 0)
   {
     std::fprintf(stderr, "usage: feat_oracle solve --dim D --level L --out DIR [...]\n");

@@ -201,6 +201,16 @@ def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, ome
     return json.loads(res.stdout.strip().splitlines()[-1])
 
 
+def feat_io(csr_in, dv_in, out_dir, timeout=300):
+    """The reference's own container readers and writers (oracle/_ref/feat_oracle io): reads the
+    binary CSR matrix and dense vector, writes rt.csr, rt.dv, rt_matrix.mtx, rt_vector.mtx and
+    rt_vector.exp into out_dir; returns its JSON summary."""
+    os.makedirs(out_dir, exist_ok=True)
+    res = subprocess.run([FEAT_BIN, "io", csr_in, dv_in, out_dir], check=True, capture_output=True, text=True,
+                         timeout=timeout)
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
 def load_dump(out_dir, level, level_min=1):
     """Read a feat_oracle dump (written with --dump-levels) into a finest-first level list."""
     def ld(name):
