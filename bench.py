@@ -480,6 +480,8 @@ def main():
                     help="levels with at most this many rows run in the cluster tail kernel (0 = off)")
     ap.add_argument("--tma-window", type=int, choices=[0, 1, 2], default=0,
                     help="gathered-vector window of a TMA chunk: 2 prefetch into L2, 1 stage in shared memory, 0 none")
+    ap.add_argument("--cycle", choices=["V", "F", "W"], default="V",
+                    help="multigrid cycle of the preconditioner (the reference's MultiGridCycle)")
     ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
                     help="device DOF ordering (the generated problems are numbered lexicographically)")
     ap.add_argument("--ws-train", type=int, default=20000, help="training instances (learned warm start)")
@@ -512,7 +514,7 @@ def main():
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
-                                    cluster_rows=args.cluster_rows, tma_rows=args.tma_rows)
+                                    cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
@@ -637,7 +639,7 @@ def main():
                 "vs_baseline": None, "dtype": "f32+f64" if precision != "f64" else "f64", "data": "synthetic",
                 "config": {"workload": args.workload + ": " + desc, "dofs": int(n), "nnz": int(info_lv[0][1]),
                            "levels": int(info_lv.shape[0]), "ordering": args.ordering, "precision": precision,
-                           "parallelism": f"replicas x{world}", "l2": L2Flush.DESC,
+                           "cycle": args.cycle, "parallelism": f"replicas x{world}", "l2": L2Flush.DESC,
                            "iterations": int(np.median(iters))},
                 "spmv_gbs": spmv_gbs, "rel_residual": rel_res,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1311,196 +1311,309 @@ namespace fb
       return used;
     }
 
-    // V-cycle from the top level; the top level's b and sol1 and skip_pre are in place.
-    // Returns the buffer holding the top level's solution (for non-PCG use).
-    void vcycle(bool pcg_top)
+    // ---- the pieces of a multigrid cycle (kernel/solver/multigrid.hpp:1350-1440); xcur[l] is the
+    // buffer (x or x2) that holds level l's solution
+
+    // pre-smoothing steps k >= 2 of level l (step 1, sol1 = D b, came with the restriction)
+    void pre_smooth(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      const int steps = std::max(1, s->cfg.smooth_steps);
+      void* xa = f.x;
+      void* xb = f.x2;
+      for(int k = 1; k < steps; ++k)
+      {
+        if(dry)
+          ;
+        else if(use_tma(f.A))
+          tma<V, S>(f.A, xa, OpSmooth<V, S>{(const S*)f.b, (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.skip_pre, s->sc});
+        else
+          k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+            (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.A, 3, 1) + f.n;
+        std::swap(xa, xb);
+      }
+      xcur[size_t(l)] = xa;
+    }
+
+    // d_l = F(b - A x_l)
+    void defect(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      if(dry)
+        ;
+      else if(use_tma(f.A))
+        tma<V, S>(f.A, xcur[size_t(l)], OpDefect<V, S>{(const S*)f.b, (S*)f.d, f.dm, s->sc});
+      else
+        k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xcur[size_t(l)],
+          (S*)f.d, f.dm, s->sc);
+      ++launches;
+      bytes += csr_bytes(f.A, 1, 1) + f.n;
+    }
+
+    // b_{l+1} = F(R d_l), sol1_{l+1} = F(D b_{l+1}) (not on the coarsest level), skip_pre_{l+1}
+    void restrict_to(int l)
+    {
+      const int nl = s->nlev;
+      DevLevel& f = L(l);
+      DevLevel& c = L(l + 1);
+      const bool coarsest = (l + 2 == nl);
+      if(dry)
+        ;
+      else if(use_tma(f.R))
+        tma<V, S>(f.R, f.d, OpRestrict<V, S>{(S*)c.b, coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm,
+          c.skip_pre, s->sc});
+      else
+        k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
+          coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
+      ++launches;
+      bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
+    }
+
+    // _apply_rest(from, smooth_first) down to level stop (exclusive of stop's own smoothing): with
+    // smooth_first == false, level `from` restricts the defect already in d_from
+    void down(int from, bool smooth_first, int stop, std::vector<void*>& xcur)
+    {
+      for(int l = from; l < stop; ++l)
+      {
+        if(smooth_first || l > from)
+        {
+          pre_smooth(l, xcur);
+          defect(l, xcur);
+        }
+        restrict_to(l);
+      }
+    }
+
+    // exact solve on the coarsest level
+    void coarse(std::vector<void*>& xcur)
+    {
+      const int nl = s->nlev;
+      DevLevel& c = L(nl - 1);
+      if(!dry) k_coarse<S><<<1, NT, 0, st>>>((const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
+      ++launches;
+      bytes += double(s->nfree) * s->nfree * 8.0 + double(c.n) * 2 * sizeof(S);
+      xcur[size_t(nl - 1)] = c.x;
+    }
+
+    // x_l += F(P x_{l+1})
+    void prolong(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      void* xf = xcur[size_t(l)];
+      if(dry)
+        ;
+      else if(use_tma(f.P))
+        tma<V, S>(f.P, xcur[size_t(l + 1)], OpProlong<V, S>{(S*)xf, f.dm, s->sc});
+      else
+        k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm,
+          s->sc);
+      ++launches;
+      bytes += csr_bytes(f.P, 1, 1) + f.n;
+    }
+
+    // a smoother applied as a correction: d = F(b - A x), c = Richardson-Jacobi(d) from zero, x += c
+    // (post-smoothing, and the peak smoother); top: the last step also forms the PCG's z and r.z
+    void post_smooth(int l, bool top, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      const int steps = std::max(1, s->cfg.smooth_steps);
+      void* xf = xcur[size_t(l)];
+      if(dry)
+        ;
+      else if(use_tma(f.A))
+        tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+      else
+        k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+          (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+      ++launches;
+      bytes += csr_bytes(f.A, 2, 2) + f.n;
+      void* ca = f.c;
+      void* cb = f.c2;
+      if(steps == 1)
+      {
+        if(!dry)
+        {
+          if(top)
+            k_post_final<S, true><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot, s->sc);
+          else
+            k_post_final<S, false><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n, s->slot, s->sc);
+        }
+        ++launches;
+        bytes += double(f.n) * sizeof(S) * 3;
+      }
+      for(int k = 2; k <= steps; ++k)
+      {
+        const bool last = (k == steps);
+        if(dry)
+          ;
+        else if(use_tma(f.A))
+        {
+          if(!last)
+            tma<V, S>(f.A, ca, OpPost2<V, S, false, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
+              (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+          else if(top)
+            tma<V, S>(f.A, ca, OpPost2<V, S, true, true>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, s->z, s->r,
+              (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+          else
+            tma<V, S>(f.A, ca, OpPost2<V, S, true, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
+              (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+        }
+        else if(!last)
+          k_post2<V, S, false, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+            (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+        else if(top)
+          k_post2<V, S, true, true><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+            (S*)cb, (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+        else
+          k_post2<V, S, true, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+            (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+        ++launches;
+        bytes += csr_bytes(f.A, 3, 1) + f.n;
+        std::swap(ca, cb);
+      }
+    }
+
+    // _apply_prol(to, smooth_last) from level start - 1 up to `to`: prolongation, then
+    // post-smoothing except on level `to` when smooth_last == false
+    void up(int to, bool smooth_last, int start, bool pcg_top, std::vector<void*>& xcur)
+    {
+      for(int l = start - 1; l >= to; --l)
+      {
+        prolong(l, xcur);
+        if(smooth_last || l > to)
+          post_smooth(l, pcg_top && l == 0, xcur);
+      }
+    }
+
+    // _apply_smooth_peak(l): the peak smoother as a correction, then the new defect d_l
+    void peak(int l, std::vector<void*>& xcur)
+    {
+      post_smooth(l, false, xcur);
+      defect(l, xcur);
+    }
+
+    // the coarse-level tail kernel (single block or cluster) from level lt down and back up
+    void tail(int lt, std::vector<void*>& xcur)
     {
       const int nl = s->nlev;
       const int steps = std::max(1, s->cfg.smooth_steps);
-      // first level of the tail (cluster kernel or single-block kernel), -1 = none
       const bool ctail = s->ctail_first >= 0;
-      const int lt = ctail ? s->ctail_first : s->tail_first;
-      std::vector<void*> xcur(static_cast<size_t>(nl));
-      for(int l = 0; l + 1 < nl; ++l)
+      TailParams<V, S> tp;
+      std::memset(&tp, 0, sizeof(tp));
+      tp.count = nl - lt;
+      tp.steps = steps;
+      tp.free_dofs = s->free_dofs;
+      tp.inv = s->cinv;
+      tp.m = s->nfree;
+      for(int l = lt; l < nl; ++l)
       {
-        if(lt >= 0 && l >= lt)
-          break;
         DevLevel& f = L(l);
-        DevLevel& c = L(l + 1);
-        void* xa = f.x;
-        void* xb = f.x2;
-        for(int k = 1; k < steps; ++k)
+        TailLevel<V, S>& t = tp.lv[l - lt];
+        t.A = view<V>(f.A);
+        if(l + 1 < nl)
         {
-          if(dry)
-            ;
-          else if(use_tma(f.A))
-            tma<V, S>(f.A, xa, OpSmooth<V, S>{(const S*)f.b, (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.skip_pre, s->sc});
-          else
-            k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
-              (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
-          ++launches;
-          bytes += csr_bytes(f.A, 3, 1) + f.n;
-          std::swap(xa, xb);
+          t.P = view<V>(f.P);
+          t.R = view<V>(f.R);
         }
-        xcur[size_t(l)] = xa;
-        if(dry)
-          ;
-        else if(use_tma(f.A))
-          tma<V, S>(f.A, xa, OpDefect<V, S>{(const S*)f.b, (S*)f.d, f.dm, s->sc});
-        else
-          k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
-        ++launches;
-        bytes += csr_bytes(f.A, 1, 1) + f.n;
-        const bool coarsest = (l + 2 == nl);
-        if(dry)
-          ;
-        else if(use_tma(f.R))
-          tma<V, S>(f.R, f.d, OpRestrict<V, S>{(S*)c.b, coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm,
-            c.skip_pre, s->sc});
-        else
-          k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
-            coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
-        ++launches;
-        bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
+        t.b = (S*)f.b;
+        t.x = (S*)f.x;
+        t.x2 = (S*)f.x2;
+        t.d = (S*)f.d;
+        t.c = (S*)f.c;
+        t.c2 = (S*)f.c2;
+        t.dinv = (const S*)f.dinv;
+        t.dm = f.dm;
+        t.skip_pre = f.skip_pre;
+        t.skip_post = f.skip_post;
+        t.n = f.n;
+        xcur[size_t(l)] = (l + 1 == nl) ? f.x : (((steps - 1) % 2) ? f.x2 : f.x);
+        if(l + 1 < nl)
+          bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
       }
-      if(lt >= 0)
+      const size_t smem = tail_layout(tp, lt, !ctail);
+      bytes += double(s->nfree) * s->nfree * 8.0;
+      if(dry)
+        ;
+      else if(ctail)
       {
-        TailParams<V, S> tp;
-        std::memset(&tp, 0, sizeof(tp));
-        tp.count = nl - lt;
-        tp.steps = steps;
-        tp.free_dofs = s->free_dofs;
-        tp.inv = s->cinv;
-        tp.m = s->nfree;
-        for(int l = lt; l < nl; ++l)
-        {
-          DevLevel& f = L(l);
-          TailLevel<V, S>& t = tp.lv[l - lt];
-          t.A = view<V>(f.A);
-          if(l + 1 < nl)
-          {
-            t.P = view<V>(f.P);
-            t.R = view<V>(f.R);
-          }
-          t.b = (S*)f.b;
-          t.x = (S*)f.x;
-          t.x2 = (S*)f.x2;
-          t.d = (S*)f.d;
-          t.c = (S*)f.c;
-          t.c2 = (S*)f.c2;
-          t.dinv = (const S*)f.dinv;
-          t.dm = f.dm;
-          t.skip_pre = f.skip_pre;
-          t.skip_post = f.skip_post;
-          t.n = f.n;
-          xcur[size_t(l)] = (l + 1 == nl) ? f.x : (((steps - 1) % 2) ? f.x2 : f.x);
-          if(l + 1 < nl)
-            bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
-        }
-        const size_t smem = tail_layout(tp, lt, !ctail);
-        bytes += double(s->nfree) * s->nfree * 8.0;
-        if(dry)
-          ;
-        else if(ctail)
-        {
-          cudaLaunchConfig_t lc = {};
-          lc.gridDim = dim3(CT_CS, 1, 1);
-          lc.blockDim = dim3(CT_NT, 1, 1);
-          lc.dynamicSmemBytes = 0;
-          lc.stream = st;
-          cudaLaunchAttribute at[1];
-          at[0].id = cudaLaunchAttributeClusterDimension;
-          at[0].val.clusterDim.x = CT_CS;
-          at[0].val.clusterDim.y = 1;
-          at[0].val.clusterDim.z = 1;
-          lc.attrs = at;
-          lc.numAttrs = 1;
-          const cudaError_t e = cudaLaunchKernelEx(&lc, k_ctail<V, S>, tp, (const Scalars*)s->sc, s->cred);
-          if(e != cudaSuccess && s->launch_err == cudaSuccess)
-            s->launch_err = e;
-        }
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(CT_CS, 1, 1);
+        lc.blockDim = dim3(CT_NT, 1, 1);
+        lc.dynamicSmemBytes = 0;
+        lc.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = CT_CS;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        const cudaError_t e = cudaLaunchKernelEx(&lc, k_ctail<V, S>, tp, (const Scalars*)s->sc, s->cred);
+        if(e != cudaSuccess && s->launch_err == cudaSuccess)
+          s->launch_err = e;
+      }
+      else
+        k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
+      ++launches;
+    }
+
+    // One multigrid cycle from the top level; the top level's b, sol1 and skip_pre are in place.
+    // V: rest(top) + coarse (or the tail kernel) + prol(top).  F and W (no tail kernel): the peak
+    // sequences of _apply_cycle_f / _apply_cycle_w (kernel/solver/multigrid.hpp:1356-1440).
+    void vcycle(bool pcg_top)
+    {
+      const int nl = s->nlev;
+      std::vector<void*> xcur(static_cast<size_t>(nl));
+      xcur[0] = L(0).x;
+      const int cyc = s->cfg.cycle;
+      if(cyc == FB_CYCLE_V)
+      {
+        const int lt = s->ctail_first >= 0 ? s->ctail_first : s->tail_first;
+        const int stop = lt >= 0 ? lt : nl - 1;
+        down(0, true, stop, xcur);
+        if(lt >= 0)
+          tail(lt, xcur);
         else
-          k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
-        ++launches;
+          coarse(xcur);
+        up(0, true, stop, pcg_top, xcur);
+        return;
+      }
+      const int last = nl - 1;
+      down(0, true, last, xcur);
+      if(cyc == FB_CYCLE_F)
+      {
+        for(int pk = last - 1; pk > 0; --pk)
+        {
+          coarse(xcur);
+          up(pk, false, last, false, xcur);
+          peak(pk, xcur);
+          down(pk, false, last, xcur);
+        }
+        coarse(xcur);
       }
       else
       {
-        DevLevel& c = L(nl - 1);
-        if(!dry) k_coarse<S><<<1, NT, 0, st>>>((const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
-        ++launches;
-        bytes += double(s->nfree) * s->nfree * 8.0 + double(c.n) * 2 * sizeof(S);
-        xcur[size_t(nl - 1)] = c.x;
-      }
-      for(int l = nl - 2; l >= 0; --l)
-      {
-        if(lt >= 0 && l >= lt)
-          continue;
-        DevLevel& f = L(l);
-        void* xf = xcur[size_t(l)];
-        if(dry)
-          ;
-        else if(use_tma(f.P))
-          tma<V, S>(f.P, xcur[size_t(l + 1)], OpProlong<V, S>{(S*)xf, f.dm, s->sc});
-        else
-          k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm,
-            s->sc);
-        ++launches;
-        bytes += csr_bytes(f.P, 1, 1) + f.n;
-        if(dry)
-          ;
-        else if(use_tma(f.A))
-          tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
-        else
-          k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
-            (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
-        ++launches;
-        bytes += csr_bytes(f.A, 2, 2) + f.n;
-        const bool top = pcg_top && l == 0;
-        void* ca = f.c;
-        void* cb = f.c2;
-        if(steps == 1)
+        coarse(xcur);
+        std::vector<int> cnt(static_cast<size_t>(nl), 0);
+        const int num_cgs = 1 << last;
+        for(int cgs = 1; cgs < num_cgs; ++cgs)
         {
-          if(!dry)
-          {
-            if(top)
-              k_post_final<S, true><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot, s->sc);
-            else
-              k_post_final<S, false><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n, s->slot, s->sc);
-          }
-          ++launches;
-          bytes += double(f.n) * sizeof(S) * 3;
-        }
-        for(int k = 2; k <= steps; ++k)
-        {
-          const bool last = (k == steps);
-          if(dry)
-            ;
-          else if(use_tma(f.A))
-          {
-            if(!last)
-              tma<V, S>(f.A, ca, OpPost2<V, S, false, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
-                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
-            else if(top)
-              tma<V, S>(f.A, ca, OpPost2<V, S, true, true>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, s->z, s->r,
-                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
-            else
-              tma<V, S>(f.A, ca, OpPost2<V, S, true, false>{(const S*)f.d, (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr,
-                (const S*)f.dinv, f.dm, f.skip_post, s->sc});
-          }
-          else if(!last)
-            k_post2<V, S, false, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
-              (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
-          else if(top)
-            k_post2<V, S, true, true><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
-              (S*)cb, (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
-          else
-            k_post2<V, S, true, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
-              (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
-          ++launches;
-          bytes += csr_bytes(f.A, 3, 1) + f.n;
-          std::swap(ca, cb);
+          int pk = last;
+          while(pk > 0)
+            if(cnt[size_t(--pk)] == 0)
+              break;
+          for(int i = last - 1; i > pk; --i)
+            cnt[size_t(i)] = 0;
+          ++cnt[size_t(pk)];
+          up(pk, false, last, false, xcur);
+          peak(pk, xcur);
+          down(pk, false, last, xcur);
+          coarse(xcur);
         }
       }
+      up(0, true, last, pcg_top, xcur);
     }
 
     const DevMat& A64() { return s->cfg.precision == FB_PREC_F64 ? L(0).A : L(0).A64; }
@@ -1707,6 +1820,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->rows_per_block = 0;
   c->tail_rows = 300;
   c->cluster_rows = 0;
+  c->cycle = FB_CYCLE_V;
   c->tma_rows = 1000;
   c->tma_window = 0;
 }
@@ -1808,7 +1922,8 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     cfg = *cfg_in;
   else
     fb_solver_config_default(&cfg);
-  if(cfg.precision < FB_PREC_F64 || cfg.precision > FB_PREC_F32_BF16 || cfg.smooth_steps < 1 || cfg.max_iter < 0)
+  if(cfg.precision < FB_PREC_F64 || cfg.precision > FB_PREC_F32_BF16 || cfg.smooth_steps < 1 || cfg.max_iter < 0 ||
+     cfg.cycle < FB_CYCLE_V || cfg.cycle > FB_CYCLE_W)
   {
     set_error("solver_create: bad configuration");
     return FB_ERR_ARG;
@@ -1927,7 +2042,7 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   // coarser level below it
   s->tail_first = -1;
   s->ctail_first = -1;
-  if(cfg.cluster_rows > 0)
+  if(cfg.cluster_rows > 0 && cfg.cycle == FB_CYCLE_V)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.cluster_rows))
       {
@@ -1936,7 +2051,7 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       }
   if(s->ctail_first >= 0)
     FB_TRY(dalloc(s.get(), (void**)&s->cred, sizeof(double) * 2 * MAX_TAIL * CT_CS));
-  if(cfg.tail_rows > 0 && s->ctail_first < 0)
+  if(cfg.tail_rows > 0 && s->ctail_first < 0 && cfg.cycle == FB_CYCLE_V)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.tail_rows))
       {

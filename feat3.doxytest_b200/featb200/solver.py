@@ -96,7 +96,7 @@ class MultiGridHierarchy:
                    smoother_peak=None):
         if isinstance(transfer_or_coarse, Transfer):
             self.levels.append({"matrix": matrix, "filter": filter, "transfer": transfer_or_coarse,
-                                "pre": smoother_pre, "post": smoother_post})
+                                "pre": smoother_pre, "post": smoother_post, "peak": smoother_peak})
         else:
             if not isinstance(transfer_or_coarse, CoarseInverse):
                 raise _lib.FeatB200Error("the device multigrid supports the exact coarse inverse only")
@@ -154,8 +154,19 @@ class MultiGridHierarchy:
 
 class MultiGrid:
     def __init__(self, hierarchy, cycle=MultiGridCycle.V):
+        """V, F or W cycle (MultiGrid::_apply_cycle_v/_f/_w, kernel/solver/multigrid.hpp:1350-1440);
+        the peak smoother is the pre/post smoother (push_level with the same smoother three times)."""
+        if cycle not in (MultiGridCycle.V, MultiGridCycle.F, MultiGridCycle.W):
+            raise _lib.FeatB200Error("unknown multigrid cycle")
         if cycle != MultiGridCycle.V:
-            raise _lib.FeatB200Error("the device multigrid implements the V-cycle")
+            # the device applies the peak smoother once, as the reference does when one is pushed;
+            # without one the reference would run pre- and post-smoother in turn
+            for lv in hierarchy.levels[:-1]:
+                pk = lv.get("peak")
+                if pk is None or not (pk is lv["pre"] or (isinstance(pk, Richardson) and isinstance(lv["pre"], Richardson)
+                                                          and (pk.omega, pk.min_iter, pk.max_iter) ==
+                                                          (lv["pre"].omega, lv["pre"].min_iter, lv["pre"].max_iter))):
+                    raise _lib.FeatB200Error("F/W cycles need the peak smoother to be the pre/post smoother")
         self.hierarchy, self.cycle = hierarchy, cycle
 
 
@@ -225,6 +236,7 @@ class PCG:
         omega, steps = h.smoother_params()
         self.cfg.omega = omega
         self.cfg.smooth_steps = steps
+        self.cfg.cycle = {MultiGridCycle.V: 0, MultiGridCycle.F: 1, MultiGridCycle.W: 2}[self.precond.cycle]
         if h._h is None:
             h.init()
         s = C.c_void_p()
@@ -326,7 +338,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None):
+                        cluster_rows=None, cycle="V"):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -337,7 +349,7 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         sm.set_max_iter(steps)
         h.push_level(lv["matrix"], lv["filter"], lv["transfer"], sm, sm, sm)
     h.push_level(levels[-1]["matrix"], levels[-1]["filter"], new_coarse_inverse())
-    mg = new_multigrid(h, MultiGridCycle.V)
+    mg = new_multigrid(h, MultiGridCycle[cycle])
     s = new_pcg(levels[0]["matrix"], levels[0]["filter"], mg)
     s.set_tol_rel(tol_rel)
     s.set_max_iter(max_iter)

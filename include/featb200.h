@@ -174,6 +174,10 @@ void fb_hierarchy_destroy(fb_hierarchy* h);
 #define FB_ORDER_RCM 1       /* reverse Cuthill-McKee per level (host, at setup); vectors are
                                 permuted on the way in and out of fb_solver_solve */
 
+#define FB_CYCLE_V 0
+#define FB_CYCLE_F 1
+#define FB_CYCLE_W 2
+
 typedef struct
 {
   int precision;        /* FB_PREC_* */
@@ -196,6 +200,9 @@ typedef struct
                            V-cycle, passes separated by the cluster barrier; takes precedence over
                            tail_rows; 0 = off (default: measured slower than the single-block tail
                            on B200 for every threshold) */
+  int cycle;            /* FB_CYCLE_V (default), FB_CYCLE_F or FB_CYCLE_W: the multigrid cycle of
+                           MultiGrid::_apply_cycle_v/_f/_w (kernel/solver/multigrid.hpp:1350-1440);
+                           F and W cycles run without the tail kernels */
   int tma_window;       /* the window of the gathered vector that a TMA-staged chunk reads:
                            0 (default) = neither: the row sums gather from global memory;
                            1 = staged in shared memory with the chunk; 2 = bulk-prefetched into L2

@@ -334,6 +334,7 @@ namespace Oracle
   struct Options
   {
     int dim = 2;
+    std::string cycle = "v";   // multigrid cycle: v, f or w
     Index level = 7;
     Index level_min = 1;
     std::string out = ".";
@@ -511,7 +512,9 @@ namespace Oracle
       auto coarse = std::make_shared<CoarseInverseSolver>(lvl.matrix, lvl.filter);
       hierarchy->push_level(lvl.matrix, lvl.filter, coarse);
     }
-    auto multigrid = Solver::new_multigrid(hierarchy, Solver::MultiGridCycle::V);
+    const Solver::MultiGridCycle cycle = opt.cycle == "f" ? Solver::MultiGridCycle::F :
+                                         (opt.cycle == "w" ? Solver::MultiGridCycle::W : Solver::MultiGridCycle::V);
+    auto multigrid = Solver::new_multigrid(hierarchy, cycle);
     auto solver = Solver::new_pcg(top.matrix, top.filter, multigrid);
     solver->set_tol_rel(DataType(opt.tol));
     solver->set_max_iter(100);
@@ -713,6 +716,7 @@ int main(int argc, char* argv[])
     else if(a == "--tol") opt.tol = std::stod(next());
     else if(a == "--iterates") opt.iterates = Index(std::stoul(next()));
     else if(a == "--vcycle") opt.vcycle = true;
+    else if(a == "--cycle") opt.cycle = next();
     else if(a == "--dump-levels") opt.dump_levels = true;
     else if(a == "--no-dump") opt.dump = false;
     else if(a == "--time") opt.time_reps = std::stoi(next());

@@ -107,4 +107,4 @@ def test_python_mirror_rejects_unsupported_configurations(featlib):
     with pytest.raises(fb.FeatB200Error):
         h.smoother_params()
     with pytest.raises(fb.FeatB200Error):
-        fb.new_multigrid(h, fb.MultiGridCycle.W)
+        fb.new_multigrid(h, "X")

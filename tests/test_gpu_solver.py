@@ -208,3 +208,33 @@ def test_cluster_tail_full_size(featlib, cuda, oracle_lib):
     assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, mg.vcycle(b))
     assert st == fb.Status.success and s.get_num_iter() == info["iters"]
     assert rel_err(x, x_ref) <= PARITY
+
+
+@pytest.mark.parametrize("cycle", ["F", "W"])
+@pytest.mark.parametrize("level,ordering,graph", [(5, "native", True), (6, "rcm", False)])
+def test_fw_cycles_match_live_reference(featlib, cuda, cycle, level, ordering, graph):
+    """F and W cycles (MultiGrid::_apply_cycle_f/_w) against the reference run with the same cycle:
+    bitwise multigrid application, same PCG iterations, solution within 1e-12."""
+    fb = featlib
+    from helpers import to_lafem_levels as conv
+    with tempfile.TemporaryDirectory() as tmp:
+        summ, levels = _live_reference(tmp, level, 2, cycle=cycle.lower())
+        rhs = np.load(os.path.join(tmp, "rhs.npy"))
+        sol = np.load(os.path.join(tmp, "sol.npy"))
+        vc = np.load(os.path.join(tmp, "vcycle.npy"))
+    lv = conv(levels)
+    s, x, st = _solve(fb, lv, rhs, ordering=ordering, use_graph=graph, cycle=cycle)
+    assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc)
+    assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
+    assert rel_err(x, sol) <= PARITY
+
+
+@pytest.mark.parametrize("cycle", ["F", "W"])
+def test_fw_cycles_mixed_precision(featlib, cuda, cycle):
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(8, 2, rhs="gauss", gauss=AS.gauss_params(5, 2))
+    _, x64, st64 = _solve(fb, levels, b, cycle=cycle)
+    s32, x32, st32 = _solve(fb, levels, b, cycle=cycle, precision="f32")
+    assert st64 == st32 == fb.Status.success
+    assert rel_err(x32, x64) <= 1e-7
