@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -394,17 +395,28 @@ namespace fb
   };
 
   // ------------------------------------------------------------------ coarse-level tail
-  // The bottom of the V-cycle (levels whose row count is at most the tail threshold, down to the
-  // coarsest) in ONE block of TAIL_NT threads: block-stride loops separated by __syncthreads
-  // replace one kernel launch per pass.  The tail's vectors live in shared memory (levels the host
-  // placed there; the tail's top level is copied in and its solution copied out), and its
-  // matrices, diagonals and masks are bulk-prefetched into L2 when the block starts, so the passes
-  // wait on shared memory and L1/L2 instead of DRAM.  The row bodies are the grid kernels' own.
+  // The part of a multigrid cycle below the tail threshold (levels whose row count is at most the
+  // threshold, down to the coarsest) in ONE block of TAIL_NT threads: block-stride loops separated
+  // by __syncthreads replace one kernel launch per pass.  k_tail runs a V-cycle bottom;
+  // k_tail_prog runs a program of cycle events (CycEv, encoded op << 4 | tail level) cut by the host
+  // out of the cycle's event list: the F- and W-cycle sub-cycles with their peak smoothing.  The
+  // tail's vectors live in shared memory (levels the host placed there; the tail's top level is
+  // copied in and its solution copied out), and its matrices, diagonals and masks are
+  // bulk-prefetched into L2 when the block starts, so the passes wait on shared memory and L1/L2
+  // instead of DRAM.  The row bodies are the grid kernels' own.
+  // events of a multigrid cycle (kernel/solver/multigrid.hpp:1350-1440): pre-smoothing steps 2..
+  // (step 1 comes with the restriction), defect, restriction to the next coarser level, coarse
+  // solve, prolongation from the next coarser level, post-smoothing (also the peak smoother) and
+  // the PCG's final post-smoothing, which also forms z and r.z
+  enum CycOp : uint8_t { EV_PRE = 0, EV_DEF = 1, EV_RES = 2, EV_CRS = 3, EV_PRO = 4, EV_POST = 5, EV_POST_TOP = 6 };
+  struct CycEv { uint8_t op; uint8_t lvl; };   // lvl: the level (restriction, prolongation: the finer one)
+
   constexpr int TAIL_NT = 512;
   constexpr int MAX_TAIL = 12;
   constexpr int MAX_TAIL_PF = 96;
   constexpr uint32_t TAIL_PF_CHUNK = 32768;
   constexpr size_t TAIL_SMEM_MAX = 200 * 1024;
+  constexpr int TAIL_PROG_CHUNK = 1024;
 
   template<typename V, typename S>
   struct TailLevel
@@ -600,6 +612,229 @@ namespace fb
   }
 
   // ------------------------------------------------------------------ cluster tail
+  // shared state of the tail kernel's interpreter
+  struct TailShared
+  {
+    double sh[32];
+    int skip_pre[MAX_TAIL];
+    int xsel[MAX_TAIL];    // 1 or 2: which x buffer holds level t's iterate
+    int skip_post;
+  };
+
+  // The events of k_tail_prog, one function each.  Each ends with its last pass written but not
+  // yet synchronised; the interpreter syncs after every event.
+
+  // pre-smoothing steps 2..steps from sol1 in x
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_pre(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    const S* fb = tail_vec(tp, sbase, t, 0);
+    S* xa = tail_vec(tp, sbase, t, 1);
+    S* xb = tail_vec(tp, sbase, t, 2);
+    int sel = 1;
+    const bool skipped = ts.skip_pre[t] != 0;
+    for(int k = 1; k < tp.steps; ++k)
+    {
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        xb[i] = smooth_row<V, S, false>(f.A, fb, xa, f.dinv, f.dm, skipped, i);
+      if(k + 1 < tp.steps)
+        __syncthreads();
+      S* tmp = xa;
+      xa = xb;
+      xb = tmp;
+      sel = 3 - sel;
+    }
+    if(threadIdx.x == 0)
+      ts.xsel[t] = sel;
+  }
+
+  // d = F(b - A x)
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_def(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    const S* fb = tail_vec(tp, sbase, t, 0);
+    const S* xa = tail_vec(tp, sbase, t, ts.xsel[t]);
+    S* fd = tail_vec(tp, sbase, t, 3);
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+      fd[i] = defect_row<V, S, false>(f.A, fb, xa, f.dm, i);
+  }
+
+  // b_{t+1} = F(R d_t), sol1_{t+1}, skip_pre_{t+1}
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_res(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    const TailLevel<V, S>& c = tp.lv[t + 1];
+    const S* fd = tail_vec(tp, sbase, t, 3);
+    const bool coarsest = (t + 2 == tp.count);
+    S* cbv = tail_vec(tp, sbase, t + 1, 0);
+    S* cxv = coarsest ? (S*)nullptr : tail_vec(tp, sbase, t + 1, 1);
+    double sq = 0.0;
+    for(uint32_t j = threadIdx.x; j < c.n; j += TAIL_NT)
+      sq += restrict_row<V, S, false>(f.R, fd, cbv, cxv, c.dinv, c.dm, j);
+    const double tot = block_sum<TAIL_NT>(sq, ts.sh);
+    if(threadIdx.x == 0)
+    {
+      if(!coarsest)
+      {
+        const int sk = skip_from_norm<S>(sqrt(tot));
+        ts.skip_pre[t + 1] = sk;
+        *(volatile int*)c.skip_pre = sk;
+      }
+      ts.xsel[t + 1] = 1;
+    }
+  }
+
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_crs(const TailParams<V, S>& tp, S* sbase, TailShared& ts)
+  {
+    const int cl = tp.count - 1;
+    coarse_block<S, TAIL_NT>(tail_vec(tp, sbase, cl, 0), tail_vec(tp, sbase, cl, 1), tp.lv[cl].n, tp.free_dofs,
+      tp.inv, tp.m);
+    if(threadIdx.x == 0)
+      ts.xsel[cl] = 1;
+  }
+
+  // x_t += F(P x_{t+1})
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_pro(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    S* xf = tail_vec(tp, sbase, t, ts.xsel[t]);
+    const S* xc = tail_vec(tp, sbase, t + 1, ts.xsel[t + 1]);
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+      xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
+  }
+
+  // post-smoothing (and the peak smoother) as a correction of x
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_post(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const TailLevel<V, S>& f = tp.lv[t];
+    const int steps = tp.steps;
+    const S* fb = tail_vec(tp, sbase, t, 0);
+    S* xf = tail_vec(tp, sbase, t, ts.xsel[t]);
+    S* fd = tail_vec(tp, sbase, t, 3);
+    S* ca = tail_vec(tp, sbase, t, 4);
+    S* cb = tail_vec(tp, sbase, t, 5);
+    double sq = 0.0;
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+      sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
+    const double tot = block_sum<TAIL_NT>(sq, ts.sh);
+    if(threadIdx.x == 0)
+    {
+      ts.skip_post = skip_from_norm<S>(sqrt(tot));
+      *(volatile int*)f.skip_post = ts.skip_post;
+    }
+    __syncthreads();
+    const bool skipped = ts.skip_post != 0;
+    if(steps == 1)
+    {
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+        xf[i] = S(add(Ac(xf[i]), skipped ? Ac(0) : Ac(ca[i])));
+    }
+    for(int k = 2; k <= steps; ++k)
+    {
+      const bool last = (k == steps);
+      for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+      {
+        const Ac cn = post2_row<V, S, false>(f.A, fd, ca, f.dinv, f.dm, skipped, i);
+        if(last)
+          xf[i] = S(add(Ac(xf[i]), cn));
+        else
+          cb[i] = S(cn);
+      }
+      if(!last)
+        __syncthreads();
+      S* tmp = ca;
+      ca = cb;
+      cb = tmp;
+    }
+  }
+
+  // The F- and W-cycle tail: the events of one run of the cycle on the tail levels, interpreted.
+  // (The V-cycle bottom runs in k_tail above, whose fixed sequence compiles without register
+  // spills; this interpreter costs about 0.1 ms per L10 solve more when it runs a V-cycle bottom.)
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(TAIL_NT) k_tail_prog(const __grid_constant__ TailParams<V, S> tp,
+    const uint8_t* __restrict__ prog, int nprog, const Scalars* __restrict__ sc)
+  {
+    extern __shared__ __align__(16) unsigned char tail_smem[];
+    __shared__ TailShared ts;
+    __shared__ uint8_t psh[TAIL_PROG_CHUNK];   // the program, a chunk at a time
+    if(gate_closed(sc))
+      return;
+    S* sbase = reinterpret_cast<S*>(tail_smem);
+    for(int e = threadIdx.x; e < min(nprog, TAIL_PROG_CHUNK); e += TAIL_NT)
+      psh[e] = prog[e];
+    // matrix data of all tail levels towards L2, asynchronously
+    {
+      // thread j issues chunks j, j + TAIL_NT, ... of the flattened chunk list
+      uint32_t g = 0;
+      for(int r = 0; r < tp.npf; ++r)
+      {
+        const uint32_t nb = tp.pf_bytes[r];
+        for(uint32_t off = 0; off < nb; off += TAIL_PF_CHUNK, ++g)
+          if(g % TAIL_NT == threadIdx.x)
+          {
+            const uint32_t sz = min(TAIL_PF_CHUNK, nb - off);
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                         :: "l"(static_cast<const unsigned char*>(tp.pf_ptr[r]) + off), "r"(sz) : "memory");
+          }
+      }
+    }
+    // the top level's input: b and sol1 = F(D .* b) written by the restriction above
+    if(tp.lv[0].in_smem)
+    {
+      S* b0 = tail_vec(tp, sbase, 0, 0);
+      S* x0 = tail_vec(tp, sbase, 0, 1);
+      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      {
+        b0[i] = tp.lv[0].b[i];
+        x0[i] = tp.lv[0].x[i];
+      }
+    }
+    if(threadIdx.x == 0)
+    {
+      ts.skip_pre[0] = *(volatile int*)tp.lv[0].skip_pre;
+      ts.xsel[0] = 1;
+    }
+    __syncthreads();
+    for(int e = 0; e < nprog; ++e)
+    {
+      if(e > 0 && e % TAIL_PROG_CHUNK == 0)
+      {
+        for(int k = threadIdx.x; k < min(nprog - e, TAIL_PROG_CHUNK); k += TAIL_NT)
+          psh[k] = prog[e + k];
+        __syncthreads();
+      }
+      const unsigned ev = psh[e % TAIL_PROG_CHUNK];
+      const int op = int(ev >> 4);
+      const int t = int(ev & 15u);
+      switch(op)
+      {
+        case EV_PRE: tail_pre(tp, sbase, t, ts); break;
+        case EV_DEF: tail_def(tp, sbase, t, ts); break;
+        case EV_RES: tail_res(tp, sbase, t, ts); break;
+        case EV_CRS: tail_crs(tp, sbase, ts); break;
+        case EV_PRO: tail_pro(tp, sbase, t, ts); break;
+        default: tail_post(tp, sbase, t, ts); break;
+      }
+      __syncthreads();
+    }
+    // the top level's solution goes to the global buffer the prolongation above reads
+    if(tp.lv[0].in_smem)
+    {
+      const S* xs = tail_vec(tp, sbase, 0, ts.xsel[0]);
+      S* xg = ts.xsel[0] == 1 ? tp.lv[0].x : tp.lv[0].x2;
+      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+        xg[i] = xs[i];
+    }
+  }
+
   // The same V-cycle bottom as k_tail, spread over a thread-block cluster of CT_CS blocks (one per
   // SM) so that larger levels fit: rows are dealt out cluster-wide, the passes are separated by the
   // cluster's hardware barrier (release/acquire at cluster scope, so every block sees the vectors
@@ -1005,6 +1240,84 @@ namespace fb
     int* skip_pre = nullptr;
     int* skip_post = nullptr;
   };
+
+  // _apply_rest(from, smooth_first) down to level stop: pre-smoothing and defect on every level
+  // but `from` when smooth_first is false (its defect is in place), restriction to the next level
+  static void ev_down(std::vector<CycEv>& ev, int from, bool smooth_first, int stop)
+  {
+    for(int l = from; l < stop; ++l)
+    {
+      if(smooth_first || l > from)
+      {
+        ev.push_back(CycEv{EV_PRE, uint8_t(l)});
+        ev.push_back(CycEv{EV_DEF, uint8_t(l)});
+      }
+      ev.push_back(CycEv{EV_RES, uint8_t(l)});
+    }
+  }
+
+  // _apply_prol(to, smooth_last) from level start - 1 up to `to`: prolongation, then
+  // post-smoothing except on level `to` when smooth_last is false
+  static void ev_up(std::vector<CycEv>& ev, int to, bool smooth_last, int start, bool top)
+  {
+    for(int l = start - 1; l >= to; --l)
+    {
+      ev.push_back(CycEv{EV_PRO, uint8_t(l)});
+      if(smooth_last || l > to)
+        ev.push_back(CycEv{uint8_t(top && l == 0 ? EV_POST_TOP : EV_POST), uint8_t(l)});
+    }
+  }
+
+  // _apply_smooth_peak(l): the peak smoother as a correction, then the new defect
+  static void ev_peak(std::vector<CycEv>& ev, int l)
+  {
+    ev.push_back(CycEv{EV_POST, uint8_t(l)});
+    ev.push_back(CycEv{EV_DEF, uint8_t(l)});
+  }
+
+  // One multigrid cycle over nl levels as events: V = rest(0) + coarse + prol(0); F and W the peak
+  // sequences of _apply_cycle_f / _apply_cycle_w (kernel/solver/multigrid.hpp:1356-1440)
+  static std::vector<CycEv> cycle_events(int cycle, int nl)
+  {
+    std::vector<CycEv> ev;
+    const int last = nl - 1;
+    const CycEv crs{EV_CRS, uint8_t(last)};
+    ev_down(ev, 0, true, last);
+    ev.push_back(crs);
+    if(cycle == FB_CYCLE_F)
+    {
+      for(int pk = last - 1; pk > 0; --pk)
+      {
+        ev_up(ev, pk, false, last, false);
+        ev_peak(ev, pk);
+        ev_down(ev, pk, false, last);
+        ev.push_back(crs);
+      }
+    }
+    else if(cycle == FB_CYCLE_W)
+    {
+      // the coarse solves number 2^last; before each one after the first, the peak level is the
+      // finest level whose counter is still zero below the deepest one that is not
+      std::vector<int> cnt(static_cast<size_t>(nl), 0);
+      const uint64_t num_cgs = uint64_t(1) << last;
+      for(uint64_t cgs = 1; cgs < num_cgs; ++cgs)
+      {
+        int pk = last;
+        while(pk > 0)
+          if(cnt[size_t(--pk)] == 0)
+            break;
+        for(int i = last - 1; i > pk; --i)
+          cnt[size_t(i)] = 0;
+        ++cnt[size_t(pk)];
+        ev_up(ev, pk, false, last, false);
+        ev_peak(ev, pk);
+        ev_down(ev, pk, false, last);
+        ev.push_back(crs);
+      }
+    }
+    ev_up(ev, 0, true, last, true);
+    return ev;
+  }
 } // namespace fb
 
 struct fb_solver
@@ -1037,6 +1350,9 @@ struct fb_solver
   cudaGraph_t vgraph = nullptr;
   cudaGraphExec_t vexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<fb::CycEv> events;            // one multigrid cycle
+  uint8_t* tail_prog = nullptr;             // tail kernel programs: events op << 4 | tail level
+  std::vector<uint32_t> seg_off, seg_len;   // program of each tail segment of `events`, in order
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
   double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
@@ -1371,21 +1687,6 @@ namespace fb
       bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
     }
 
-    // _apply_rest(from, smooth_first) down to level stop (exclusive of stop's own smoothing): with
-    // smooth_first == false, level `from` restricts the defect already in d_from
-    void down(int from, bool smooth_first, int stop, std::vector<void*>& xcur)
-    {
-      for(int l = from; l < stop; ++l)
-      {
-        if(smooth_first || l > from)
-        {
-          pre_smooth(l, xcur);
-          defect(l, xcur);
-        }
-        restrict_to(l);
-      }
-    }
-
     // exact solve on the coarsest level
     void coarse(std::vector<void*>& xcur)
     {
@@ -1475,27 +1776,9 @@ namespace fb
       }
     }
 
-    // _apply_prol(to, smooth_last) from level start - 1 up to `to`: prolongation, then
-    // post-smoothing except on level `to` when smooth_last == false
-    void up(int to, bool smooth_last, int start, bool pcg_top, std::vector<void*>& xcur)
-    {
-      for(int l = start - 1; l >= to; --l)
-      {
-        prolong(l, xcur);
-        if(smooth_last || l > to)
-          post_smooth(l, pcg_top && l == 0, xcur);
-      }
-    }
-
-    // _apply_smooth_peak(l): the peak smoother as a correction, then the new defect d_l
-    void peak(int l, std::vector<void*>& xcur)
-    {
-      post_smooth(l, false, xcur);
-      defect(l, xcur);
-    }
-
-    // the coarse-level tail kernel (single block or cluster) from level lt down and back up
-    void tail(int lt, std::vector<void*>& xcur)
+    // the coarse-level tail kernel (single block or cluster) for the events [e0, e1) of the cycle,
+    // which run on levels lt and below; segment `seg` is their program
+    void tail(int lt, size_t e0, size_t e1, size_t seg, std::vector<void*>& xcur)
     {
       const int nl = s->nlev;
       const int steps = std::max(1, s->cfg.smooth_steps);
@@ -1528,12 +1811,18 @@ namespace fb
         t.skip_pre = f.skip_pre;
         t.skip_post = f.skip_post;
         t.n = f.n;
-        xcur[size_t(l)] = (l + 1 == nl) ? f.x : (((steps - 1) % 2) ? f.x2 : f.x);
-        if(l + 1 < nl)
-          bytes += (steps + 3) * (csr_bytes(f.A, 3, 1) + f.n) + csr_bytes(f.R, 0, 3) + csr_bytes(f.P, 1, 1);
       }
+      {
+        // algorithmic bytes: the events as the grid kernels would run them
+        const bool was_dry = dry;
+        const uint64_t nlaunch = launches;
+        dry = true;
+        run_events(e0, e1, false, -1, xcur);
+        dry = was_dry;
+        launches = nlaunch;
+      }
+      xcur[size_t(lt)] = ((steps - 1) % 2) ? L(lt).x2 : L(lt).x;
       const size_t smem = tail_layout(tp, lt, !ctail);
-      bytes += double(s->nfree) * s->nfree * 8.0;
       if(dry)
         ;
       else if(ctail)
@@ -1554,66 +1843,54 @@ namespace fb
         if(e != cudaSuccess && s->launch_err == cudaSuccess)
           s->launch_err = e;
       }
-      else
+      else if(s->cfg.cycle == FB_CYCLE_V)
         k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
+      else
+        k_tail_prog<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->tail_prog + s->seg_off[seg], int(s->seg_len[seg]), s->sc);
       ++launches;
     }
 
+    // the cycle's events [e0, e1) as grid kernels, except the runs on levels lt and below (lt >= 0),
+    // which go to the tail kernel one launch each; pcg_top: the final post-smoothing forms z, r.z
+    void run_events(size_t e0, size_t e1, bool pcg_top, int lt, std::vector<void*>& xcur)
+    {
+      const std::vector<CycEv>& ev = s->events;
+      size_t seg = 0;
+      for(size_t i = e0; i < e1;)
+      {
+        const CycEv e = ev[i];
+        const int l = e.lvl;
+        if(lt >= 0 && l >= lt)
+        {
+          size_t j = i;
+          while(j < e1 && ev[j].lvl >= lt)
+            ++j;
+          tail(lt, i, j, seg++, xcur);
+          i = j;
+          continue;
+        }
+        switch(e.op)
+        {
+          case EV_PRE: pre_smooth(l, xcur); break;
+          case EV_DEF: defect(l, xcur); break;
+          case EV_RES: restrict_to(l); break;
+          case EV_CRS: coarse(xcur); break;
+          case EV_PRO: prolong(l, xcur); break;
+          case EV_POST: post_smooth(l, false, xcur); break;
+          default: post_smooth(l, pcg_top, xcur); break;
+        }
+        ++i;
+      }
+    }
+
     // One multigrid cycle from the top level; the top level's b, sol1 and skip_pre are in place.
-    // V: rest(top) + coarse (or the tail kernel) + prol(top).  F and W (no tail kernel): the peak
-    // sequences of _apply_cycle_f / _apply_cycle_w (kernel/solver/multigrid.hpp:1356-1440).
     void vcycle(bool pcg_top)
     {
       const int nl = s->nlev;
       std::vector<void*> xcur(static_cast<size_t>(nl));
       xcur[0] = L(0).x;
-      const int cyc = s->cfg.cycle;
-      if(cyc == FB_CYCLE_V)
-      {
-        const int lt = s->ctail_first >= 0 ? s->ctail_first : s->tail_first;
-        const int stop = lt >= 0 ? lt : nl - 1;
-        down(0, true, stop, xcur);
-        if(lt >= 0)
-          tail(lt, xcur);
-        else
-          coarse(xcur);
-        up(0, true, stop, pcg_top, xcur);
-        return;
-      }
-      const int last = nl - 1;
-      down(0, true, last, xcur);
-      if(cyc == FB_CYCLE_F)
-      {
-        for(int pk = last - 1; pk > 0; --pk)
-        {
-          coarse(xcur);
-          up(pk, false, last, false, xcur);
-          peak(pk, xcur);
-          down(pk, false, last, xcur);
-        }
-        coarse(xcur);
-      }
-      else
-      {
-        coarse(xcur);
-        std::vector<int> cnt(static_cast<size_t>(nl), 0);
-        const int num_cgs = 1 << last;
-        for(int cgs = 1; cgs < num_cgs; ++cgs)
-        {
-          int pk = last;
-          while(pk > 0)
-            if(cnt[size_t(--pk)] == 0)
-              break;
-          for(int i = last - 1; i > pk; --i)
-            cnt[size_t(i)] = 0;
-          ++cnt[size_t(pk)];
-          up(pk, false, last, false, xcur);
-          peak(pk, xcur);
-          down(pk, false, last, xcur);
-          coarse(xcur);
-        }
-      }
-      up(0, true, last, pcg_top, xcur);
+      const int lt = s->ctail_first >= 0 ? s->ctail_first : s->tail_first;
+      run_events(0, s->events.size(), pcg_top, lt, xcur);
     }
 
     const DevMat& A64() { return s->cfg.precision == FB_PREC_F64 ? L(0).A : L(0).A64; }
@@ -1687,6 +1964,7 @@ namespace fb
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tail<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
+    FB_CUDA(cudaFuncSetAttribute(k_tail_prog<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     return FB_OK;
   }
 
@@ -2051,13 +2329,43 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       }
   if(s->ctail_first >= 0)
     FB_TRY(dalloc(s.get(), (void**)&s->cred, sizeof(double) * 2 * MAX_TAIL * CT_CS));
-  if(cfg.tail_rows > 0 && s->ctail_first < 0 && cfg.cycle == FB_CYCLE_V)
+  if(cfg.tail_rows > 0 && s->ctail_first < 0)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.tail_rows))
       {
         s->tail_first = (s->nlev - l <= MAX_TAIL) ? l : -1;
         break;
       }
+  // the cycle as events, and the tail kernel's program for each run of events on the tail levels
+  // (identical runs share one program)
+  s->events = cycle_events(cfg.cycle, s->nlev);
+  if(s->tail_first >= 0 && cfg.cycle != FB_CYCLE_V)
+  {
+    const int lt = s->tail_first;
+    std::vector<uint8_t> progs;
+    std::map<std::vector<uint8_t>, uint32_t> seen;
+    for(size_t i = 0; i < s->events.size();)
+    {
+      if(s->events[i].lvl < lt)
+      {
+        ++i;
+        continue;
+      }
+      std::vector<uint8_t> pg;
+      for(; i < s->events.size() && s->events[i].lvl >= lt; ++i)
+        pg.push_back(uint8_t((s->events[i].op << 4) | (s->events[i].lvl - lt)));
+      auto it = seen.find(pg);
+      if(it == seen.end())
+      {
+        it = seen.emplace(pg, uint32_t(progs.size())).first;
+        progs.insert(progs.end(), pg.begin(), pg.end());
+      }
+      s->seg_off.push_back(it->second);
+      s->seg_len.push_back(uint32_t(pg.size()));
+    }
+    FB_TRY(dalloc(s.get(), (void**)&s->tail_prog, progs.size()));
+    FB_CUDA(cudaMemcpy(s->tail_prog, progs.data(), progs.size(), cudaMemcpyHostToDevice));
+  }
   Scalars h0;
   std::memset(&h0, 0, sizeof(h0));
   h0.tol_rel = cfg.tol_rel;

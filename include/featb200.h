@@ -192,17 +192,17 @@ typedef struct
   int rows_per_block;   /* batch solver: rows (threads) per block of the V-cycle passes, a multiple
                            of 32 up to 512; 0 = picked per level by the autotuner at creation */
   int tail_rows;        /* levels (below the finest) with at most this many rows, down to the
-                           coarsest, run in one single-block kernel per V-cycle; 0 = off */
+                           coarsest, run in one single-block kernel per visit of the cycle (a
+                           V-cycle bottom, or an F/W sub-cycle with its peak smoothing); 0 = off */
   int tma_rows;         /* levels with at least this many rows use the TMA-staged persistent
                            passes (bulk copies into shared memory); 0 = off */
   int cluster_rows;     /* levels (below the finest) with at most this many rows, down to the
                            coarsest, run in one kernel on a cluster of 8 thread blocks (8 SMs) per
                            V-cycle, passes separated by the cluster barrier; takes precedence over
-                           tail_rows; 0 = off (default: measured slower than the single-block tail
-                           on B200 for every threshold) */
+                           tail_rows; V-cycle only; 0 = off (default: measured slower than the
+                           single-block tail on B200 for every threshold) */
   int cycle;            /* FB_CYCLE_V (default), FB_CYCLE_F or FB_CYCLE_W: the multigrid cycle of
-                           MultiGrid::_apply_cycle_v/_f/_w (kernel/solver/multigrid.hpp:1350-1440);
-                           F and W cycles run without the tail kernels */
+                           MultiGrid::_apply_cycle_v/_f/_w (kernel/solver/multigrid.hpp:1350-1440) */
   int tma_window;       /* the window of the gathered vector that a TMA-staged chunk reads:
                            0 (default) = neither: the row sums gather from global memory;
                            1 = staged in shared memory with the chunk; 2 = bulk-prefetched into L2

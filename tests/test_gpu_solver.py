@@ -223,10 +223,12 @@ def test_fw_cycles_match_live_reference(featlib, cuda, cycle, level, ordering, g
         sol = np.load(os.path.join(tmp, "sol.npy"))
         vc = np.load(os.path.join(tmp, "vcycle.npy"))
     lv = conv(levels)
-    s, x, st = _solve(fb, lv, rhs, ordering=ordering, use_graph=graph, cycle=cycle)
-    assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc)
-    assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
-    assert rel_err(x, sol) <= PARITY
+    # default tail threshold, no tail kernel, every level below the finest in the tail kernel
+    for tail in (None, 0, 1 << 20):
+        s, x, st = _solve(fb, lv, rhs, ordering=ordering, use_graph=graph, cycle=cycle, tail_rows=tail)
+        assert np.array_equal(s.apply_precond(fb.DenseVector(rhs)).elements, vc), tail
+        assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
+        assert rel_err(x, sol) <= PARITY
 
 
 @pytest.mark.parametrize("cycle", ["F", "W"])
