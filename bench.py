@@ -480,6 +480,8 @@ def main():
                     help="levels with at most this many rows run in the cluster tail kernel (0 = off)")
     ap.add_argument("--tma-window", type=int, choices=[0, 1, 2], default=0,
                     help="gathered-vector window of a TMA chunk: 2 prefetch into L2, 1 stage in shared memory, 0 none")
+    ap.add_argument("--diagonal", type=int, choices=[0, 1], default=1,
+                    help="diagonal storage of system matrices on at most 27 diagonals (1) or sliced ELL (0)")
     ap.add_argument("--cycle", choices=["V", "F", "W"], default="V",
                     help="multigrid cycle of the preconditioner (the reference's MultiGridCycle)")
     ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
@@ -514,7 +516,8 @@ def main():
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
-                                    cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle)
+                                    cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle,
+                                    diagonal=args.diagonal)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
@@ -582,7 +585,8 @@ def main():
 
     extra = {}
     if not args.no_plain and precision != "f64":
-        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window)
+        plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window,
+                                       diagonal=args.diagonal)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush()

@@ -394,6 +394,11 @@ namespace fb
     __device__ void finish(double total) const { sc->alpha = sc->gamma / total; }
   };
 
+  // passes over a level's system matrix (the only matrices kept in diagonal storage)
+  template<class Op> struct OnSystem { static constexpr bool value = true; };
+  template<typename V, typename S> struct OnSystem<OpRestrict<V, S>> { static constexpr bool value = false; };
+  template<typename V, typename S> struct OnSystem<OpProlong<V, S>> { static constexpr bool value = false; };
+
   // ------------------------------------------------------------------ coarse-level tail
   // The part of a multigrid cycle below the tail threshold (levels whose row count is at most the
   // threshold, down to the coarsest) in ONE block of TAIL_NT threads: block-stride loops separated
@@ -1222,11 +1227,12 @@ namespace fb
     // only; xwin = 0: no window (gathers from global memory)
     uint32_t* xlo = nullptr;
     uint32_t xwin = 0;
+    int32_t* doff = nullptr;                // diagonal storage: the diagonals' offsets
   };
 
   template<typename V> DCsr<V> view(const DevMat& m)
   {
-    return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw};
+    return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw, m.doff};
   }
 
   struct DevLevel
@@ -1403,9 +1409,10 @@ namespace fb
   }
 
   // CSR -> the device layout (build_sell), values converted to the storage precision.
-  static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty)
+  static fb_status upload_mat(fb_solver* s, DevMat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty,
+                              bool allow_diag = false)
   {
-    const HostSell H = build_sell(M, empty);
+    const HostSell H = build_sell(M, empty, true, allow_diag);
     const uint32_t ns = (H.rows + 31u) / 32u;
     d.rows = H.rows;
     d.cols = H.cols;
@@ -1417,7 +1424,14 @@ namespace fb
       d.kmax = std::max(d.kmax, (H.soff[sl + 1] - H.soff[sl]) / 32u);
     const size_t vb = valsize_of(prec);
     const size_t cb = H.narrow ? 2 : 4;
-    d.bytes = double(H.entries) * double(vb + cb) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
+    d.bytes = double(H.entries) * double(vb + (H.doff.empty() ? cb : 0)) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
+    if(!H.doff.empty())
+    {
+      // diagonal storage: values and the offsets only (the grid kernels serve it)
+      FB_TRY(dalloc(s, (void**)&d.doff, sizeof(int32_t) * H.doff.size()));
+      FB_CUDA(cudaMemcpy(d.doff, H.doff.data(), sizeof(int32_t) * H.doff.size(), cudaMemcpyHostToDevice));
+    }
+    else
     {
       // column window of every TMA chunk (real entries; narrow padding reads the row itself),
       // start rounded down to 4 entries (16-byte copies for FP32 and FP64 vectors)
@@ -1468,7 +1482,9 @@ namespace fb
     FB_TRY(dalloc(s, (void**)&d.soff, sizeof(uint32_t) * H.soff.size()));
     FB_CUDA(cudaMemcpy(d.soff, H.soff.data(), sizeof(uint32_t) * H.soff.size(), cudaMemcpyHostToDevice));
     const size_t ne = std::max<size_t>(1, size_t(H.entries));
-    if(H.narrow)
+    if(d.doff)
+      ;
+    else if(H.narrow)
     {
       FB_TRY(dalloc(s, (void**)&d.dcol, 2 * ne));
       if(H.entries)
@@ -1520,19 +1536,22 @@ namespace fb
     cudaStream_t st;
     bool dry = false;          // count launches and bytes only
 
+    // column index bytes per entry
+    static uint32_t colbytes(const DevMat& m) { return m.doff ? 0u : (m.dcol ? 2u : 4u); }
+
     bool use_tma_f64(const DevMat& m) const
     {
-      if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
+      if(s->cfg.tma_rows <= 0 || !m.kmax || (m.doff && m.kw != 9 && m.kw != 27) || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(tma_stages<double>()) * tma_stage_bytes<double>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
+      return uint64_t(tma_stages<double>()) * tma_stage_bytes<double>(m.kmax, colbytes(m)) <= TMA_SMEM_MAX;
     }
 
     // the TMA-staged pass serves matrices of at least tma_rows rows whose stages fit
     bool use_tma(const DevMat& m) const
     {
-      if(s->cfg.tma_rows <= 0 || !m.kmax || m.rows < uint32_t(s->cfg.tma_rows))
+      if(s->cfg.tma_rows <= 0 || !m.kmax || (m.doff && m.kw != 9 && m.kw != 27) || m.rows < uint32_t(s->cfg.tma_rows))
         return false;
-      return uint64_t(tma_stages<V>()) * tma_stage_bytes<V>(m.kmax, m.dcol != nullptr) <= TMA_SMEM_MAX;
+      return uint64_t(tma_stages<V>()) * tma_stage_bytes<V>(m.kmax, colbytes(m)) <= TMA_SMEM_MAX;
     }
     template<typename VV, typename XS, class Op>
     void tma(const DevMat& m, const void* x, const Op& op)
@@ -1542,10 +1561,10 @@ namespace fb
       uint32_t xw = s->cfg.tma_window ? m.xwin : 0u;
       const int xstage = s->cfg.tma_window == 1 ? 1 : 0;
       if(xw && xstage &&
-         uint64_t(tma_stages<VV>()) * (tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + uint64_t(xw) * sizeof(XS)) >
+         uint64_t(tma_stages<VV>()) * (tma_stage_bytes<VV>(m.kmax, colbytes(m)) + uint64_t(xw) * sizeof(XS)) >
            TMA_SMEM_MAX)
         xw = 0;
-      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, m.dcol != nullptr) + (xstage ? xw * uint32_t(sizeof(XS)) : 0u);
+      const uint32_t sb = tma_stage_bytes<VV>(m.kmax, colbytes(m)) + (xstage ? xw * uint32_t(sizeof(XS)) : 0u);
       const size_t smem = size_t(tma_stages<VV>()) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
@@ -1553,7 +1572,19 @@ namespace fb
       const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
       // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
       const uint32_t nxa = (m.cols + 8u) & ~3u;
-      // the 2D Q1 stencil (ELL of width 9) runs the fully unrolled row sum
+      // diagonal storage of the 2D / 3D Q1 stencils (9 / 27 diagonals); the 2D Q1 stencil in ELL of
+      // width 9 runs the fully unrolled row sum
+      if constexpr(OnSystem<Op>::value)
+        if(m.doff)
+        {
+          if(m.kw == 9)
+            k_tma_pass<VV, XS, Op, 9, true><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded,
+              m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
+          else
+            k_tma_pass<VV, XS, Op, 27, true><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded,
+              m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
+          return;
+        }
       if(m.kw == 9)
         k_tma_pass<VV, XS, Op, 9><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
                                                              xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
@@ -1940,6 +1971,14 @@ namespace fb
     }
   };
 
+  template<typename V, typename S, class Op>
+  static fb_status set_tma_attr_dg(int mx)
+  {
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, Op, 9, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, Op, 27, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    return FB_OK;
+  }
+
   // dynamic shared memory above 48 KB for the TMA-staged passes
   template<typename V, typename S>
   static fb_status set_tma_attrs()
@@ -1963,6 +2002,13 @@ namespace fb
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, OpProlong<V, S>, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     FB_CUDA(cudaFuncSetAttribute(k_tma_pass<double, double, OpPcgQ, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_TRY((set_tma_attr_dg<V, S, OpSmooth<V, S>>(mx)));
+    FB_TRY((set_tma_attr_dg<V, S, OpDefect<V, S>>(mx)));
+    FB_TRY((set_tma_attr_dg<V, S, OpPost1<V, S>>(mx)));
+    FB_TRY((set_tma_attr_dg<V, S, OpPost2<V, S, false, false>>(mx)));
+    FB_TRY((set_tma_attr_dg<V, S, OpPost2<V, S, true, false>>(mx)));
+    FB_TRY((set_tma_attr_dg<V, S, OpPost2<V, S, true, true>>(mx)));
+    FB_TRY((set_tma_attr_dg<double, double, OpPcgQ>(mx)));
     FB_CUDA(cudaFuncSetAttribute(k_tail<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     FB_CUDA(cudaFuncSetAttribute(k_tail_prog<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     return FB_OK;
@@ -2101,6 +2147,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->cycle = FB_CYCLE_V;
   c->tma_rows = 1000;
   c->tma_window = 0;
+  c->diagonal = 1;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -2243,9 +2290,9 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     D.n = H.A.rows;
     max_blocks = std::max(max_blocks, blocks(D.n));
     HostCsr A = permute(H.A, pf, inv_f);
-    FB_TRY(upload_mat(s.get(), D.A, A, prec, &dms[size_t(l)]));
+    FB_TRY(upload_mat(s.get(), D.A, A, prec, &dms[size_t(l)], cfg.diagonal != 0));
     if(l == 0 && prec != FB_PREC_F64)
-      FB_TRY(upload_mat(s.get(), D.A64, A, FB_PREC_F64, &dms[size_t(l)]));
+      FB_TRY(upload_mat(s.get(), D.A64, A, FB_PREC_F64, &dms[size_t(l)], cfg.diagonal != 0));
     if(l + 1 < s->nlev)
     {
       const std::vector<uint32_t>& pc = s->perms[size_t(l + 1)];
@@ -2750,7 +2797,7 @@ namespace fb
     std::vector<uint8_t> dm(A.rows);
     for(uint32_t k = 0; k < A.rows; ++k)
       dm[k] = H.dmask[pf.empty() ? k : pf[k]];
-    const HostSell S = build_sell(permute(A, pf, inv), &dm);
+    const HostSell S = build_sell(permute(A, pf, inv), &dm, true, s->cfg.diagonal != 0);
     std::vector<uint32_t> slot(std::max<size_t>(1, A.col.size()), 0xffffffffu);
     std::vector<uint32_t> diag(std::max<uint32_t>(1, A.rows), 0xffffffffu);
     for(uint32_t r = 0; r < A.rows; ++r)
@@ -2761,7 +2808,7 @@ namespace fb
         if(A.col[j] == r && diag[k] == 0xffffffffu)
           diag[k] = j;
         if(!dm[k])
-          slot[j] = S.soff[k / 32u] + (j - A.rp[r]) * 32u + (k % 32u);
+          slot[j] = uint32_t(S.slot(k, j - A.rp[r], inv.empty() ? A.col[j] : inv[A.col[j]]));
       }
     }
     uint32_t* ds = nullptr;

@@ -15,6 +15,9 @@ namespace fb
   // slot at index `cols`, or the row itself for narrow storage).  Rows whose result the unit
   // filter discards (Dirichlet rows) are stored empty.  Column indices are either absolute u32
   // (`col`) or, for square matrices whose |col - row| fits, int16 offsets from the row (`dcol`).
+  // Diagonal storage (`doff`): uniform width kw, entry k of every row on the diagonal doff[k]
+  // (column = row + doff[k]; out-of-range columns of padding entries read the row itself), no
+  // column indices at all.
   template<typename V>
   struct DCsr
   {
@@ -24,6 +27,7 @@ namespace fb
     const V* val;
     uint32_t rows;
     uint32_t kw;            // uniform entries per row (ELL: slice s starts at 32*kw*s), 0 = sliced
+    const int32_t* doff = nullptr;   // diagonal offsets (diagonal storage), or nullptr
   };
 
 
@@ -68,7 +72,13 @@ namespace fb
         {
           const uint32_t e = base + (k0 + u) * 32u;
           v[u] = to_acc(ldg_v(M.val + e));
-          c[u] = M.dcol ? uint32_t(int32_t(row) + int32_t(__ldg(M.dcol + e))) : __ldg(M.col + e);
+          if(M.doff)
+          {
+            const uint32_t cc = uint32_t(int32_t(row) + __ldg(M.doff + k0 + u));
+            c[u] = cc < M.rows ? cc : row;
+          }
+          else
+            c[u] = M.dcol ? uint32_t(int32_t(row) + int32_t(__ldg(M.dcol + e))) : __ldg(M.col + e);
         }
       A xv[U];
       #pragma unroll

@@ -185,9 +185,71 @@ namespace fb
     return d;
   }
 
-  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow)
+  uint64_t HostSell::slot(uint32_t r, uint32_t j, uint32_t c) const
+  {
+    if(!doff.empty())
+    {
+      const int32_t o = int32_t(int64_t(c) - int64_t(r));
+      const uint32_t k = uint32_t(std::lower_bound(doff.begin(), doff.end(), o) - doff.begin());
+      return uint64_t(soff[r / 32u]) + uint64_t(k) * 32u + (r % 32u);
+    }
+    return uint64_t(soff[r / 32u]) + uint64_t(j) * 32u + (r % 32u);
+  }
+
+  // Diagonal storage of a square matrix (see HostSell); false when it does not qualify or would
+  // store more than 12.5% padding.
+  static bool build_diag(HostSell& H, const HostCsr& M, const std::vector<uint8_t>* empty)
+  {
+    const uint32_t n = M.rows, ns = (n + 31u) / 32u;
+    std::vector<int32_t> offs;
+    uint64_t nnz = 0;
+    for(uint32_t r = 0; r < n; ++r)
+    {
+      if(empty && (*empty)[r])
+        continue;
+      int64_t prev = INT64_MIN;
+      for(uint32_t j = M.rp[r]; j < M.rp[r + 1]; ++j)
+      {
+        const int64_t d = int64_t(M.col[j]) - int64_t(r);
+        if(d <= prev)
+          return false;
+        prev = d;
+        if(std::find(offs.begin(), offs.end(), int32_t(d)) == offs.end())
+        {
+          if(offs.size() >= DIAG_MAX)
+            return false;
+          offs.push_back(int32_t(d));
+        }
+      }
+      nnz += M.rp[r + 1] - M.rp[r];
+    }
+    const uint32_t K = uint32_t(offs.size());
+    if(!K || uint64_t(K) * 32u * ns > nnz + nnz / 8)
+      return false;
+    std::sort(offs.begin(), offs.end());
+    H.rows = n;
+    H.cols = M.cols;
+    H.kw = K;
+    H.nnz = nnz;
+    H.narrow = false;
+    H.doff = offs;
+    H.soff.assign(size_t(ns) + 1, 0u);
+    for(uint32_t sl = 0; sl <= ns; ++sl)
+      H.soff[sl] = sl * 32u * K;
+    H.entries = H.soff[ns];
+    H.val.assign(H.entries, 0.0);
+    for(uint32_t r = 0; r < n; ++r)
+      if(!(empty && (*empty)[r]))
+        for(uint32_t j = M.rp[r]; j < M.rp[r + 1]; ++j)
+          H.val[H.slot(r, j - M.rp[r], M.col[j])] = M.val[j];
+    return true;
+  }
+
+  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow, bool allow_diag)
   {
     HostSell H;
+    if(allow_diag && M.rows == M.cols && build_diag(H, M, empty))
+      return H;
     const uint32_t n = M.rows, ns = (n + 31u) / 32u;
     H.rows = n;
     H.cols = M.cols;

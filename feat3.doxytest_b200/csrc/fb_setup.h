@@ -54,6 +54,11 @@ namespace fb
   // stores at most 12.5% more entries).  Rows flagged in `empty` are stored without entries;
   // padding has value 0 and the zero-slot column `cols` (or offset 0 for narrow storage).  Square
   // matrices whose |col - row| fits in int16 get 2-byte column offsets (dcol) instead of col.
+  // Diagonal storage (allow_diag, square matrices): when every stored entry lies on one of at most
+  // DIAG_MAX diagonals and every row's columns are strictly increasing, the matrix is stored as
+  // plain ELL whose entry k of every row is the diagonal doff[k] (column = row + doff[k]), without
+  // column indices: a row's entries keep their stored order, the diagonals it lacks hold value 0.
+  constexpr uint32_t DIAG_MAX = 27;
   struct HostSell
   {
     uint32_t rows = 0, cols = 0, kw = 0;
@@ -62,9 +67,13 @@ namespace fb
     std::vector<uint32_t> soff;
     std::vector<uint32_t> col;
     std::vector<int16_t> dcol;
+    std::vector<int32_t> doff;   // diagonal storage: the offsets, ascending; empty otherwise
     std::vector<double> val;
+    // slot of entry j (column c) of row r, stored order within the row
+    uint64_t slot(uint32_t r, uint32_t j, uint32_t c) const;
   };
-  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow = true);
+  HostSell build_sell(const HostCsr& M, const std::vector<uint8_t>* empty, bool allow_narrow = true,
+                      bool allow_diag = false);
 } // namespace fb
 
 // the opaque hierarchy handle of the C ABI: levels finest first, as pushed by the caller

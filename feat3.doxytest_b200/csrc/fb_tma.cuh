@@ -121,11 +121,12 @@ namespace fb
     return sum;
   }
 
-  // Shared memory bytes of one stage for a matrix of (maximum) width K.
+  // Shared memory bytes of one stage for a matrix of (maximum) width K with cbytes bytes of column
+  // index per entry (4 absolute, 2 row-relative, 0 diagonal storage).
   template<typename V>
-  __host__ __device__ __forceinline__ uint32_t tma_stage_bytes(uint32_t K, bool narrow)
+  __host__ __device__ __forceinline__ uint32_t tma_stage_bytes(uint32_t K, uint32_t cbytes)
   {
-    return uint32_t(TMA_NT) * K * uint32_t(sizeof(V) + (narrow ? 2u : 4u));
+    return uint32_t(TMA_NT) * K * uint32_t(sizeof(V) + cbytes);
   }
 
   // Generic persistent pass: for every row i < A.rows, op(i, sum_i, op.pre(i)) with
@@ -136,11 +137,15 @@ namespace fb
   // ends at nxa, the entries the vector's allocation holds, at the latest).  xstage != 0: that window
   // is staged in shared memory with the chunk; xstage == 0: it is only bulk-prefetched into L2 when
   // the chunk's copies are issued, so the gathers find it there.
-  template<typename V, typename S, class Op, int KC = 0>
+  // DG: diagonal storage of width KC: only the values are copied; a row's gathers x[i + doff[k]]
+  // depend on no staged data, so they are issued before the wait for the chunk's copies.
+  template<typename V, typename S, class Op, int KC = 0, bool DG = false>
   __global__ void __launch_bounds__(TMA_NT) k_tma_pass(DCsr<V> A, const S* __restrict__ x, uint32_t padded_rows,
     uint32_t kst, const uint32_t* __restrict__ xlo, uint32_t xw, uint32_t nxa, int xstage, Op op, RedSlot slot,
     int* err)
   {
+    static_assert(!DG || KC > 0, "diagonal storage needs a fixed width");
+    typedef typename ValueTraits<V>::acc Ac;
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
     __shared__ double sh[32];
@@ -150,7 +155,15 @@ namespace fb
     constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
-    const uint32_t mb = tma_stage_bytes<V>(kst, narrow);
+    const uint32_t cbytes = DG ? 0u : (narrow ? 2u : 4u);
+    int32_t doff[DG ? KC : 1];
+    if(DG)
+    {
+      #pragma unroll
+      for(int u = 0; u < (DG ? KC : 1); ++u)
+        doff[u] = __ldg(A.doff + u);
+    }
+    const uint32_t mb = tma_stage_bytes<V>(kst, cbytes);
     const uint32_t sb = mb + (xlo && xstage ? xw * uint32_t(sizeof(S)) : 0u);
     const uint32_t nsl = padded_rows / 32u;
     const uint32_t nch = (padded_rows + TMA_NT - 1) / TMA_NT;
@@ -169,7 +182,7 @@ namespace fb
         ne = __ldg(A.soff + min(c * SPC + SPC, nsl)) - e0;
       }
       const uint32_t vb = ne * uint32_t(sizeof(V));
-      const uint32_t cb = ne * (narrow ? 2u : 4u);
+      const uint32_t cb = ne * cbytes;
       unsigned char* st = tma_smem + size_t(s) * sb;
       uint32_t x0 = 0, xb = 0;
       if(xlo && ne)
@@ -190,7 +203,9 @@ namespace fb
       if(xb)
         bulk_g2s(st + mb, x + x0, xb, &bar[s]);
       bulk_g2s(st, A.val + e0, vb, &bar[s]);
-      if(narrow)
+      if(DG)
+        ;
+      else if(narrow)
         bulk_g2s(st + size_t(TMA_NT) * kst * sizeof(V), A.dcol + e0, cb, &bar[s]);
       else
         bulk_g2s(st + size_t(TMA_NT) * kst * sizeof(V), A.col + e0, cb, &bar[s]);
@@ -216,6 +231,20 @@ namespace fb
     {
       const int s = int(it % NS);
       const uint32_t par = (it / NS) & 1u;
+      const uint32_t i = c * TMA_NT + threadIdx.x;
+      // diagonal storage: the row's vector entries and gathers go out before the wait
+      Ac xv[DG ? KC : 1];
+      typename Op::Pre dpre{};
+      if(DG && i < A.rows)
+      {
+        dpre = op.pre(i);
+        #pragma unroll
+        for(int u = 0; u < (DG ? KC : 1); ++u)
+        {
+          const uint32_t cc = uint32_t(int32_t(i) + doff[u]);
+          xv[u] = Ac(__ldg(x + (cc < A.rows ? cc : i)));
+        }
+      }
       // one warp polls the barrier; the others wait in __syncthreads without taking issue slots
       bool ok = true;
       if(threadIdx.x < 32)
@@ -238,8 +267,20 @@ namespace fb
       const unsigned char* st = tma_smem + size_t(s) * sb;
       const V* sv = reinterpret_cast<const V*>(st);
       const void* scol = st + size_t(TMA_NT) * kst * sizeof(V);
-      const uint32_t i = c * TMA_NT + threadIdx.x;
-      if(i < A.rows)
+      if(DG)
+      {
+        if(i < A.rows)
+        {
+          // entries in stored order (ascending diagonals), each product and sum rounded
+          const uint32_t base = (threadIdx.x >> 5) * 32u * uint32_t(KC) + (threadIdx.x & 31u);
+          Ac sum = Ac(0);
+          #pragma unroll
+          for(int u = 0; u < (DG ? KC : 1); ++u)
+            sum = add(sum, mul(to_acc(sv[base + uint32_t(u) * 32u]), xv[u]));
+          part += op(i, sum, dpre);
+        }
+      }
+      else if(i < A.rows)
       {
         // the row's own vector entries are loaded first; they do not depend on the gathers
         const typename Op::Pre pre = op.pre(i);

@@ -32,7 +32,8 @@ class SolverConfig(C.Structure):
                 ("smooth_steps", C.c_int), ("tol_rel", C.c_double), ("tol_abs", C.c_double),
                 ("max_iter", C.c_int), ("min_iter", C.c_int), ("use_graph", C.c_int),
                 ("rows_per_block", C.c_int), ("tail_rows", C.c_int), ("tma_rows", C.c_int),
-                ("cluster_rows", C.c_int), ("cycle", C.c_int), ("tma_window", C.c_int)]
+                ("cluster_rows", C.c_int), ("cycle", C.c_int), ("tma_window", C.c_int),
+                ("diagonal", C.c_int)]
 
 
 class SolveInfo(C.Structure):

@@ -227,6 +227,11 @@ class PCG:
         thread blocks (0 = off; takes precedence over set_tail_rows)."""
         self.cfg.cluster_rows = int(rows)
 
+    def set_diagonal(self, on):
+        """Store system matrices that lie on at most 27 diagonals of the device numbering as
+        diagonals without column indices (1, default) or always as sliced ELL (0)."""
+        self.cfg.diagonal = int(bool(on))
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -338,7 +343,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None, cycle="V"):
+                        cluster_rows=None, cycle="V", diagonal=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -364,6 +369,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_tma_window(tma_window)
     if cluster_rows is not None:
         s.set_cluster_rows(cluster_rows)
+    if diagonal is not None:
+        s.set_diagonal(diagonal)
     h.init()
     s.init()
     return s

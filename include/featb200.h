@@ -207,6 +207,11 @@ typedef struct
                            0 (default) = neither: the row sums gather from global memory;
                            1 = staged in shared memory with the chunk; 2 = bulk-prefetched into L2
                            when the chunk's copies are issued.  Both measured slower on B200 */
+  int diagonal;         /* 1 (default): a level's system matrix whose entries lie on at most 27
+                           diagonals of the device numbering, with strictly increasing columns in
+                           every row (structured grids numbered lexicographically), is stored as
+                           its diagonals without column indices (row sums keep the stored order;
+                           missing diagonals hold zeros); 0 = always sliced ELL */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,

@@ -92,10 +92,34 @@ def test_fp64_full_size_against_oracle(featlib, cuda, oracle_lib):
     mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
     x_ref, info = mg.solve(b)
     z_ref = mg.vcycle(b)
-    s, x, st = _solve(fb, levels, b, ordering="rcm")
-    assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref)
-    assert st == fb.Status.success and s.get_num_iter() == info["iters"]
-    assert rel_err(x, x_ref) <= PARITY
+    # rcm: sliced ELL; native (lexicographic numbering): diagonal storage of the system matrices
+    for ordering, diagonal in (("rcm", 1), ("native", 1), ("native", 0)):
+        s, x, st = _solve(fb, levels, b, ordering=ordering, diagonal=diagonal)
+        assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref), (ordering, diagonal)
+        assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+        assert rel_err(x, x_ref) <= PARITY
+
+
+@pytest.mark.parametrize("level", [6, 8])
+@pytest.mark.parametrize("graph", [True, False])
+def test_diagonal_storage_against_oracle(featlib, cuda, oracle_lib, level, graph):
+    """Diagonal storage (native numbering of the generated problems): bitwise V-cycle and iterates
+    against the C restatement, with and without the tail kernel, F and W cycles included."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(level, 2, rhs="gauss", gauss=AS.gauss_params(2, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    z_ref = mg.vcycle(b)
+    for tail in (None, 0):
+        s, x, st = _solve(fb, levels, b, use_graph=graph, tail_rows=tail, tma_rows=64)
+        assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref), tail
+        assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+        assert rel_err(x, x_ref) <= PARITY
+    for cycle in ("F", "W"):
+        s_e, x_e, _ = _solve(fb, levels, b, cycle=cycle, diagonal=0)
+        s_d, x_d, _ = _solve(fb, levels, b, cycle=cycle, diagonal=1)
+        assert np.array_equal(x_d, x_e) and s_d.get_num_iter() == s_e.get_num_iter()
 
 
 @pytest.mark.parametrize("precision", ["f32", "f32_bf16"])
