@@ -482,6 +482,8 @@ def main():
                     help="gathered-vector window of a TMA chunk: 2 prefetch into L2, 1 stage in shared memory, 0 none")
     ap.add_argument("--diagonal", type=int, choices=[0, 1], default=1,
                     help="diagonal storage of system matrices on at most 27 diagonals (1) or sliced ELL (0)")
+    ap.add_argument("--pdl", type=int, choices=[0, 1], default=1,
+                    help="programmatic dependent launch of the solve's kernels (1) or plain stream order (0)")
     ap.add_argument("--cycle", choices=["V", "F", "W"], default="V",
                     help="multigrid cycle of the preconditioner (the reference's MultiGridCycle)")
     ap.add_argument("--ordering", choices=["native", "rcm"], default="rcm",
@@ -517,7 +519,7 @@ def main():
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
                                     cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle,
-                                    diagonal=args.diagonal)
+                                    diagonal=args.diagonal, pdl=args.pdl)
     info_lv = solver.level_info()
 
     stream = torch.cuda.current_stream()
@@ -586,7 +588,7 @@ def main():
     extra = {}
     if not args.no_plain and precision != "f64":
         plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window,
-                                       diagonal=args.diagonal)
+                                       diagonal=args.diagonal, pdl=args.pdl)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush()

@@ -56,6 +56,16 @@ namespace fb
   __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
   __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
 
+  // ------------------------------------------------------------------ programmatic dependent launch
+  // A kernel launched with programmatic stream serialisation may be scheduled before its
+  // predecessor in the stream has finished; pdl_wait blocks until the predecessor has completed
+  // and its writes are visible (a no-op for a kernel launched without the attribute).  No kernel
+  // signals its dependents early (griddepcontrol.launch_dependents): the successor is released as
+  // the predecessor's blocks exit, so only its launch and its work before pdl_wait overlap.  (An
+  // early signal at kernel start was measured faster but gave wrong V-cycles on B200 when FP32
+  // sliced-ELL staged passes ran with the single-block tail; the cause was not found.)
+  __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
   // ------------------------------------------------------------------ deterministic reductions
   // Block sum in a fixed order (warp shuffles, then warp 0 over the per-warp partials).
   template<int NT>

@@ -63,6 +63,7 @@ namespace fb
     S* __restrict__ xo, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip,
     const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     if(gate_closed(sc))
       return;
     const uint32_t i = blockIdx.x * NT + threadIdx.x;
@@ -75,6 +76,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_defect(DCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ d, const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     if(gate_closed(sc))
       return;
     const uint32_t i = blockIdx.x * NT + threadIdx.x;
@@ -89,6 +91,7 @@ namespace fb
     S* __restrict__ xc, const S* __restrict__ dinvc, const uint8_t* __restrict__ dmc, int* __restrict__ skipc,
     RedSlot slot, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
@@ -107,6 +110,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_coarse(const S* __restrict__ b, S* __restrict__ x, uint32_t n,
     const uint32_t* __restrict__ free_dofs, const double* __restrict__ inv, uint32_t m, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     if(gate_closed(sc))
       return;
     coarse_block<S, NT>(b, x, n, free_dofs, inv, m);
@@ -116,6 +120,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ x,
     const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     if(gate_closed(sc))
       return;
     const uint32_t i = blockIdx.x * NT + threadIdx.x;
@@ -129,6 +134,7 @@ namespace fb
     S* __restrict__ d, S* __restrict__ c, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
     int* __restrict__ skip, RedSlot slot, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
@@ -149,6 +155,7 @@ namespace fb
     const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip, RedSlot slot,
     Scalars* __restrict__ sc)
   {
+    pdl_wait();
     typedef typename ValueTraits<V>::acc Ac;
     __shared__ double sh[32];
     if(gate_closed(sc))
@@ -190,6 +197,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_post_final(const S* __restrict__ c, S* __restrict__ x, double* __restrict__ z,
     const double* __restrict__ r, const int* __restrict__ skip, uint32_t n, RedSlot slot, Scalars* __restrict__ sc)
   {
+    pdl_wait();
     typedef S Ac;
     __shared__ double sh[32];
     if(gate_closed(sc))
@@ -473,6 +481,7 @@ namespace fb
   template<typename V, typename S>
   __global__ void __launch_bounds__(TAIL_NT) k_tail(const __grid_constant__ TailParams<V, S> tp, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     typedef typename ValueTraits<V>::acc Ac;
     extern __shared__ __align__(16) unsigned char tail_smem[];
     __shared__ double sh[32];
@@ -767,6 +776,7 @@ namespace fb
   __global__ void __launch_bounds__(TAIL_NT) k_tail_prog(const __grid_constant__ TailParams<V, S> tp,
     const uint8_t* __restrict__ prog, int nprog, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char tail_smem[];
     __shared__ TailShared ts;
     __shared__ uint8_t psh[TAIL_PROG_CHUNK];   // the program, a chunk at a time
@@ -1025,6 +1035,7 @@ namespace fb
     const S* __restrict__ dinv, int* __restrict__ skip_top, double* __restrict__ hist, RedSlot slot,
     Scalars* __restrict__ sc, cudaGraphConditionalHandle cond)
   {
+    pdl_wait();
     __shared__ double sh[32];
     const uint32_t r0 = blockIdx.x * NT;
     const uint32_t i = r0 + threadIdx.x;
@@ -1069,6 +1080,7 @@ namespace fb
     S* __restrict__ x1, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, int* __restrict__ skip_top,
     uint32_t n, int scale_from_def, RedSlot slot, Scalars* __restrict__ sc)
   {
+    pdl_wait();
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
@@ -1095,6 +1107,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_pcg_q(DCsr<double> A, const double* __restrict__ p, double* __restrict__ q,
     const uint8_t* __restrict__ dm, RedSlot slot, Scalars* __restrict__ sc)
   {
+    pdl_wait();
     __shared__ double sh[32];
     if(gate_closed(sc))
       return;
@@ -1123,6 +1136,7 @@ namespace fb
     S* __restrict__ x1, const S* __restrict__ dinv, int* __restrict__ skip_top, double* __restrict__ hist, uint32_t n,
     RedSlot slot, Scalars* __restrict__ sc, cudaGraphConditionalHandle cond)
   {
+    pdl_wait();
     __shared__ double sh[32];
     if(gate_closed(sc))
     {
@@ -1174,6 +1188,7 @@ namespace fb
   __global__ void __launch_bounds__(NT) k_pcg_p(double* __restrict__ p, const double* __restrict__ z, uint32_t n,
     int first, const Scalars* __restrict__ sc)
   {
+    pdl_wait();
     if(gate_closed(sc))
       return;
     const uint32_t i = blockIdx.x * NT + threadIdx.x;
@@ -1536,6 +1551,28 @@ namespace fb
     cudaStream_t st;
     bool dry = false;          // count launches and bytes only
 
+    // Every kernel of a solve is launched with programmatic stream serialisation (when cfg.pdl):
+    // it may be scheduled while its predecessor's last blocks finish, and waits for the
+    // predecessor's results in griddepcontrol.wait (pdl_wait; the TMA pass first stages its
+    // first chunks of matrix data, which no kernel of a solve writes).
+    template<typename... KA, typename... A>
+    void go(void (*k)(KA...), dim3 g, dim3 b, size_t smem, A&&... a)
+    {
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = g;
+      lc.blockDim = b;
+      lc.dynamicSmemBytes = smem;
+      lc.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      lc.attrs = at;
+      lc.numAttrs = s->cfg.pdl ? 1 : 0;
+      const cudaError_t e = cudaLaunchKernelEx(&lc, k, std::forward<A>(a)...);
+      if(e != cudaSuccess && s->launch_err == cudaSuccess)
+        s->launch_err = e;
+    }
+
     // column index bytes per entry
     static uint32_t colbytes(const DevMat& m) { return m.doff ? 0u : (m.dcol ? 2u : 4u); }
 
@@ -1578,18 +1615,18 @@ namespace fb
         if(m.doff)
         {
           if(m.kw == 9)
-            k_tma_pass<VV, XS, Op, 9, true><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded,
+            go(k_tma_pass<VV, XS, Op, 9, true>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded,
               m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
           else
-            k_tma_pass<VV, XS, Op, 27, true><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded,
+            go(k_tma_pass<VV, XS, Op, 27, true>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded,
               m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
           return;
         }
       if(m.kw == 9)
-        k_tma_pass<VV, XS, Op, 9><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
+        go(k_tma_pass<VV, XS, Op, 9>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
                                                              xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
       else
-        k_tma_pass<VV, XS, Op, 0><<<grid, TMA_NT, smem, st>>>(view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
+        go(k_tma_pass<VV, XS, Op, 0>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
                                                              xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
     }
     uint64_t launches = 0;
@@ -1675,7 +1712,7 @@ namespace fb
         else if(use_tma(f.A))
           tma<V, S>(f.A, xa, OpSmooth<V, S>{(const S*)f.b, (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.skip_pre, s->sc});
         else
-          k_smooth<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+          go(k_smooth<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
             (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
         ++launches;
         bytes += csr_bytes(f.A, 3, 1) + f.n;
@@ -1693,7 +1730,7 @@ namespace fb
       else if(use_tma(f.A))
         tma<V, S>(f.A, xcur[size_t(l)], OpDefect<V, S>{(const S*)f.b, (S*)f.d, f.dm, s->sc});
       else
-        k_defect<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xcur[size_t(l)],
+        go(k_defect<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.b, (const S*)xcur[size_t(l)],
           (S*)f.d, f.dm, s->sc);
       ++launches;
       bytes += csr_bytes(f.A, 1, 1) + f.n;
@@ -1712,7 +1749,7 @@ namespace fb
         tma<V, S>(f.R, f.d, OpRestrict<V, S>{(S*)c.b, coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm,
           c.skip_pre, s->sc});
       else
-        k_restrict<V, S><<<blocks(c.n), NT, f.R.smem, st>>>(view<V>(f.R), (const S*)f.d, (S*)c.b,
+        go(k_restrict<V, S>, blocks(c.n), NT, f.R.smem, view<V>(f.R), (const S*)f.d, (S*)c.b,
           coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->sc);
       ++launches;
       bytes += csr_bytes(f.R, 0, coarsest ? 1 : 3) + c.n;
@@ -1723,7 +1760,7 @@ namespace fb
     {
       const int nl = s->nlev;
       DevLevel& c = L(nl - 1);
-      if(!dry) k_coarse<S><<<1, NT, 0, st>>>((const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
+      if(!dry) go(k_coarse<S>, 1, NT, 0, (const S*)c.b, (S*)c.x, c.n, s->free_dofs, s->cinv, s->nfree, s->sc);
       ++launches;
       bytes += double(s->nfree) * s->nfree * 8.0 + double(c.n) * 2 * sizeof(S);
       xcur[size_t(nl - 1)] = c.x;
@@ -1739,7 +1776,7 @@ namespace fb
       else if(use_tma(f.P))
         tma<V, S>(f.P, xcur[size_t(l + 1)], OpProlong<V, S>{(S*)xf, f.dm, s->sc});
       else
-        k_prolong<V, S><<<blocks(f.n), NT, f.P.smem, st>>>(view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm,
+        go(k_prolong<V, S>, blocks(f.n), NT, f.P.smem, view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm,
           s->sc);
       ++launches;
       bytes += csr_bytes(f.P, 1, 1) + f.n;
@@ -1757,7 +1794,7 @@ namespace fb
       else if(use_tma(f.A))
         tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
       else
-        k_post1<V, S><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+        go(k_post1<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
           (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
       ++launches;
       bytes += csr_bytes(f.A, 2, 2) + f.n;
@@ -1768,9 +1805,9 @@ namespace fb
         if(!dry)
         {
           if(top)
-            k_post_final<S, true><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot, s->sc);
+            go(k_post_final<S, true>, blocks(f.n), NT, 0, (const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot, s->sc);
           else
-            k_post_final<S, false><<<blocks(f.n), NT, 0, st>>>((const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n, s->slot, s->sc);
+            go(k_post_final<S, false>, blocks(f.n), NT, 0, (const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n, s->slot, s->sc);
         }
         ++launches;
         bytes += double(f.n) * sizeof(S) * 3;
@@ -1793,13 +1830,13 @@ namespace fb
               (const S*)f.dinv, f.dm, f.skip_post, s->sc});
         }
         else if(!last)
-          k_post2<V, S, false, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+          go(k_post2<V, S, false, false>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.d, (const S*)ca,
             (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
         else if(top)
-          k_post2<V, S, true, true><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+          go(k_post2<V, S, true, true>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.d, (const S*)ca,
             (S*)cb, (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
         else
-          k_post2<V, S, true, false><<<blocks(f.n), NT, f.A.smem, st>>>(view<V>(f.A), (const S*)f.d, (const S*)ca,
+          go(k_post2<V, S, true, false>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.d, (const S*)ca,
             (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
         ++launches;
         bytes += csr_bytes(f.A, 3, 1) + f.n;
@@ -1875,9 +1912,9 @@ namespace fb
           s->launch_err = e;
       }
       else if(s->cfg.cycle == FB_CYCLE_V)
-        k_tail<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->sc);
+        go(k_tail<V, S>, 1, TAIL_NT, smem, tp, s->sc);
       else
-        k_tail_prog<V, S><<<1, TAIL_NT, smem, st>>>(tp, s->tail_prog + s->seg_off[seg], int(s->seg_len[seg]), s->sc);
+        go(k_tail_prog<V, S>, 1, TAIL_NT, smem, tp, s->tail_prog + s->seg_off[seg], int(s->seg_len[seg]), s->sc);
       ++launches;
     }
 
@@ -1931,13 +1968,13 @@ namespace fb
       DevLevel& t = L(0);
       const bool f64 = s->cfg.precision == FB_PREC_F64;
       const DevMat& A = A64();
-      if(!dry) k_pcg_init<S><<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->rhs, s->x, s->r, t.dm,
+      if(!dry) go(k_pcg_init<S>, blocks(t.n), NT, A.smem, view<double>(A), s->rhs, s->x, s->r, t.dm,
         f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->hist, s->slot, s->sc, 0);
       ++launches;
       bytes += A.bytes + double(t.n) * 8 * 4 + t.n;
       if(!f64)
       {
-        if(!dry) k_mg_prep<S><<<blocks(t.n), NT, 0, st>>>(s->r, (S*)t.b, (S*)t.x, (const S*)t.dinv, t.dm, t.skip_pre, t.n, 1,
+        if(!dry) go(k_mg_prep<S>, blocks(t.n), NT, 0, s->r, (S*)t.b, (S*)t.x, (const S*)t.dinv, t.dm, t.skip_pre, t.n, 1,
           s->slot, s->sc);
         ++launches;
         bytes += double(t.n) * (8 + 3 * sizeof(S)) + t.n;
@@ -1949,20 +1986,20 @@ namespace fb
       DevLevel& t = L(0);
       const bool f64 = s->cfg.precision == FB_PREC_F64;
       const DevMat& A = A64();
-      if(!dry) k_pcg_p<<<blocks(t.n), NT, 0, st>>>(s->p, s->z, t.n, first ? 1 : 0, s->sc);
+      if(!dry) go(k_pcg_p, blocks(t.n), NT, 0, s->p, s->z, t.n, first ? 1 : 0, s->sc);
       if(dry)
         ;
       else if(use_tma_f64(A))
         tma<double, double>(A, s->p, OpPcgQ{s->p, s->q, t.dm, s->sc});
       else
-        k_pcg_q<<<blocks(t.n), NT, A.smem, st>>>(view<double>(A), s->p, s->q, t.dm, s->slot, s->sc);
+        go(k_pcg_q, blocks(t.n), NT, A.smem, view<double>(A), s->p, s->q, t.dm, s->slot, s->sc);
       if(dry)
         ;
       else if(f64)
-        k_pcg_x<S, false><<<blocks(t.n), NT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
+        go(k_pcg_x<S, false>, blocks(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
           (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
       else
-        k_pcg_x<S, true><<<blocks(t.n), NT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)t.b, (S*)t.x,
+        go(k_pcg_x<S, true>, blocks(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)t.b, (S*)t.x,
           (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
       launches += 3;
       bytes += double(t.n) * 8 * (first ? 2 : 3);                                    // P
@@ -2148,6 +2185,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->tma_rows = 1000;
   c->tma_window = 0;
   c->diagonal = 1;
+  c->pdl = 1;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)

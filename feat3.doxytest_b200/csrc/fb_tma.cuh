@@ -149,8 +149,6 @@ namespace fb
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
     __shared__ double sh[32];
-    if(op.closed())
-      return;
     constexpr int NS = tma_stages<V>();
     constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
@@ -217,13 +215,33 @@ namespace fb
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if(threadIdx.x == 0)
-      for(int s = 0; s < NS; ++s)
-      {
-        const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
-        if(c < nch)
-          issue(c, s);
-      }
+    // the first chunks' matrix copies do not depend on the preceding kernel (the matrix is never
+    // written during a solve): they go out before the wait for the predecessor; a gathered window
+    // of x does, so with windows they wait
+    auto issue_first = [&]()
+    {
+      if(threadIdx.x == 0)
+        for(int s = 0; s < NS; ++s)
+        {
+          const uint32_t c = blockIdx.x + uint32_t(s) * gridDim.x;
+          if(c < nch)
+            issue(c, s);
+        }
+    };
+    if(!xlo)
+      issue_first();
+    pdl_wait();
+    if(xlo)
+      issue_first();
+    if(op.closed())
+    {
+      // drain the first copies (bounded) before the block exits
+      if(threadIdx.x == 0)
+        for(int s = 0; s < NS; ++s)
+          if(blockIdx.x + uint32_t(s) * gridDim.x < nch)
+            mbar_wait(&bar[s], 0u);
+      return;
+    }
     double part = 0.0;
     bool failed = false;
     uint32_t it = 0;

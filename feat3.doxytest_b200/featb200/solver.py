@@ -232,6 +232,11 @@ class PCG:
         diagonals without column indices (1, default) or always as sliced ELL (0)."""
         self.cfg.diagonal = int(bool(on))
 
+    def set_pdl(self, on):
+        """Launch the solve's kernels with programmatic dependent launch (1, default) or in plain
+        stream order (0)."""
+        self.cfg.pdl = int(bool(on))
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -343,7 +348,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None, cycle="V", diagonal=None):
+                        cluster_rows=None, cycle="V", diagonal=None, pdl=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -371,6 +376,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_cluster_rows(cluster_rows)
     if diagonal is not None:
         s.set_diagonal(diagonal)
+    if pdl is not None:
+        s.set_pdl(pdl)
     h.init()
     s.init()
     return s

@@ -212,6 +212,9 @@ typedef struct
                            every row (structured grids numbered lexicographically), is stored as
                            its diagonals without column indices (row sums keep the stored order;
                            missing diagonals hold zeros); 0 = always sliced ELL */
+  int pdl;              /* 1 (default): the solve's kernels are launched with programmatic stream
+                           serialisation, so each one's launch and its matrix prologue overlap the
+                           end of its predecessor; 0 = plain stream order */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
