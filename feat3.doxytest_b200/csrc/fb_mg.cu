@@ -37,6 +37,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <vector>
 
@@ -1543,6 +1544,28 @@ namespace fb
 
   static unsigned int blocks(uint32_t n) { return std::max(1u, (n + NT - 1) / NT); }
 
+  // Blocks of `kern` (TMA_NT threads, `smem` dynamic shared memory) resident on one SM at once, at
+  // most 8 (cached: the occupancy query is made once per kernel and size)
+  static uint32_t resident_blocks(const void* kern, size_t smem)
+  {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, uint32_t> cache;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(kern, smem);
+    const auto it = cache.find(key);
+    if(it != cache.end())
+      return it->second;
+    int nb = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TMA_NT, smem) != cudaSuccess || nb < 1)
+    {
+      (void)cudaGetLastError();
+      nb = 1;
+    }
+    const uint32_t r = uint32_t(std::min(nb, 8));
+    cache.emplace(key, r);
+    return r;
+  }
+
   // ---------------------------------------------------------------- launch sequences
   template<typename V, typename S>
   struct Launcher
@@ -1605,29 +1628,30 @@ namespace fb
       const size_t smem = size_t(tma_stages<VV>()) * sb;
       const uint32_t padded = (m.rows + 31u) & ~31u;
       const uint32_t nch = (padded + TMA_NT - 1) / TMA_NT;
-      const uint32_t bps = std::max(1u, std::min(8u, uint32_t((227u * 1024u) / (smem + 1536u))));
-      const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * bps));
       // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
       const uint32_t nxa = (m.cols + 8u) & ~3u;
+      // a persistent grid of as many blocks as stay resident together (one wave)
+      auto launch = [&](auto kern, const uint32_t* xl, uint32_t xwa, int xs)
+      {
+        const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * resident_blocks((const void*)kern, smem)));
+        go(kern, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax, xl, xwa, nxa, xs, op,
+           s->slot, s->err);
+      };
       // diagonal storage of the 2D / 3D Q1 stencils (9 / 27 diagonals); the 2D Q1 stencil in ELL of
       // width 9 runs the fully unrolled row sum
       if constexpr(OnSystem<Op>::value)
         if(m.doff)
         {
           if(m.kw == 9)
-            go(k_tma_pass<VV, XS, Op, 9, true>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded,
-              m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
+            launch(k_tma_pass<VV, XS, Op, 9, true>, nullptr, 0u, 0);
           else
-            go(k_tma_pass<VV, XS, Op, 27, true>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded,
-              m.kmax, nullptr, 0u, nxa, 0, op, s->slot, s->err);
+            launch(k_tma_pass<VV, XS, Op, 27, true>, nullptr, 0u, 0);
           return;
         }
       if(m.kw == 9)
-        go(k_tma_pass<VV, XS, Op, 9>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
-                                                             xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
+        launch(k_tma_pass<VV, XS, Op, 9>, xw ? m.xlo : nullptr, xw, xstage);
       else
-        go(k_tma_pass<VV, XS, Op, 0>, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax,
-                                                             xw ? m.xlo : nullptr, xw, nxa, xstage, op, s->slot, s->err);
+        launch(k_tma_pass<VV, XS, Op, 0>, xw ? m.xlo : nullptr, xw, xstage);
     }
     uint64_t launches = 0;
     double bytes = 0;
