@@ -58,7 +58,8 @@ DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
 
 # DRAM bytes of one launch of the roofline kernel, from one ncu capture (summarised in profiles/):
 # (workload, ordering) -> bytes read + written
-MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.055808e6 + 4.434432e6}
+MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.055808e6 + 4.434432e6,
+                    ("poisson2d_l10_mixed", "native"): 85.146368e6 + 3.247616e6}
 
 
 def dist_env():
@@ -669,7 +670,9 @@ def main():
                                        "for native order, sliced ELL for rcm)",
                              "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": alg_k,
                              "bytes_definition": "CSR: nnz*(8+4) + (n+1)*4 + n*8 (gathered p) + n*8 (q written)",
-                             "stored_bytes_per_launch": by_k, "launch_ms": ms_k},
+                             "stored_bytes_per_launch": by_k, "launch_ms": ms_k,
+                             "traffic_frac": (MEASURED_TRAFFIC[(args.workload, args.ordering)] / (ms_k * 1e-3) / 1e9 / peak
+                                              if (args.workload, args.ordering) in MEASURED_TRAFFIC else None)},
                 "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(2 * 8 * n),
                         "d2h_bytes_per_step": int(8 * n)},
                 "gpu_launches": int(launches), "clocks": clk}
