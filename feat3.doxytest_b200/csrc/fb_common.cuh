@@ -129,6 +129,43 @@ namespace fb
     return threadIdx.x == 0;
   }
 
+  // Two grid sums at once (partials of b at partials[gridDim.x + block]); true in thread 0 of the
+  // last block, with ta, tb set.
+  template<int NT>
+  __device__ __forceinline__ bool grid_sum2_last(double a, double b, RedSlot slot, double* sh, double& ta, double& tb)
+  {
+    __shared__ bool am_last;
+    const double pa = block_sum<NT>(a, sh);
+    const double pb = block_sum<NT>(b, sh);
+    if(threadIdx.x == 0)
+    {
+      slot.partials[blockIdx.x] = pa;
+      slot.partials[gridDim.x + blockIdx.x] = pb;
+      __threadfence();
+      unsigned int prev = atomicAdd(slot.counter, 1u);
+      am_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if(!am_last)
+      return false;
+    __threadfence();
+    double sa = 0.0, sb = 0.0;
+    for(unsigned int i = threadIdx.x; i < gridDim.x; i += NT)
+    {
+      sa += ((volatile double*)slot.partials)[i];
+      sb += ((volatile double*)slot.partials)[gridDim.x + i];
+    }
+    const double t1 = block_sum<NT>(sa, sh);
+    const double t2 = block_sum<NT>(sb, sh);
+    if(threadIdx.x == 0)
+    {
+      *slot.counter = 0u;
+      ta = t1;
+      tb = t2;
+    }
+    return threadIdx.x == 0;
+  }
+
   constexpr double EPS64 = 2.220446049250313080847e-16;
   constexpr float EPS32 = 1.1920928955078125e-7f;
 } // namespace fb

@@ -229,6 +229,110 @@ namespace fb
     }
   }
 
+  // ------------------------------------------------------------------ adaptive coarse-grid correction
+  // MultiGrid::_apply_prol with MultiGridAdaptCGC::MinEnergy / MinDefect (multigrid.hpp:1880-1960):
+  // cor = F(P x_c); tmp = F(A cor); w = (d, cor) / (tmp, cor) or (d, tmp) / (tmp, tmp); x += w cor;
+  // d += -w tmp; the post-smoother then starts from that defect.  One thread per row.
+
+  // cor = F(P x_c)
+  template<typename V, typename S>
+  __global__ void __launch_bounds__(NT) k_cgc_prolong(DCsr<V> P, const S* __restrict__ xc, S* __restrict__ cor,
+    const uint8_t* __restrict__ dm, const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    pdl_wait();
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    if(i >= P.rows)
+      return;
+    const bool d = __ldg(dm + i) != 0;
+    const Ac sum = row_sum<V, S, true>(P, i, xc);
+    cor[i] = d ? S(0) : S(add(sum, Ac(0)));
+  }
+
+  // the two dot products of the step length for row i
+  template<int MODE>
+  __device__ __forceinline__ void cgc_dots(double d, double c, double t, double& a, double& b)
+  {
+    if(MODE == FB_CGC_MIN_ENERGY)
+    {
+      a = d * c;
+      b = t * c;
+    }
+    else
+    {
+      a = d * t;
+      b = t * t;
+    }
+  }
+
+  // tmp = F(A cor) and w = a / b into *omega
+  template<typename V, typename S, int MODE>
+  __global__ void __launch_bounds__(NT) k_cgc_apply(DCsr<V> A, const S* __restrict__ cor, const S* __restrict__ d,
+    S* __restrict__ tmp, const uint8_t* __restrict__ dm, double* __restrict__ omega, RedSlot slot,
+    const Scalars* __restrict__ sc)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    __shared__ double sh[32];
+    pdl_wait();
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    double a = 0.0, b = 0.0;
+    if(i < A.rows)
+    {
+      const bool dd = __ldg(dm + i) != 0;
+      const Ac sum = row_sum<V, S, true>(A, i, cor);
+      const S t = dd ? S(0) : S(add(sum, Ac(0)));
+      tmp[i] = t;
+      cgc_dots<MODE>(double(d[i]), double(cor[i]), double(t), a, b);
+    }
+    double ta, tb;
+    if(grid_sum2_last<NT>(a, b, slot, sh, ta, tb))
+      *omega = ta / tb;
+  }
+
+  // x += w cor, d += -w tmp
+  template<typename S>
+  __global__ void __launch_bounds__(NT) k_cgc_update(S* __restrict__ x, const S* __restrict__ cor, S* __restrict__ d,
+    const S* __restrict__ tmp, const double* __restrict__ omega, uint32_t n, const Scalars* __restrict__ sc)
+  {
+    pdl_wait();
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    if(i >= n)
+      return;
+    const S w = S(*omega);
+    x[i] = add(mul(w, cor[i]), x[i]);
+    d[i] = add(mul(S(-w), tmp[i]), d[i]);
+  }
+
+  // first post-smoothing step from the updated defect: c = F(D .* d), ||d|| -> skip flag
+  template<typename S>
+  __global__ void __launch_bounds__(NT) k_cgc_post1(const S* __restrict__ d, S* __restrict__ c,
+    const S* __restrict__ dinv, const uint8_t* __restrict__ dm, uint32_t n, int* __restrict__ skip, RedSlot slot,
+    const Scalars* __restrict__ sc)
+  {
+    __shared__ double sh[32];
+    pdl_wait();
+    if(gate_closed(sc))
+      return;
+    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    double sq = 0.0;
+    if(i < n)
+    {
+      const bool dd = __ldg(dm + i) != 0;
+      const S dv = d[i];
+      c[i] = dd ? S(0) : add(S(0), mul(__ldg(dinv + i), dv));
+      sq = double(dv) * double(dv);
+    }
+    double total;
+    if(grid_sum_last<NT>(sq, slot, sh, total))
+      *skip = skip_from_norm<S>(sqrt(total));
+  }
+
   // ------------------------------------------------------------------ TMA-staged pass epilogues
   // Row epilogues for k_tma_pass (fb_tma.cuh); each repeats the arithmetic of the matching row body
   // (fb_rows.cuh) on a row sum computed from the staged chunk, so both paths round identically.
@@ -422,7 +526,10 @@ namespace fb
   // (step 1 comes with the restriction), defect, restriction to the next coarser level, coarse
   // solve, prolongation from the next coarser level, post-smoothing (also the peak smoother) and
   // the PCG's final post-smoothing, which also forms z and r.z
-  enum CycOp : uint8_t { EV_PRE = 0, EV_DEF = 1, EV_RES = 2, EV_CRS = 3, EV_PRO = 4, EV_POST = 5, EV_POST_TOP = 6 };
+  // (with adaptive coarse-grid correction: the scaled prolongation, and post-smoothing that starts
+  // from the defect it updated)
+  enum CycOp : uint8_t { EV_PRE = 0, EV_DEF = 1, EV_RES = 2, EV_CRS = 3, EV_PRO = 4, EV_POST = 5, EV_POST_TOP = 6,
+                         EV_PROC = 7, EV_POSTC = 8, EV_POSTC_TOP = 9 };
   struct CycEv { uint8_t op; uint8_t lvl; };   // lvl: the level (restriction, prolongation: the finer one)
 
   constexpr int TAIL_NT = 512;
@@ -457,6 +564,7 @@ namespace fb
     const double* inv;
     uint32_t m;
     int npf;               // L2 prefetch ranges (16-byte aligned, multiples of 16 bytes)
+    int cgc;               // coarse-grid correction (FB_CGC_*), k_tail_prog only
     const void* pf_ptr[MAX_TAIL_PF];
     uint32_t pf_bytes[MAX_TAIL_PF];
   };
@@ -634,6 +742,7 @@ namespace fb
     int skip_pre[MAX_TAIL];
     int xsel[MAX_TAIL];    // 1 or 2: which x buffer holds level t's iterate
     int skip_post;
+    double omega;          // adaptive coarse-grid correction: the step length
   };
 
   // The events of k_tail_prog, one function each.  Each ends with its last pass written but not
@@ -723,28 +832,18 @@ namespace fb
       xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
   }
 
-  // post-smoothing (and the peak smoother) as a correction of x
+  // post-smoothing steps 2..steps (and the single step's update of x) after the first step wrote
+  // d, c and the skip flag
   template<typename V, typename S>
-  __device__ __forceinline__ void tail_post(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  __device__ __forceinline__ void tail_post_rest(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
   {
     typedef typename ValueTraits<V>::acc Ac;
     const TailLevel<V, S>& f = tp.lv[t];
     const int steps = tp.steps;
-    const S* fb = tail_vec(tp, sbase, t, 0);
     S* xf = tail_vec(tp, sbase, t, ts.xsel[t]);
     S* fd = tail_vec(tp, sbase, t, 3);
     S* ca = tail_vec(tp, sbase, t, 4);
     S* cb = tail_vec(tp, sbase, t, 5);
-    double sq = 0.0;
-    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
-      sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
-    const double tot = block_sum<TAIL_NT>(sq, ts.sh);
-    if(threadIdx.x == 0)
-    {
-      ts.skip_post = skip_from_norm<S>(sqrt(tot));
-      *(volatile int*)f.skip_post = ts.skip_post;
-    }
-    __syncthreads();
     const bool skipped = ts.skip_post != 0;
     if(steps == 1)
     {
@@ -768,6 +867,96 @@ namespace fb
       ca = cb;
       cb = tmp;
     }
+  }
+
+  // post-smoothing (and the peak smoother) as a correction of x
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_post(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    const S* fb = tail_vec(tp, sbase, t, 0);
+    S* xf = tail_vec(tp, sbase, t, ts.xsel[t]);
+    S* fd = tail_vec(tp, sbase, t, 3);
+    S* ca = tail_vec(tp, sbase, t, 4);
+    double sq = 0.0;
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+      sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
+    const double tot = block_sum<TAIL_NT>(sq, ts.sh);
+    if(threadIdx.x == 0)
+    {
+      ts.skip_post = skip_from_norm<S>(sqrt(tot));
+      *(volatile int*)f.skip_post = ts.skip_post;
+    }
+    __syncthreads();
+    tail_post_rest(tp, sbase, t, ts);
+  }
+
+  // adaptive coarse-grid correction (k_cgc_prolong, k_cgc_apply, k_cgc_update in one block)
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_proc(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    const TailLevel<V, S>& f = tp.lv[t];
+    S* xf = tail_vec(tp, sbase, t, ts.xsel[t]);
+    const S* xc = tail_vec(tp, sbase, t + 1, ts.xsel[t + 1]);
+    S* fd = tail_vec(tp, sbase, t, 3);
+    S* cor = tail_vec(tp, sbase, t, 4);
+    S* tmp = tail_vec(tp, sbase, t, 5);
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+    {
+      const Ac sum = row_sum<V, S, false>(f.P, i, xc);
+      cor[i] = __ldg(f.dm + i) ? S(0) : S(add(sum, Ac(0)));
+    }
+    __syncthreads();
+    double a = 0.0, b = 0.0;
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+    {
+      const Ac sum = row_sum<V, S, false>(f.A, i, cor);
+      const S tv = __ldg(f.dm + i) ? S(0) : S(add(sum, Ac(0)));
+      tmp[i] = tv;
+      double pa, pb;
+      if(tp.cgc == FB_CGC_MIN_ENERGY)
+        cgc_dots<FB_CGC_MIN_ENERGY>(double(fd[i]), double(cor[i]), double(tv), pa, pb);
+      else
+        cgc_dots<FB_CGC_MIN_DEFECT>(double(fd[i]), double(cor[i]), double(tv), pa, pb);
+      a += pa;
+      b += pb;
+    }
+    const double ta = block_sum<TAIL_NT>(a, ts.sh);
+    const double tb = block_sum<TAIL_NT>(b, ts.sh);
+    if(threadIdx.x == 0)
+      ts.omega = ta / tb;
+    __syncthreads();
+    const S w = S(ts.omega);
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+    {
+      xf[i] = add(mul(w, cor[i]), xf[i]);
+      fd[i] = add(mul(S(-w), tmp[i]), fd[i]);
+    }
+  }
+
+  // post-smoothing from the defect updated by tail_proc
+  template<typename V, typename S>
+  __device__ __forceinline__ void tail_postc(const TailParams<V, S>& tp, S* sbase, int t, TailShared& ts)
+  {
+    const TailLevel<V, S>& f = tp.lv[t];
+    const S* fd = tail_vec(tp, sbase, t, 3);
+    S* ca = tail_vec(tp, sbase, t, 4);
+    double sq = 0.0;
+    for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
+    {
+      const S dv = fd[i];
+      ca[i] = __ldg(f.dm + i) ? S(0) : add(S(0), mul(__ldg(f.dinv + i), dv));
+      sq += double(dv) * double(dv);
+    }
+    const double tot = block_sum<TAIL_NT>(sq, ts.sh);
+    if(threadIdx.x == 0)
+    {
+      ts.skip_post = skip_from_norm<S>(sqrt(tot));
+      *(volatile int*)f.skip_post = ts.skip_post;
+    }
+    __syncthreads();
+    tail_post_rest(tp, sbase, t, ts);
   }
 
   // The F- and W-cycle tail: the events of one run of the cycle on the tail levels, interpreted.
@@ -837,6 +1026,9 @@ namespace fb
         case EV_RES: tail_res(tp, sbase, t, ts); break;
         case EV_CRS: tail_crs(tp, sbase, ts); break;
         case EV_PRO: tail_pro(tp, sbase, t, ts); break;
+        case EV_PROC: tail_proc(tp, sbase, t, ts); break;
+        case EV_POSTC:
+        case EV_POSTC_TOP: tail_postc(tp, sbase, t, ts); break;
         default: tail_post(tp, sbase, t, ts); break;
       }
       __syncthreads();
@@ -1280,13 +1472,16 @@ namespace fb
 
   // _apply_prol(to, smooth_last) from level start - 1 up to `to`: prolongation, then
   // post-smoothing except on level `to` when smooth_last is false
-  static void ev_up(std::vector<CycEv>& ev, int to, bool smooth_last, int start, bool top)
+  static void ev_up(std::vector<CycEv>& ev, int to, bool smooth_last, int start, bool top, bool cgc)
   {
     for(int l = start - 1; l >= to; --l)
     {
-      ev.push_back(CycEv{EV_PRO, uint8_t(l)});
+      ev.push_back(CycEv{uint8_t(cgc ? EV_PROC : EV_PRO), uint8_t(l)});
       if(smooth_last || l > to)
-        ev.push_back(CycEv{uint8_t(top && l == 0 ? EV_POST_TOP : EV_POST), uint8_t(l)});
+      {
+        const bool t = top && l == 0;
+        ev.push_back(CycEv{uint8_t(cgc ? (t ? EV_POSTC_TOP : EV_POSTC) : (t ? EV_POST_TOP : EV_POST)), uint8_t(l)});
+      }
     }
   }
 
@@ -1299,7 +1494,7 @@ namespace fb
 
   // One multigrid cycle over nl levels as events: V = rest(0) + coarse + prol(0); F and W the peak
   // sequences of _apply_cycle_f / _apply_cycle_w (kernel/solver/multigrid.hpp:1356-1440)
-  static std::vector<CycEv> cycle_events(int cycle, int nl)
+  static std::vector<CycEv> cycle_events(int cycle, int nl, bool cgc)
   {
     std::vector<CycEv> ev;
     const int last = nl - 1;
@@ -1310,7 +1505,7 @@ namespace fb
     {
       for(int pk = last - 1; pk > 0; --pk)
       {
-        ev_up(ev, pk, false, last, false);
+        ev_up(ev, pk, false, last, false, cgc);
         ev_peak(ev, pk);
         ev_down(ev, pk, false, last);
         ev.push_back(crs);
@@ -1331,13 +1526,13 @@ namespace fb
         for(int i = last - 1; i > pk; --i)
           cnt[size_t(i)] = 0;
         ++cnt[size_t(pk)];
-        ev_up(ev, pk, false, last, false);
+        ev_up(ev, pk, false, last, false, cgc);
         ev_peak(ev, pk);
         ev_down(ev, pk, false, last);
         ev.push_back(crs);
       }
     }
-    ev_up(ev, 0, true, last, true);
+    ev_up(ev, 0, true, last, true, cgc);
     return ev;
   }
 } // namespace fb
@@ -1375,6 +1570,7 @@ struct fb_solver
   std::vector<fb::CycEv> events;            // one multigrid cycle
   uint8_t* tail_prog = nullptr;             // tail kernel programs: events op << 4 | tail level
   std::vector<uint32_t> seg_off, seg_len;   // program of each tail segment of `events`, in order
+  double* cgc_omega = nullptr;   // step length of the adaptive coarse-grid correction
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
   double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
@@ -1806,22 +2002,49 @@ namespace fb
       bytes += csr_bytes(f.P, 1, 1) + f.n;
     }
 
+    // adaptive coarse-grid correction of level l: cor = F(P x_{l+1}) in c, tmp = F(A cor) in c2,
+    // the step length w, x += w cor, d += -w tmp
+    void prolong_cgc(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      void* xf = xcur[size_t(l)];
+      if(!dry)
+      {
+        go(k_cgc_prolong<V, S>, blocks(f.n), NT, f.P.smem, view<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)f.c, f.dm,
+          s->sc);
+        if(s->cfg.adapt_cgc == FB_CGC_MIN_ENERGY)
+          go(k_cgc_apply<V, S, FB_CGC_MIN_ENERGY>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.c, (const S*)f.d,
+            (S*)f.c2, f.dm, s->cgc_omega, s->slot, s->sc);
+        else
+          go(k_cgc_apply<V, S, FB_CGC_MIN_DEFECT>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.c, (const S*)f.d,
+            (S*)f.c2, f.dm, s->cgc_omega, s->slot, s->sc);
+        go(k_cgc_update<S>, blocks(f.n), NT, 0, (S*)xf, (const S*)f.c, (S*)f.d, (const S*)f.c2,
+          (const double*)s->cgc_omega, f.n, s->sc);
+      }
+      launches += 3;
+      bytes += csr_bytes(f.P, 1, 1) + f.n + csr_bytes(f.A, 2, 1) + f.n + double(f.n) * sizeof(S) * 6;
+    }
+
     // a smoother applied as a correction: d = F(b - A x), c = Richardson-Jacobi(d) from zero, x += c
     // (post-smoothing, and the peak smoother); top: the last step also forms the PCG's z and r.z
-    void post_smooth(int l, bool top, std::vector<void*>& xcur)
+    // from_cgc: the defect d was updated by the adaptive coarse-grid correction (no recomputation)
+    void post_smooth(int l, bool top, std::vector<void*>& xcur, bool from_cgc = false)
     {
       DevLevel& f = L(l);
       const int steps = std::max(1, s->cfg.smooth_steps);
       void* xf = xcur[size_t(l)];
       if(dry)
         ;
+      else if(from_cgc)
+        go(k_cgc_post1<S>, blocks(f.n), NT, 0, (const S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.n, f.skip_post, s->slot,
+          s->sc);
       else if(use_tma(f.A))
         tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
       else
         go(k_post1<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
           (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
       ++launches;
-      bytes += csr_bytes(f.A, 2, 2) + f.n;
+      bytes += from_cgc ? double(f.n) * (3 * sizeof(S)) + f.n : csr_bytes(f.A, 2, 2) + f.n;
       void* ca = f.c;
       void* cb = f.c2;
       if(steps == 1)
@@ -1879,6 +2102,7 @@ namespace fb
       std::memset(&tp, 0, sizeof(tp));
       tp.count = nl - lt;
       tp.steps = steps;
+      tp.cgc = s->cfg.adapt_cgc;
       tp.free_dofs = s->free_dofs;
       tp.inv = s->cinv;
       tp.m = s->nfree;
@@ -1935,7 +2159,7 @@ namespace fb
         if(e != cudaSuccess && s->launch_err == cudaSuccess)
           s->launch_err = e;
       }
-      else if(s->cfg.cycle == FB_CYCLE_V)
+      else if(s->cfg.cycle == FB_CYCLE_V && s->cfg.adapt_cgc == FB_CGC_FIXED)
         go(k_tail<V, S>, 1, TAIL_NT, smem, tp, s->sc);
       else
         go(k_tail_prog<V, S>, 1, TAIL_NT, smem, tp, s->tail_prog + s->seg_off[seg], int(s->seg_len[seg]), s->sc);
@@ -1969,7 +2193,10 @@ namespace fb
           case EV_CRS: coarse(xcur); break;
           case EV_PRO: prolong(l, xcur); break;
           case EV_POST: post_smooth(l, false, xcur); break;
-          default: post_smooth(l, pcg_top, xcur); break;
+          case EV_POST_TOP: post_smooth(l, pcg_top, xcur); break;
+          case EV_PROC: prolong_cgc(l, xcur); break;
+          case EV_POSTC: post_smooth(l, false, xcur, true); break;
+          default: post_smooth(l, pcg_top, xcur, true); break;
         }
         ++i;
       }
@@ -2210,6 +2437,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->tma_window = 0;
   c->diagonal = 1;
   c->pdl = 1;
+  c->adapt_cgc = FB_CGC_FIXED;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -2310,7 +2538,8 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   else
     fb_solver_config_default(&cfg);
   if(cfg.precision < FB_PREC_F64 || cfg.precision > FB_PREC_F32_BF16 || cfg.smooth_steps < 1 || cfg.max_iter < 0 ||
-     cfg.cycle < FB_CYCLE_V || cfg.cycle > FB_CYCLE_W)
+     cfg.cycle < FB_CYCLE_V || cfg.cycle > FB_CYCLE_W || cfg.adapt_cgc < FB_CGC_FIXED ||
+     cfg.adapt_cgc > FB_CGC_MIN_DEFECT)
   {
     set_error("solver_create: bad configuration");
     return FB_ERR_ARG;
@@ -2423,13 +2652,14 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     FB_CUDA(cudaGetDevice(&dev));
     FB_CUDA(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev));
   }
-  FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * (max_blocks + 1)));
+  FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * 2 * (max_blocks + 1)));
+  FB_TRY(dalloc(s.get(), (void**)&s->cgc_omega, sizeof(double)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
   // the tail starts at the first level (below the top) with at most tail_rows rows, if it has a
   // coarser level below it
   s->tail_first = -1;
   s->ctail_first = -1;
-  if(cfg.cluster_rows > 0 && cfg.cycle == FB_CYCLE_V)
+  if(cfg.cluster_rows > 0 && cfg.cycle == FB_CYCLE_V && cfg.adapt_cgc == FB_CGC_FIXED)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.cluster_rows))
       {
@@ -2447,8 +2677,8 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       }
   // the cycle as events, and the tail kernel's program for each run of events on the tail levels
   // (identical runs share one program)
-  s->events = cycle_events(cfg.cycle, s->nlev);
-  if(s->tail_first >= 0 && cfg.cycle != FB_CYCLE_V)
+  s->events = cycle_events(cfg.cycle, s->nlev, cfg.adapt_cgc != FB_CGC_FIXED);
+  if(s->tail_first >= 0 && (cfg.cycle != FB_CYCLE_V || cfg.adapt_cgc != FB_CGC_FIXED))
   {
     const int lt = s->tail_first;
     std::vector<uint8_t> progs;

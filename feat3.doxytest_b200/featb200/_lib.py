@@ -33,7 +33,8 @@ class SolverConfig(C.Structure):
                 ("max_iter", C.c_int), ("min_iter", C.c_int), ("use_graph", C.c_int),
                 ("rows_per_block", C.c_int), ("tail_rows", C.c_int), ("tma_rows", C.c_int),
                 ("cluster_rows", C.c_int), ("cycle", C.c_int), ("tma_window", C.c_int),
-                ("diagonal", C.c_int), ("pdl", C.c_int)]
+                ("diagonal", C.c_int), ("pdl", C.c_int),
+                ("adapt_cgc", C.c_int)]
 
 
 class SolveInfo(C.Structure):

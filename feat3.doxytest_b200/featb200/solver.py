@@ -51,6 +51,13 @@ class MultiGridCycle(enum.Enum):
     W = 2
 
 
+class MultiGridAdaptCGC(enum.Enum):
+    """Coarse-grid correction (kernel/solver/multigrid.hpp:39-47)."""
+    Fixed = 0
+    MinEnergy = 1
+    MinDefect = 2
+
+
 class JacobiPrecond:
     def __init__(self, matrix, filter, omega=1.0):
         self.matrix, self.filter, self.omega = matrix, filter, float(omega)
@@ -168,6 +175,14 @@ class MultiGrid:
                                                           (lv["pre"].omega, lv["pre"].min_iter, lv["pre"].max_iter))):
                     raise _lib.FeatB200Error("F/W cycles need the peak smoother to be the pre/post smoother")
         self.hierarchy, self.cycle = hierarchy, cycle
+        self.adapt_cgc = MultiGridAdaptCGC.Fixed
+
+    def set_adapt_cgc(self, adapt_cgc):
+        """MultiGrid::set_adapt_cgc (multigrid.hpp:1091): scale each coarse-grid correction by the
+        step length minimising the energy or the defect."""
+        if not isinstance(adapt_cgc, MultiGridAdaptCGC):
+            raise _lib.FeatB200Error("adapt_cgc must be a MultiGridAdaptCGC")
+        self.adapt_cgc = adapt_cgc
 
 
 def new_multigrid(hierarchy, cycle=MultiGridCycle.V):
@@ -247,6 +262,7 @@ class PCG:
         self.cfg.omega = omega
         self.cfg.smooth_steps = steps
         self.cfg.cycle = {MultiGridCycle.V: 0, MultiGridCycle.F: 1, MultiGridCycle.W: 2}[self.precond.cycle]
+        self.cfg.adapt_cgc = self.precond.adapt_cgc.value
         if h._h is None:
             h.init()
         s = C.c_void_p()
@@ -348,7 +364,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None, cycle="V", diagonal=None, pdl=None):
+                        cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed"):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -360,6 +376,7 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         h.push_level(lv["matrix"], lv["filter"], lv["transfer"], sm, sm, sm)
     h.push_level(levels[-1]["matrix"], levels[-1]["filter"], new_coarse_inverse())
     mg = new_multigrid(h, MultiGridCycle[cycle])
+    mg.set_adapt_cgc(MultiGridAdaptCGC[adapt_cgc])
     s = new_pcg(levels[0]["matrix"], levels[0]["filter"], mg)
     s.set_tol_rel(tol_rel)
     s.set_max_iter(max_iter)

@@ -177,6 +177,10 @@ void fb_hierarchy_destroy(fb_hierarchy* h);
 #define FB_CYCLE_V 0
 #define FB_CYCLE_F 1
 #define FB_CYCLE_W 2
+/* coarse-grid correction of the multigrid (MultiGridAdaptCGC, kernel/solver/multigrid.hpp:39-50) */
+#define FB_CGC_FIXED 0        /* x += P x_c */
+#define FB_CGC_MIN_ENERGY 1   /* x += w P x_c, w = (d, c) / (A c, c) */
+#define FB_CGC_MIN_DEFECT 2   /* x += w P x_c, w = (d, A c) / (A c, A c) */
 
 typedef struct
 {
@@ -215,6 +219,10 @@ typedef struct
   int pdl;              /* 1 (default): the solve's kernels are launched with programmatic stream
                            serialisation, so each one's launch and its matrix prologue overlap the
                            end of its predecessor; 0 = plain stream order */
+  int adapt_cgc;        /* FB_CGC_FIXED (default), FB_CGC_MIN_ENERGY or FB_CGC_MIN_DEFECT: the
+                           coarse-grid correction is scaled by the step length that minimises the
+                           energy or the defect, and the post-smoother starts from the defect
+                           updated with A P x_c (MultiGrid::_apply_prol, multigrid.hpp:1880-1960) */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,

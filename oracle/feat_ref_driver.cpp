@@ -18,7 +18,8 @@
 //   feat_oracle fd M D DIR     (the reference's basic_solver-test problem, see run_fd)
 //   feat_oracle solve --dim D --level L --out DIR [--rhs sine|gauss] [--params FILE]
 //                     [--kappa FILE] [--omega W] [--steps S] [--tol T] [--iterates K]
-//                     [--vcycle] [--dump-levels] [--time REPS] [--no-dump]
+//                     [--vcycle] [--dump-levels] [--time REPS] [--no-dump] [--cycle v|f|w]
+//                     [--cgc fixed|energy|defect]
 //
 // The params files are written by the caller (tests/bench) so that the reference and the GPU
 // path consume exactly the same Gaussian and random-field coefficients.
@@ -335,6 +336,7 @@ namespace Oracle
   {
     int dim = 2;
     std::string cycle = "v";   // multigrid cycle: v, f or w
+    std::string cgc = "fixed"; // coarse-grid correction: fixed, energy or defect
     Index level = 7;
     Index level_min = 1;
     std::string out = ".";
@@ -515,6 +517,10 @@ namespace Oracle
     const Solver::MultiGridCycle cycle = opt.cycle == "f" ? Solver::MultiGridCycle::F :
                                          (opt.cycle == "w" ? Solver::MultiGridCycle::W : Solver::MultiGridCycle::V);
     auto multigrid = Solver::new_multigrid(hierarchy, cycle);
+    if(opt.cgc == "energy")
+      multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinEnergy);
+    else if(opt.cgc == "defect")
+      multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinDefect);
     auto solver = Solver::new_pcg(top.matrix, top.filter, multigrid);
     solver->set_tol_rel(DataType(opt.tol));
     solver->set_max_iter(100);
@@ -717,6 +723,7 @@ int main(int argc, char* argv[])
     else if(a == "--iterates") opt.iterates = Index(std::stoul(next()));
     else if(a == "--vcycle") opt.vcycle = true;
     else if(a == "--cycle") opt.cycle = next();
+    else if(a == "--cgc") opt.cgc = next();
     else if(a == "--dump-levels") opt.dump_levels = true;
     else if(a == "--no-dump") opt.dump = false;
     else if(a == "--time") opt.time_reps = std::stoi(next());

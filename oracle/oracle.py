@@ -181,11 +181,11 @@ def feat_available():
 
 def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, omega=0.7, steps=2,
                tol=1e-8, iterates=0, vcycle=False, dump_levels=False, time_reps=0, dump=True,
-               level_min=1, timeout=3600, cycle="v"):
+               level_min=1, timeout=3600, cycle="v", cgc="fixed"):
     """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary."""
     cmd = [FEAT_BIN, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
            "--out", out_dir, "--rhs", rhs, "--omega", repr(omega), "--steps", str(steps), "--tol",
-           repr(tol), "--iterates", str(iterates), "--time", str(time_reps), "--cycle", cycle]
+           repr(tol), "--iterates", str(iterates), "--time", str(time_reps), "--cycle", cycle, "--cgc", cgc]
     if params:
         cmd += ["--params", params]
     if kappa:

@@ -264,3 +264,37 @@ def test_fw_cycles_mixed_precision(featlib, cuda, cycle):
     s32, x32, st32 = _solve(fb, levels, b, cycle=cycle, precision="f32")
     assert st64 == st32 == fb.Status.success
     assert rel_err(x32, x64) <= 1e-7
+
+
+@pytest.mark.parametrize("cgc", ["energy", "defect"])
+@pytest.mark.parametrize("cycle", ["V", "F", "W"])
+def test_adaptive_cgc_matches_live_reference(featlib, cuda, cgc, cycle):
+    """MultiGridAdaptCGC::MinEnergy / MinDefect (multigrid.hpp:1880-1960) against the reference run with
+    the same setting.  The step length comes from two dot products whose summation order differs
+    from the reference's sequential loop, so the cycle agrees to rounding, not bitwise."""
+    fb = featlib
+    from helpers import to_lafem_levels as conv
+    mode = {"energy": "MinEnergy", "defect": "MinDefect"}[cgc]
+    with tempfile.TemporaryDirectory() as tmp:
+        summ, levels = _live_reference(tmp, 6, 2, cycle=cycle.lower(), cgc=cgc)
+        rhs = np.load(os.path.join(tmp, "rhs.npy"))
+        sol = np.load(os.path.join(tmp, "sol.npy"))
+        vc = np.load(os.path.join(tmp, "vcycle.npy"))
+    lv = conv(levels)
+    for tail, graph in ((None, True), (0, False), (1 << 20, True)):
+        s, x, st = _solve(fb, lv, rhs, cycle=cycle, adapt_cgc=mode, tail_rows=tail, use_graph=graph)
+        z = s.apply_precond(fb.DenseVector(rhs)).elements
+        assert rel_err(z, vc) <= 1e-12, (tail, rel_err(z, vc))
+        assert st == fb.Status.success and s.get_num_iter() == summ["iters"]
+        assert rel_err(x, sol) <= 1e-11, (tail, rel_err(x, sol))
+
+
+@pytest.mark.parametrize("cgc", ["MinEnergy", "MinDefect"])
+def test_adaptive_cgc_mixed_precision(featlib, cuda, oracle_lib, cgc):
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(9, 2, rhs="gauss", gauss=AS.gauss_params(4, 2))
+    _, x64, st64 = _solve(fb, levels, b, adapt_cgc=cgc)
+    _, x32, st32 = _solve(fb, levels, b, adapt_cgc=cgc, precision="f32")
+    assert st64 == st32 == fb.Status.success
+    assert rel_err(x32, x64) <= 1e-7
