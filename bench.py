@@ -627,6 +627,11 @@ def main():
     alg_d = csr_alg_bytes(nnz0, n0, n0, sv, 4, sx, row_vectors=1)
     achieved = alg_k / (ms_k * 1e-3) / 1e9
     spmv_gbs = {"pcg_spmv_f64": achieved, "mg_defect_" + precision: alg_d / (ms_d * 1e-3) / 1e9}
+    # where a preconditioner application goes: one whole cycle, and its coarse-level tail kernel
+    breakdown = {"mg_cycle_us": solver.time_kernel("mg_cycle", reps=20, flush_l2=False)[0] * 1e3}
+    if args.tail_rows != 0 and args.cluster_rows in (None, 0):
+        breakdown["mg_tail_us"] = solver.time_kernel("mg_tail", reps=20, flush_l2=False)[0] * 1e3
+        breakdown["mg_tail_us_cold_l2"] = solver.time_kernel("mg_tail", reps=20, flush_l2=True)[0] * 1e3
 
     # end to end through the C ABI with host buffers (copies inside the timed region)
     pin_rhs = torch.tensor(b).pin_memory()
@@ -661,7 +666,7 @@ def main():
                            "levels": int(info_lv.shape[0]), "ordering": args.ordering, "precision": precision,
                            "cycle": args.cycle, "parallelism": f"replicas x{world}", "l2": L2Flush.DESC,
                            "iterations": int(np.median(iters))},
-                "spmv_gbs": spmv_gbs, "rel_residual": rel_res,
+                "spmv_gbs": spmv_gbs, "rel_residual": rel_res, "breakdown": breakdown,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get((args.workload, args.ordering)),
                              "traffic_source": "profiles/k_tma_pass_OpPcgQ_l10_f64.md (ncu dram__bytes_read.sum + "

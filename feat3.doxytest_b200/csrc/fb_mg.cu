@@ -532,7 +532,7 @@ namespace fb
                          EV_PROC = 7, EV_POSTC = 8, EV_POSTC_TOP = 9 };
   struct CycEv { uint8_t op; uint8_t lvl; };   // lvl: the level (restriction, prolongation: the finer one)
 
-  constexpr int TAIL_NT = 512;
+  constexpr int TAIL_NT = 320;
   constexpr int MAX_TAIL = 12;
   constexpr int MAX_TAIL_PF = 96;
   constexpr uint32_t TAIL_PF_CHUNK = 32768;
@@ -591,6 +591,15 @@ namespace fb
   __global__ void __launch_bounds__(TAIL_NT) k_tail(const __grid_constant__ TailParams<V, S> tp, const Scalars* __restrict__ sc)
   {
     pdl_wait();
+    // the parameters in shared memory: the passes index the levels with a run-time level number,
+    // which in the parameter space would be constant-cache loads with a dynamic offset
+    __shared__ __align__(16) TailParams<V, S> tps;
+    {
+      typedef TailParams<V, S> TP;
+      const uint32_t nw = uint32_t(offsetof(TP, pf_ptr) / 4);
+      for(uint32_t k = threadIdx.x; k < nw; k += TAIL_NT)
+        reinterpret_cast<uint32_t*>(&tps)[k] = reinterpret_cast<const uint32_t*>(&tp)[k];
+    }
     typedef typename ValueTraits<V>::acc Ac;
     extern __shared__ __align__(16) unsigned char tail_smem[];
     __shared__ double sh[32];
@@ -615,30 +624,31 @@ namespace fb
           }
       }
     }
-    const int cnt = tp.count;
-    const int steps = tp.steps;
+    __syncthreads();
+    const int cnt = tps.count;
+    const int steps = tps.steps;
     // the top level's input: b and sol1 = F(D .* b) written by the restriction above
-    if(tp.lv[0].in_smem)
+    if(tps.lv[0].in_smem)
     {
-      S* b0 = tail_vec(tp, sbase, 0, 0);
-      S* x0 = tail_vec(tp, sbase, 0, 1);
-      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      S* b0 = tail_vec(tps, sbase, 0, 0);
+      S* x0 = tail_vec(tps, sbase, 0, 1);
+      for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
       {
-        b0[i] = tp.lv[0].b[i];
-        x0[i] = tp.lv[0].x[i];
+        b0[i] = tps.lv[0].b[i];
+        x0[i] = tps.lv[0].x[i];
       }
     }
     if(threadIdx.x == 0)
-      skip_pre_sh[0] = *(volatile int*)tp.lv[0].skip_pre;
+      skip_pre_sh[0] = *(volatile int*)tps.lv[0].skip_pre;
     __syncthreads();
     int xsel[MAX_TAIL];   // 1 or 2: which x buffer holds level t's iterate after pre-smoothing
     for(int t = 0; t + 1 < cnt; ++t)
     {
-      const TailLevel<V, S>& f = tp.lv[t];
-      const TailLevel<V, S>& c = tp.lv[t + 1];
-      const S* fb = tail_vec(tp, sbase, t, 0);
-      S* xa = tail_vec(tp, sbase, t, 1);
-      S* xb = tail_vec(tp, sbase, t, 2);
+      const TailLevel<V, S>& f = tps.lv[t];
+      const TailLevel<V, S>& c = tps.lv[t + 1];
+      const S* fb = tail_vec(tps, sbase, t, 0);
+      S* xa = tail_vec(tps, sbase, t, 1);
+      S* xb = tail_vec(tps, sbase, t, 2);
       int sel = 1;
       const bool skipped = skip_pre_sh[t] != 0;
       for(int k = 1; k < steps; ++k)
@@ -652,13 +662,13 @@ namespace fb
         sel = 3 - sel;
       }
       xsel[t] = sel;
-      S* fd = tail_vec(tp, sbase, t, 3);
+      S* fd = tail_vec(tps, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         fd[i] = defect_row<V, S, false>(f.A, fb, xa, f.dm, i);
       __syncthreads();
       const bool coarsest = (t + 2 == cnt);
-      S* cbv = tail_vec(tp, sbase, t + 1, 0);
-      S* cxv = coarsest ? (S*)nullptr : tail_vec(tp, sbase, t + 1, 1);
+      S* cbv = tail_vec(tps, sbase, t + 1, 0);
+      S* cxv = coarsest ? (S*)nullptr : tail_vec(tps, sbase, t + 1, 1);
       double sq = 0.0;
       for(uint32_t j = threadIdx.x; j < c.n; j += TAIL_NT)
         sq += restrict_row<V, S, false>(f.R, fd, cbv, cxv, c.dinv, c.dm, j);
@@ -672,24 +682,24 @@ namespace fb
       __syncthreads();
     }
     {
-      const TailLevel<V, S>& c = tp.lv[cnt - 1];
-      coarse_block<S, TAIL_NT>(tail_vec(tp, sbase, cnt - 1, 0), tail_vec(tp, sbase, cnt - 1, 1), c.n, tp.free_dofs,
-        tp.inv, tp.m);
+      const TailLevel<V, S>& c = tps.lv[cnt - 1];
+      coarse_block<S, TAIL_NT>(tail_vec(tps, sbase, cnt - 1, 0), tail_vec(tps, sbase, cnt - 1, 1), c.n, tps.free_dofs,
+        tps.inv, tps.m);
       xsel[cnt - 1] = 1;
       __syncthreads();
     }
     for(int t = cnt - 2; t >= 0; --t)
     {
-      const TailLevel<V, S>& f = tp.lv[t];
-      S* xf = tail_vec(tp, sbase, t, xsel[t]);
-      const S* xc = tail_vec(tp, sbase, t + 1, xsel[t + 1]);
-      const S* fb = tail_vec(tp, sbase, t, 0);
-      S* fd = tail_vec(tp, sbase, t, 3);
+      const TailLevel<V, S>& f = tps.lv[t];
+      S* xf = tail_vec(tps, sbase, t, xsel[t]);
+      const S* xc = tail_vec(tps, sbase, t + 1, xsel[t + 1]);
+      const S* fb = tail_vec(tps, sbase, t, 0);
+      S* fd = tail_vec(tps, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
       __syncthreads();
-      S* ca = tail_vec(tp, sbase, t, 4);
-      S* cb = tail_vec(tp, sbase, t, 5);
+      S* ca = tail_vec(tps, sbase, t, 4);
+      S* cb = tail_vec(tps, sbase, t, 5);
       double sq = 0.0;
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
@@ -725,11 +735,11 @@ namespace fb
       }
     }
     // the top level's solution goes to the global buffer the prolongation above reads
-    if(tp.lv[0].in_smem)
+    if(tps.lv[0].in_smem)
     {
-      const S* xs = tail_vec(tp, sbase, 0, xsel[0]);
-      S* xg = xsel[0] == 1 ? tp.lv[0].x : tp.lv[0].x2;
-      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      const S* xs = tail_vec(tps, sbase, 0, xsel[0]);
+      S* xg = xsel[0] == 1 ? tps.lv[0].x : tps.lv[0].x2;
+      for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
         xg[i] = xs[i];
     }
   }
@@ -967,6 +977,15 @@ namespace fb
     const uint8_t* __restrict__ prog, int nprog, const Scalars* __restrict__ sc)
   {
     pdl_wait();
+    // the parameters in shared memory: the passes index the levels with a run-time level number,
+    // which in the parameter space would be constant-cache loads with a dynamic offset
+    __shared__ __align__(16) TailParams<V, S> tps;
+    {
+      typedef TailParams<V, S> TP;
+      const uint32_t nw = uint32_t(offsetof(TP, pf_ptr) / 4);
+      for(uint32_t k = threadIdx.x; k < nw; k += TAIL_NT)
+        reinterpret_cast<uint32_t*>(&tps)[k] = reinterpret_cast<const uint32_t*>(&tp)[k];
+    }
     extern __shared__ __align__(16) unsigned char tail_smem[];
     __shared__ TailShared ts;
     __shared__ uint8_t psh[TAIL_PROG_CHUNK];   // the program, a chunk at a time
@@ -991,20 +1010,21 @@ namespace fb
           }
       }
     }
+    __syncthreads();
     // the top level's input: b and sol1 = F(D .* b) written by the restriction above
-    if(tp.lv[0].in_smem)
+    if(tps.lv[0].in_smem)
     {
-      S* b0 = tail_vec(tp, sbase, 0, 0);
-      S* x0 = tail_vec(tp, sbase, 0, 1);
-      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      S* b0 = tail_vec(tps, sbase, 0, 0);
+      S* x0 = tail_vec(tps, sbase, 0, 1);
+      for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
       {
-        b0[i] = tp.lv[0].b[i];
-        x0[i] = tp.lv[0].x[i];
+        b0[i] = tps.lv[0].b[i];
+        x0[i] = tps.lv[0].x[i];
       }
     }
     if(threadIdx.x == 0)
     {
-      ts.skip_pre[0] = *(volatile int*)tp.lv[0].skip_pre;
+      ts.skip_pre[0] = *(volatile int*)tps.lv[0].skip_pre;
       ts.xsel[0] = 1;
     }
     __syncthreads();
@@ -1021,24 +1041,24 @@ namespace fb
       const int t = int(ev & 15u);
       switch(op)
       {
-        case EV_PRE: tail_pre(tp, sbase, t, ts); break;
-        case EV_DEF: tail_def(tp, sbase, t, ts); break;
-        case EV_RES: tail_res(tp, sbase, t, ts); break;
-        case EV_CRS: tail_crs(tp, sbase, ts); break;
-        case EV_PRO: tail_pro(tp, sbase, t, ts); break;
-        case EV_PROC: tail_proc(tp, sbase, t, ts); break;
+        case EV_PRE: tail_pre(tps, sbase, t, ts); break;
+        case EV_DEF: tail_def(tps, sbase, t, ts); break;
+        case EV_RES: tail_res(tps, sbase, t, ts); break;
+        case EV_CRS: tail_crs(tps, sbase, ts); break;
+        case EV_PRO: tail_pro(tps, sbase, t, ts); break;
+        case EV_PROC: tail_proc(tps, sbase, t, ts); break;
         case EV_POSTC:
-        case EV_POSTC_TOP: tail_postc(tp, sbase, t, ts); break;
-        default: tail_post(tp, sbase, t, ts); break;
+        case EV_POSTC_TOP: tail_postc(tps, sbase, t, ts); break;
+        default: tail_post(tps, sbase, t, ts); break;
       }
       __syncthreads();
     }
     // the top level's solution goes to the global buffer the prolongation above reads
-    if(tp.lv[0].in_smem)
+    if(tps.lv[0].in_smem)
     {
-      const S* xs = tail_vec(tp, sbase, 0, ts.xsel[0]);
-      S* xg = ts.xsel[0] == 1 ? tp.lv[0].x : tp.lv[0].x2;
-      for(uint32_t i = threadIdx.x; i < tp.lv[0].n; i += TAIL_NT)
+      const S* xs = tail_vec(tps, sbase, 0, ts.xsel[0]);
+      S* xg = ts.xsel[0] == 1 ? tps.lv[0].x : tps.lv[0].x2;
+      for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
         xg[i] = xs[i];
     }
   }
@@ -2940,7 +2960,14 @@ namespace fb
     Launcher<V, S> l{s, st, false};
     const DevLevel& t = s->lv[0];
     const DevMat& A64 = s->cfg.precision == FB_PREC_F64 ? t.A : t.A64;
-    if(which == FB_KERNEL_PCG_SPMV)
+    if(which == FB_KERNEL_MG_TAIL)
+    {
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      l.tail(s->ctail_first >= 0 ? s->ctail_first : s->tail_first, 0, 0, 0, xcur);
+    }
+    else if(which == FB_KERNEL_MG_CYCLE)
+      l.vcycle(false);
+    else if(which == FB_KERNEL_PCG_SPMV)
     {
       if(l.use_tma_f64(A64))
         l.template tma<double, double>(A64, s->p, OpPcgQ{s->p, s->q, t.dm, s->sc});
@@ -2960,7 +2987,8 @@ extern "C" {
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
   double* bytes_per_launch)
 {
-  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || (which != FB_KERNEL_PCG_SPMV && which != FB_KERNEL_MG_DEFECT))
+  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_CYCLE ||
+     (which == FB_KERNEL_MG_TAIL && s->tail_first < 0 && s->ctail_first < 0))
   {
     set_error("solver_time_kernel: bad arguments");
     return FB_ERR_ARG;
@@ -2981,8 +3009,10 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   const double sv = double(vsize_of(s->cfg.precision));
   if(which == FB_KERNEL_PCG_SPMV)
     *bytes_per_launch = A64.bytes + double(t.n) * 8.0 * 2.0 + double(t.n);
-  else
+  else if(which == FB_KERNEL_MG_DEFECT)
     *bytes_per_launch = t.A.bytes + double(t.n) * sv * 3.0 + double(t.n);
+  else
+    *bytes_per_launch = 0.0;   // several passes: no single figure
   k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_PROGRESS);
   FB_LAUNCHED(1);
   double total = 0.0;

@@ -48,6 +48,34 @@ namespace fb
     typedef typename ValueTraits<V>::acc A;
     constexpr uint32_t U = 9;
     const uint32_t sl = row >> 5;
+    if(M.kw == U && (M.dcol || M.doff))
+    {
+      // 2D Q1 stencil, row-relative or diagonal columns: fully unrolled, no width tests
+      const uint32_t base = sl * 32u * U + (row & 31u);
+      A v[U], xv[U];
+      uint32_t c[U];
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+      {
+        const uint32_t e = base + u * 32u;
+        v[u] = to_acc(ldg_v(M.val + e));
+        if(M.doff)
+        {
+          const uint32_t cc = uint32_t(int32_t(row) + __ldg(M.doff + u));
+          c[u] = cc < M.rows ? cc : row;
+        }
+        else
+          c[u] = uint32_t(int32_t(row) + int32_t(__ldg(M.dcol + e)));
+      }
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        xv[u] = NC ? A(__ldg(x + c[u])) : A(x[c[u]]);
+      A sum = A(0);
+      #pragma unroll
+      for(uint32_t u = 0; u < U; ++u)
+        sum = add(sum, mul(v[u], xv[u]));
+      return sum;
+    }
     uint32_t b0, K;
     if(M.kw)
     {

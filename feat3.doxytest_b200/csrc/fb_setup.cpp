@@ -223,8 +223,10 @@ namespace fb
       }
       nnz += M.rp[r + 1] - M.rp[r];
     }
+    // small matrices (the coarse levels) take the diagonal form whatever their padding: the bytes
+    // do not matter there, the shorter row sums do
     const uint32_t K = uint32_t(offs.size());
-    if(!K || uint64_t(K) * 32u * ns > nnz + nnz / 8)
+    if(!K || (uint64_t(K) * 32u * ns > nnz + nnz / 8 && n > DIAG_SMALL_ROWS))
       return false;
     std::sort(offs.begin(), offs.end());
     H.rows = n;

@@ -57,8 +57,10 @@ namespace fb
   // Diagonal storage (allow_diag, square matrices): when every stored entry lies on one of at most
   // DIAG_MAX diagonals and every row's columns are strictly increasing, the matrix is stored as
   // plain ELL whose entry k of every row is the diagonal doff[k] (column = row + doff[k]), without
-  // column indices: a row's entries keep their stored order, the diagonals it lacks hold value 0.
+  // column indices: a row's entries keep their stored order, the diagonals it lacks hold value 0
+  // (at most 12.5% padding, except for matrices of at most DIAG_SMALL_ROWS rows).
   constexpr uint32_t DIAG_MAX = 27;
+  constexpr uint32_t DIAG_SMALL_ROWS = 4096;   // up to this many rows: no padding limit
   struct HostSell
   {
     uint32_t rows = 0, cols = 0, kw = 0;

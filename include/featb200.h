@@ -264,6 +264,8 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
 /* Kernels that fb_solver_time_kernel can time in isolation. */
 #define FB_KERNEL_PCG_SPMV 0   /* q = F(A p) with q.p, finest level, FP64 (the PCG matrix product) */
 #define FB_KERNEL_MG_DEFECT 1  /* d = F(b - A x), finest level, in the V-cycle's precision */
+#define FB_KERNEL_MG_TAIL 2    /* the coarse-level tail kernel (one launch; needs a tail level) */
+#define FB_KERNEL_MG_CYCLE 3   /* one whole multigrid cycle from the finest level (all its launches) */
 
 /* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
  * on that stream; with flush_l2 != 0 a 256 MiB buffer is overwritten and another 256 MiB buffer read
