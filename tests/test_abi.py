@@ -51,6 +51,10 @@ def test_config_defaults_match_reference(featlib):
     assert cfg.tol_rel == 1e-8 and cfg.max_iter == 100 and cfg.min_iter == 0
     assert cfg.tol_abs == 1.0 / eps ** 2
     assert cfg.omega == 0.7 and cfg.smooth_steps == 2 and cfg.precision == 0
+    # the multigrid's own defaults (multigrid.hpp:1068-1075): V cycle, fixed coarse-grid correction;
+    # device choices on by default: diagonal storage where it applies, programmatic dependent launch
+    assert cfg.cycle == 0 and cfg.adapt_cgc == 0
+    assert cfg.diagonal == 1 and cfg.pdl == 1 and cfg.tail_rows == 300 and cfg.tma_rows == 1000
 
 
 def _csr(rp, ci, val, shape):
@@ -108,3 +112,27 @@ def test_python_mirror_rejects_unsupported_configurations(featlib):
         h.smoother_params()
     with pytest.raises(fb.FeatB200Error):
         fb.new_multigrid(h, "X")
+    with pytest.raises(fb.FeatB200Error):
+        fb.new_multigrid(h).set_adapt_cgc("MinEnergy")
+
+
+def test_solver_create_rejects_bad_cycle_and_correction(featlib):
+    """fb_solver_create validates the configuration before touching a device."""
+    from featb200 import _lib
+    from helpers import load_golden, to_lafem_levels
+    fb = featlib
+    L = featlib.lib()
+    lv = to_lafem_levels(load_golden("c1_L4")["levels"])
+    h = fb.MultiGridHierarchy(len(lv))
+    for d in lv[:-1]:
+        sm = fb.new_richardson(d["matrix"], d["filter"], 1.0, fb.new_jacobi_precond(d["matrix"], d["filter"], 0.7))
+        h.push_level(d["matrix"], d["filter"], d["transfer"], sm, sm, sm)
+    h.push_level(lv[-1]["matrix"], lv[-1]["filter"], fb.new_coarse_inverse())
+    h.init()   # host-side upload of the levels: no device needed
+    for field, bad in (("cycle", 3), ("adapt_cgc", 3), ("adapt_cgc", -1), ("precision", 7), ("smooth_steps", 0)):
+        cfg = _lib.SolverConfig()
+        L.fb_solver_config_default(C.byref(cfg))
+        setattr(cfg, field, bad)
+        s = C.c_void_p()
+        assert L.fb_solver_create(C.byref(s), h._h, C.byref(cfg)) == 1, field
+        assert b"bad configuration" in L.fb_last_error()
