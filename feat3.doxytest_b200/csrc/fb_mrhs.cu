@@ -62,6 +62,31 @@ namespace mr
 
   __device__ __forceinline__ bool closed(const MScal* sc) { return sc->progress <= 0; }
 
+  // a lane's R consecutive vector entries, in one load where the width allows (8- or 16-byte aligned:
+  // the row stride is 32 R entries and the lane offset R entries)
+  template<typename S, int R>
+  __device__ __forceinline__ void ldg_row(const S* p, S (&v)[R])
+  {
+    if(R == 2 && sizeof(S) == 4)
+    {
+      const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+      v[0] = S(t.x);
+      v[R - 1] = S(t.y);
+    }
+    else if(R == 2 && sizeof(S) == 8)
+    {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+      v[0] = S(t.x);
+      v[R - 1] = S(t.y);
+    }
+    else
+    {
+      #pragma unroll
+      for(int r = 0; r < R; ++r)
+        v[r] = __ldg(p + r);
+    }
+  }
+
   template<typename S> __device__ __forceinline__ double epsq();
   template<> __device__ __forceinline__ double epsq<double>() { return EPS64 * EPS64; }
   template<> __device__ __forceinline__ double epsq<float>() { return double(EPS32) * double(EPS32); }
@@ -91,15 +116,18 @@ namespace mr
         v = ldg_m(M.val + base + lane);
         c = __ldg(M.col + base + lane);
       }
-      #pragma unroll 4
+      // 9 entries per step (the 2D and 3D Q1 rows are 9 and 27 long): their gathers go out together
+      #pragma unroll 9
       for(uint32_t k = 0; k < cnt; ++k)
       {
         const A vk = A(shfl_v(v, int(k)));
         const uint32_t ck = __shfl_sync(0xffffffffu, c, int(k));
         const S* xr = x + size_t(ck) * (32 * R) + lane * R;
+        S xv[R];
+        ldg_row<S, R>(xr, xv);
         #pragma unroll
         for(int r = 0; r < R; ++r)
-          sum[r] = add(sum[r], mul(vk, A(__ldg(xr + r))));
+          sum[r] = add(sum[r], mul(vk, A(xv[r])));
       }
     }
   }
