@@ -1847,27 +1847,28 @@ namespace fb
       // vectors hold cols + 8 entries (dalloc pads 64 bytes): windows end there at the latest
       const uint32_t nxa = (m.cols + 8u) & ~3u;
       // a persistent grid of as many blocks as stay resident together (one wave)
-      auto launch = [&](auto kern, const uint32_t* xl, uint32_t xwa, int xs)
+      auto launch = [&](auto kern, const uint32_t* xl, uint32_t xwa, int xs, size_t sm)
       {
-        const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * resident_blocks((const void*)kern, smem)));
-        go(kern, grid, TMA_NT, smem, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax, xl, xwa, nxa, xs, op,
+        const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * resident_blocks((const void*)kern, sm)));
+        go(kern, grid, TMA_NT, sm, view<VV>(m), static_cast<const XS*>(x), padded, m.kmax, xl, xwa, nxa, xs, op,
            s->slot, s->err);
       };
+      const size_t smem_dg = size_t(tma_stages_dg<VV, true>()) * sb;
       // diagonal storage of the 2D / 3D Q1 stencils (9 / 27 diagonals); the 2D Q1 stencil in ELL of
       // width 9 runs the fully unrolled row sum
       if constexpr(OnSystem<Op>::value)
         if(m.doff)
         {
           if(m.kw == 9)
-            launch(k_tma_pass<VV, XS, Op, 9, true>, nullptr, 0u, 0);
+            launch(k_tma_pass<VV, XS, Op, 9, true>, nullptr, 0u, 0, smem_dg);
           else
-            launch(k_tma_pass<VV, XS, Op, 27, true>, nullptr, 0u, 0);
+            launch(k_tma_pass<VV, XS, Op, 27, true>, nullptr, 0u, 0, smem_dg);
           return;
         }
       if(m.kw == 9)
-        launch(k_tma_pass<VV, XS, Op, 9>, xw ? m.xlo : nullptr, xw, xstage);
+        launch(k_tma_pass<VV, XS, Op, 9>, xw ? m.xlo : nullptr, xw, xstage, smem);
       else
-        launch(k_tma_pass<VV, XS, Op, 0>, xw ? m.xlo : nullptr, xw, xstage);
+        launch(k_tma_pass<VV, XS, Op, 0>, xw ? m.xlo : nullptr, xw, xstage, smem);
     }
     uint64_t launches = 0;
     double bytes = 0;

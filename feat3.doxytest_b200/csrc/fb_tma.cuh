@@ -19,6 +19,10 @@ namespace fb
   // more blocks (rows in flight) per SM; measured faster for FP64 on B200, three for FP32/BF16.
   template<typename V>
   __host__ __device__ constexpr int tma_stages() { return sizeof(V) == 8 ? 2 : 3; }
+  // Diagonal storage stages values only, and its gathers go out before the wait: two stages leave
+  // room for more resident blocks (measured faster for FP32 too).
+  template<typename V, bool DG>
+  __host__ __device__ constexpr int tma_stages_dg() { return DG ? 2 : tma_stages<V>(); }
   constexpr uint32_t TMA_SPIN = 1u << 22;
   constexpr uint32_t TMA_XWIN_MAX = 8192;              // entries of a staged x window
   constexpr uint64_t TMA_SMEM_MAX = 128u * 1024u;      // dynamic shared memory of all stages
@@ -149,7 +153,7 @@ namespace fb
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) uint64_t bar[TMA_STAGES];
     __shared__ double sh[32];
-    constexpr int NS = tma_stages<V>();
+    constexpr int NS = tma_stages_dg<V, DG>();
     constexpr uint32_t SPC = TMA_NT / 32;   // slices per chunk
     const uint32_t K = A.kw;
     const bool narrow = A.dcol != nullptr;
