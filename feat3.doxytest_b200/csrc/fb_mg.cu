@@ -587,7 +587,17 @@ namespace fb
     }
   }
 
-  template<typename V, typename S>
+  // SM: every tail level's vectors are in shared memory, so the pointers derive from the shared
+  // array alone and the compiler addresses them as shared memory (32-bit, no generic check)
+  template<bool SM, typename V, typename S>
+  __device__ __forceinline__ S* tail_vec_s(const TailParams<V, S>& tp, S* sbase, int t, int k)
+  {
+    if(SM)
+      return sbase + tp.lv[t].soff + uint32_t(k) * tp.lv[t].np;
+    return tail_vec(tp, sbase, t, k);
+  }
+
+  template<typename V, typename S, bool SM>
   __global__ void __launch_bounds__(TAIL_NT) k_tail(const __grid_constant__ TailParams<V, S> tp, const Scalars* __restrict__ sc)
   {
     pdl_wait();
@@ -630,8 +640,8 @@ namespace fb
     // the top level's input: b and sol1 = F(D .* b) written by the restriction above
     if(tps.lv[0].in_smem)
     {
-      S* b0 = tail_vec(tps, sbase, 0, 0);
-      S* x0 = tail_vec(tps, sbase, 0, 1);
+      S* b0 = tail_vec_s<SM>(tps, sbase, 0, 0);
+      S* x0 = tail_vec_s<SM>(tps, sbase, 0, 1);
       for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
       {
         b0[i] = tps.lv[0].b[i];
@@ -646,9 +656,9 @@ namespace fb
     {
       const TailLevel<V, S>& f = tps.lv[t];
       const TailLevel<V, S>& c = tps.lv[t + 1];
-      const S* fb = tail_vec(tps, sbase, t, 0);
-      S* xa = tail_vec(tps, sbase, t, 1);
-      S* xb = tail_vec(tps, sbase, t, 2);
+      const S* fb = tail_vec_s<SM>(tps, sbase, t, 0);
+      S* xa = tail_vec_s<SM>(tps, sbase, t, 1);
+      S* xb = tail_vec_s<SM>(tps, sbase, t, 2);
       int sel = 1;
       const bool skipped = skip_pre_sh[t] != 0;
       for(int k = 1; k < steps; ++k)
@@ -662,13 +672,13 @@ namespace fb
         sel = 3 - sel;
       }
       xsel[t] = sel;
-      S* fd = tail_vec(tps, sbase, t, 3);
+      S* fd = tail_vec_s<SM>(tps, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         fd[i] = defect_row<V, S, false>(f.A, fb, xa, f.dm, i);
       __syncthreads();
       const bool coarsest = (t + 2 == cnt);
-      S* cbv = tail_vec(tps, sbase, t + 1, 0);
-      S* cxv = coarsest ? (S*)nullptr : tail_vec(tps, sbase, t + 1, 1);
+      S* cbv = tail_vec_s<SM>(tps, sbase, t + 1, 0);
+      S* cxv = coarsest ? (S*)nullptr : tail_vec_s<SM>(tps, sbase, t + 1, 1);
       double sq = 0.0;
       for(uint32_t j = threadIdx.x; j < c.n; j += TAIL_NT)
         sq += restrict_row<V, S, false>(f.R, fd, cbv, cxv, c.dinv, c.dm, j);
@@ -683,7 +693,7 @@ namespace fb
     }
     {
       const TailLevel<V, S>& c = tps.lv[cnt - 1];
-      coarse_block<S, TAIL_NT>(tail_vec(tps, sbase, cnt - 1, 0), tail_vec(tps, sbase, cnt - 1, 1), c.n, tps.free_dofs,
+      coarse_block<S, TAIL_NT>(tail_vec_s<SM>(tps, sbase, cnt - 1, 0), tail_vec_s<SM>(tps, sbase, cnt - 1, 1), c.n, tps.free_dofs,
         tps.inv, tps.m);
       xsel[cnt - 1] = 1;
       __syncthreads();
@@ -691,15 +701,15 @@ namespace fb
     for(int t = cnt - 2; t >= 0; --t)
     {
       const TailLevel<V, S>& f = tps.lv[t];
-      S* xf = tail_vec(tps, sbase, t, xsel[t]);
-      const S* xc = tail_vec(tps, sbase, t + 1, xsel[t + 1]);
-      const S* fb = tail_vec(tps, sbase, t, 0);
-      S* fd = tail_vec(tps, sbase, t, 3);
+      S* xf = tail_vec_s<SM>(tps, sbase, t, xsel[t]);
+      const S* xc = tail_vec_s<SM>(tps, sbase, t + 1, xsel[t + 1]);
+      const S* fb = tail_vec_s<SM>(tps, sbase, t, 0);
+      S* fd = tail_vec_s<SM>(tps, sbase, t, 3);
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         xf[i] = prolong_row<V, S, false>(f.P, xc, xf, f.dm, i);
       __syncthreads();
-      S* ca = tail_vec(tps, sbase, t, 4);
-      S* cb = tail_vec(tps, sbase, t, 5);
+      S* ca = tail_vec_s<SM>(tps, sbase, t, 4);
+      S* cb = tail_vec_s<SM>(tps, sbase, t, 5);
       double sq = 0.0;
       for(uint32_t i = threadIdx.x; i < f.n; i += TAIL_NT)
         sq += post1_row<V, S, false>(f.A, fb, xf, fd, ca, f.dinv, f.dm, i);
@@ -737,7 +747,7 @@ namespace fb
     // the top level's solution goes to the global buffer the prolongation above reads
     if(tps.lv[0].in_smem)
     {
-      const S* xs = tail_vec(tps, sbase, 0, xsel[0]);
+      const S* xs = tail_vec_s<SM>(tps, sbase, 0, xsel[0]);
       S* xg = xsel[0] == 1 ? tps.lv[0].x : tps.lv[0].x2;
       for(uint32_t i = threadIdx.x; i < tps.lv[0].n; i += TAIL_NT)
         xg[i] = xs[i];
@@ -2181,7 +2191,15 @@ namespace fb
           s->launch_err = e;
       }
       else if(s->cfg.cycle == FB_CYCLE_V && s->cfg.adapt_cgc == FB_CGC_FIXED)
-        go(k_tail<V, S>, 1, TAIL_NT, smem, tp, s->sc);
+      {
+        bool all_smem = true;
+        for(int t = 0; t < tp.count; ++t)
+          all_smem = all_smem && tp.lv[t].in_smem;
+        if(all_smem)
+          go(k_tail<V, S, true>, 1, TAIL_NT, smem, tp, s->sc);
+        else
+          go(k_tail<V, S, false>, 1, TAIL_NT, smem, tp, s->sc);
+      }
       else
         go(k_tail_prog<V, S>, 1, TAIL_NT, smem, tp, s->tail_prog + s->seg_off[seg], int(s->seg_len[seg]), s->sc);
       ++launches;
@@ -2318,7 +2336,8 @@ namespace fb
     FB_TRY((set_tma_attr_dg<V, S, OpPost2<V, S, true, false>>(mx)));
     FB_TRY((set_tma_attr_dg<V, S, OpPost2<V, S, true, true>>(mx)));
     FB_TRY((set_tma_attr_dg<double, double, OpPcgQ>(mx)));
-    FB_CUDA(cudaFuncSetAttribute(k_tail<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
+    FB_CUDA(cudaFuncSetAttribute(k_tail<V, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
+    FB_CUDA(cudaFuncSetAttribute(k_tail<V, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     FB_CUDA(cudaFuncSetAttribute(k_tail_prog<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(TAIL_SMEM_MAX)));
     return FB_OK;
   }
