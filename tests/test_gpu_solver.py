@@ -298,3 +298,20 @@ def test_adaptive_cgc_mixed_precision(featlib, cuda, oracle_lib, cgc):
     _, x32, st32 = _solve(fb, levels, b, adapt_cgc=cgc, precision="f32")
     assert st64 == st32 == fb.Status.success
     assert rel_err(x32, x64) <= 1e-7
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_diagonal_storage_3d_against_oracle(featlib, cuda, oracle_lib, graph):
+    """3D Q1 (27 diagonals) in native numbering: the 27-wide diagonal-storage staged passes and row
+    sums, bitwise V-cycle and iterates against the C restatement."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(5, 3, rhs="gauss", gauss=AS.gauss_params(2, 3))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2)
+    x_ref, info = mg.solve(b)
+    z_ref = mg.vcycle(b)
+    for tma in (None, 64):
+        s, x, st = _solve(fb, levels, b, use_graph=graph, tma_rows=tma)
+        assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref), tma
+        assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+        assert rel_err(x, x_ref) <= PARITY
