@@ -3,7 +3,7 @@
 FP64 ("plain") mode: the V-cycle is bitwise equal to the reference (no global reductions inside it
 other than the smoother's skip test), the PCG iterates and the solution agree to 1e-12 relative
 (only the dot products and norms are summed in a different order).  Low-precision modes report
-their error against the FP64 result (north-star bound 1e-7 relative, residual 1e-8)."""
+their error against the FP64 result (bound 1e-7 relative at residual 1e-8)."""
 import os
 import tempfile
 
