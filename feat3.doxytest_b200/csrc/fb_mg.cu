@@ -3068,6 +3068,25 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   return FB_OK;
 }
 
+fb_status fb_multigrid_cycle_events(int cycle, int adapt_cgc, int num_levels, uint8_t* ops, uint8_t* levels,
+                                    uint64_t capacity, uint64_t* count)
+{
+  if(!count || num_levels < 2 || num_levels > 24 || cycle < FB_CYCLE_V || cycle > FB_CYCLE_W ||
+     adapt_cgc < FB_CGC_FIXED || adapt_cgc > FB_CGC_MIN_DEFECT || (capacity && (!ops || !levels)))
+  {
+    set_error("multigrid_cycle_events: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const std::vector<CycEv> ev = cycle_events(cycle, num_levels, adapt_cgc != FB_CGC_FIXED);
+  for(uint64_t i = 0; i < ev.size() && i < capacity; ++i)
+  {
+    ops[i] = ev[i].op;
+    levels[i] = ev[i].lvl;
+  }
+  *count = ev.size();
+  return FB_OK;
+}
+
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out)
 {
   if(!s || !out)

@@ -7,8 +7,9 @@ is the host-side mirror of the reference's interface.
 """
 from ._lib import FeatB200Error, exported_symbols, launch_count, lib  # noqa: F401
 from .lafem import DenseVector, SparseMatrixCSR, Transfer, UnitFilter, arch  # noqa: F401
-from .solver import (BatchPCG, MultiGrid, MultiGridAdaptCGC, MultiGridCycle, MultiGridHierarchy, MultiRhsPCG, PCG, Status,  # noqa: F401
-                     build_hierarchy, build_pcg_multigrid, new_coarse_inverse, new_jacobi_precond, new_multigrid,
-                     new_pcg, new_richardson, solve, status_success)
+from .solver import (BatchPCG, MultiGrid, MultiGridAdaptCGC, MultiGridCycle, MultiGridHierarchy,  # noqa: F401
+                     MultiRhsPCG, PCG, Status, build_hierarchy, build_pcg_multigrid, cycle_events,
+                     new_coarse_inverse, new_jacobi_precond, new_multigrid, new_pcg, new_richardson, solve,
+                     status_success)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -89,6 +89,7 @@ _PROTOS = {
     "fb_solver_solve_device": (I, [P, P, P, P, C.POINTER(SolveInfo)]),
     "fb_solver_vcycle": (I, [P, P, P]),
     "fb_solver_level_info": (I, [P, P]),
+    "fb_multigrid_cycle_events": (I, [I, I, I, P, P, U64, C.POINTER(C.c_uint64)]),
     "fb_solver_update_matrix": (I, [P, I, P, P]),
     "fb_solver_set_tolerances": (I, [P, D, D]),
     "fb_q1_pattern_2d": (I, [I, P, P, P]),

@@ -185,6 +185,26 @@ class MultiGrid:
         self.adapt_cgc = adapt_cgc
 
 
+EVENT_NAMES = ("pre", "def", "res", "crs", "pro", "post", "post_top", "proc", "postc", "postc_top")
+
+
+def cycle_events(cycle="V", num_levels=2, adapt_cgc="Fixed"):
+    """The events one multigrid cycle runs, [(name, level)] (fb_multigrid_cycle_events): what the
+    device executes for MultiGrid::_apply_cycle_v/_f/_w over num_levels levels, finest = 0."""
+    import numpy as np
+    cyc = {"V": 0, "F": 1, "W": 2}[cycle]
+    cgc = MultiGridAdaptCGC[adapt_cgc].value
+    n = C.c_uint64()
+    _lib.check(_lib.lib().fb_multigrid_cycle_events(cyc, cgc, int(num_levels), None, None, 0, C.byref(n)),
+               "fb_multigrid_cycle_events")
+    ops = np.zeros(max(1, n.value), dtype=np.uint8)
+    lvl = np.zeros(max(1, n.value), dtype=np.uint8)
+    _lib.check(_lib.lib().fb_multigrid_cycle_events(cyc, cgc, int(num_levels), ops.ctypes.data_as(C.c_void_p),
+                                                     lvl.ctypes.data_as(C.c_void_p), n.value, C.byref(n)),
+               "fb_multigrid_cycle_events")
+    return [(EVENT_NAMES[int(o)], int(l)) for o, l in zip(ops[:n.value], lvl[:n.value])]
+
+
 def new_multigrid(hierarchy, cycle=MultiGridCycle.V):
     return MultiGrid(hierarchy, cycle)
 

@@ -280,6 +280,25 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
  * removed).  `out` holds 3 * num_levels entries. */
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
 
+/* Events of one multigrid cycle, as a solver with this cycle and coarse-grid correction runs them */
+#define FB_EV_PRE 0        /* pre-smoothing steps 2.. on a level (step 1 comes with the restriction) */
+#define FB_EV_DEF 1        /* defect on a level */
+#define FB_EV_RES 2        /* restriction from a level to the next coarser one */
+#define FB_EV_CRS 3        /* coarse solve */
+#define FB_EV_PRO 4        /* prolongation into a level (x += P x_c) */
+#define FB_EV_POST 5       /* post-smoothing (also the peak smoother) on a level */
+#define FB_EV_POST_TOP 6   /* the finest level's last post-smoothing (forms the PCG's z and r.z) */
+#define FB_EV_PROC 7       /* prolongation with adaptive coarse-grid correction */
+#define FB_EV_POSTC 8      /* post-smoothing from the defect that FB_EV_PROC updated */
+#define FB_EV_POSTC_TOP 9  /* as FB_EV_POST_TOP after FB_EV_PROC */
+
+/* The event list of one cycle over num_levels levels (finest = level 0): MultiGrid::_apply_cycle_v,
+ * _f, _w with _apply_rest, _apply_prol and _apply_smooth_peak (kernel/solver/multigrid.hpp:1335-1990).
+ * Writes at most `capacity` (op, level) pairs into ops[] / levels[]; *count receives the full
+ * number of events.  Host only (no device is touched). */
+fb_status fb_multigrid_cycle_events(int cycle, int adapt_cgc, int num_levels, uint8_t* ops, uint8_t* levels,
+                                    uint64_t capacity, uint64_t* count);
+
 /* New stopping tolerances for the following solves (IterativeSolver::set_tol_rel/set_tol_abs,
  * kernel/solver/iterative.hpp): converged when ||d|| <= tol_abs and ||d|| <= tol_rel * ||d_0||. */
 fb_status fb_solver_set_tolerances(fb_solver* s, double tol_rel, double tol_abs);
