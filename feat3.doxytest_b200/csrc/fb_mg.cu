@@ -3068,6 +3068,54 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
   return FB_OK;
 }
 
+fb_status fb_matrix_storage_plan(const fb_csr_host* M, const uint64_t* empty_rows, uint64_t num_empty, int rcm,
+                                 int allow_diag, fb_storage_plan* out)
+{
+  if(!M || !out || (num_empty && !empty_rows))
+  {
+    set_error("matrix_storage_plan: bad arguments");
+    return FB_ERR_ARG;
+  }
+  HostCsr A;
+  const std::string e = import_csr(A, M->rows, M->columns, M->used_elements, M->row_ptr, M->col_ind, M->val, false);
+  if(!e.empty())
+  {
+    set_error("matrix_storage_plan: " + e);
+    return FB_ERR_ARG;
+  }
+  std::vector<uint8_t> empty(A.rows, 0);
+  for(uint64_t k = 0; k < num_empty; ++k)
+  {
+    if(empty_rows[k] >= A.rows)
+    {
+      set_error("matrix_storage_plan: empty row out of range");
+      return FB_ERR_ARG;
+    }
+    empty[size_t(empty_rows[k])] = 1;
+  }
+  if(rcm && A.rows == A.cols)
+  {
+    const std::vector<uint32_t> perm = rcm_order(A);
+    const std::vector<uint32_t> inv = inverse_perm(perm);
+    A = permute(A, perm, inv);
+    std::vector<uint8_t> ep(A.rows);
+    for(uint32_t k = 0; k < A.rows; ++k)
+      ep[k] = empty[perm[k]];
+    empty.swap(ep);
+  }
+  const HostSell H = build_sell(A, &empty, true, allow_diag != 0);
+  const uint32_t ns = (H.rows + 31u) / 32u;
+  uint32_t kmax = H.kw;
+  for(uint32_t sl = 0; sl < ns; ++sl)
+    kmax = std::max(kmax, (H.soff[sl + 1] - H.soff[sl]) / 32u);
+  out->kind = !H.doff.empty() ? 2 : (H.kw ? 1 : 0);
+  out->narrow = H.narrow ? 1 : 0;
+  out->width = kmax;
+  out->diagonals = uint32_t(H.doff.size());
+  out->entries = H.entries;
+  return FB_OK;
+}
+
 fb_status fb_multigrid_cycle_events(int cycle, int adapt_cgc, int num_levels, uint8_t* ops, uint8_t* levels,
                                     uint64_t capacity, uint64_t* count)
 {

@@ -10,6 +10,6 @@ from .lafem import DenseVector, SparseMatrixCSR, Transfer, UnitFilter, arch  # n
 from .solver import (BatchPCG, MultiGrid, MultiGridAdaptCGC, MultiGridCycle, MultiGridHierarchy,  # noqa: F401
                      MultiRhsPCG, PCG, Status, build_hierarchy, build_pcg_multigrid, cycle_events,
                      new_coarse_inverse, new_jacobi_precond, new_multigrid, new_pcg, new_richardson, solve,
-                     status_success)
+                     status_success, storage_plan)
 
 __all__ = [n for n in dir() if not n.startswith("_")]

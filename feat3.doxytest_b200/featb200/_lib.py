@@ -37,6 +37,11 @@ class SolverConfig(C.Structure):
                 ("adapt_cgc", C.c_int)]
 
 
+class StoragePlan(C.Structure):
+    _fields_ = [("kind", C.c_int), ("narrow", C.c_int), ("width", C.c_uint32), ("diagonals", C.c_uint32),
+                ("entries", C.c_uint64)]
+
+
 class SolveInfo(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("def_init", C.c_double),
                 ("def_final", C.c_double), ("solve_ms", C.c_double), ("kernel_launches", C.c_uint64),
@@ -90,6 +95,7 @@ _PROTOS = {
     "fb_solver_vcycle": (I, [P, P, P]),
     "fb_solver_level_info": (I, [P, P]),
     "fb_multigrid_cycle_events": (I, [I, I, I, P, P, U64, C.POINTER(C.c_uint64)]),
+    "fb_matrix_storage_plan": (I, [C.POINTER(CsrHost), P, U64, I, I, C.POINTER(StoragePlan)]),
     "fb_solver_update_matrix": (I, [P, I, P, P]),
     "fb_solver_set_tolerances": (I, [P, D, D]),
     "fb_q1_pattern_2d": (I, [I, P, P, P]),

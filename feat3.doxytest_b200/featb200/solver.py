@@ -205,6 +205,19 @@ def cycle_events(cycle="V", num_levels=2, adapt_cgc="Fixed"):
     return [(EVENT_NAMES[int(o)], int(l)) for o, l in zip(ops[:n.value], lvl[:n.value])]
 
 
+def storage_plan(matrix, empty_rows=None, ordering="native", diagonal=True):
+    """How the solver stores `matrix` (a SparseMatrixCSR) on the device (fb_matrix_storage_plan):
+    dict(kind='sliced'|'ell'|'diagonal', width, narrow, diagonals, entries)."""
+    c = matrix.c_host()
+    er = np.ascontiguousarray(np.zeros(0) if empty_rows is None else empty_rows, dtype=np.uint64)
+    out = _lib.StoragePlan()
+    _lib.check(_lib.lib().fb_matrix_storage_plan(C.byref(c), er.ctypes.data_as(C.c_void_p), er.size,
+                                                  1 if ordering == "rcm" else 0, 1 if diagonal else 0,
+                                                  C.byref(out)), "fb_matrix_storage_plan")
+    return {"kind": ("sliced", "ell", "diagonal")[out.kind], "width": int(out.width), "narrow": bool(out.narrow),
+            "diagonals": int(out.diagonals), "entries": int(out.entries)}
+
+
 def new_multigrid(hierarchy, cycle=MultiGridCycle.V):
     return MultiGrid(hierarchy, cycle)
 

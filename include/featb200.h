@@ -280,6 +280,21 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
  * removed).  `out` holds 3 * num_levels entries. */
 fb_status fb_solver_level_info(const fb_solver* s, uint64_t* out);
 
+/* How a solver would store a matrix on the device (host only, no device touched).  kind: 0 sliced
+ * ELL, 1 uniform-width ELL, 2 diagonal storage; width: entries per row (the widest slice for sliced
+ * ELL); narrow: column indices as int16 offsets from the row; diagonals: the number of diagonals
+ * (kind 2); entries: stored slots including padding.  rcm != 0: in reverse Cuthill-McKee order (the
+ * solver's FB_ORDER_RCM); allow_diag != 0: diagonal storage allowed (the solver's `diagonal`, for
+ * system matrices).  Rows listed in empty_rows (Dirichlet rows, NULL for none) are stored empty. */
+typedef struct
+{
+  int kind, narrow;
+  uint32_t width, diagonals;
+  uint64_t entries;
+} fb_storage_plan;
+fb_status fb_matrix_storage_plan(const fb_csr_host* M, const uint64_t* empty_rows, uint64_t num_empty, int rcm,
+                                 int allow_diag, fb_storage_plan* out);
+
 /* Events of one multigrid cycle, as a solver with this cycle and coarse-grid correction runs them */
 #define FB_EV_PRE 0        /* pre-smoothing steps 2.. on a level (step 1 comes with the restriction) */
 #define FB_EV_DEF 1        /* defect on a level */
