@@ -162,6 +162,8 @@ typedef struct
   double* cinv;
   /* PCG vectors on the finest level */
   double *r, *p, *t;
+  int cycle;             /* 0 V, 1 F, 2 W (MultiGridCycle) */
+  int cgc;               /* 0 fixed, 1 energy minimisation, 2 defect minimisation (MultiGridAdaptCGC) */
 } oc_mg;
 
 static int coarse_factor(oc_mg* mg)
@@ -334,39 +336,134 @@ static void coarse_apply(const oc_mg* mg, double* x, const double* b)
   }
 }
 
-/* cor = MG_V(def) (multigrid.hpp:1270-1350) */
-int oc_mg_vcycle(oc_mg* mg, double* cor, const double* def)
+/* MultiGrid::_apply_rest(cur_lvl, cur_smooth) (multigrid.hpp:1713-1840): pre-smoothing and defect on
+ * every level but cur_lvl when cur_smooth is false, then restriction to the next coarser level */
+static void apply_rest(oc_mg* mg, int cur, int smooth)
 {
-  const int L = mg->nlevels;
-  memcpy(mg->lv[0].rhs, def, sizeof(double) * mg->lv[0].n);
-  /* _apply_rest(top, true) */
-  for(int i = 0; i + 1 < L; ++i)
+  const int last = mg->nlevels - 1;
+  for(int i = cur; i < last; ++i)
   {
     oc_level* f = &mg->lv[i];
     oc_level* c = &mg->lv[i + 1];
-    richardson_apply(mg, f, f->sol, f->rhs);
-    oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+    if(smooth || i > cur)
+    {
+      richardson_apply(mg, f, f->sol, f->rhs);
+      oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+    }
     oc_filter_def(f->def, f->in.fidx, f->in.nf);
     oc_csr_apply(c->rhs, 1.0, f->def, 0.0, c->rhs, &f->in.R, 0);
     oc_filter_def(c->rhs, c->in.fidx, c->in.nf);
   }
-  /* _apply_coarse */
-  if(L > 0)
-    coarse_apply(mg, mg->lv[L - 1].sol, mg->lv[L - 1].rhs);
-  /* _apply_prol(top, true) */
-  for(int i = L - 2; i >= 0; --i)
+}
+
+/* MultiGrid::_apply_prol(cur_lvl, cur_smooth) (multigrid.hpp:1845-1990): prolongation, the (adaptive)
+ * coarse-grid correction, post-smoothing on every level but cur_lvl when cur_smooth is false */
+static void apply_prol(oc_mg* mg, int cur, int smooth)
+{
+  const int last = mg->nlevels - 1;
+  for(int i = last - 1; i >= cur; --i)
   {
     oc_level* f = &mg->lv[i];
     oc_level* c = &mg->lv[i + 1];
+    const uint64_t n = f->n;
     oc_csr_apply(f->cor, 1.0, c->sol, 0.0, f->cor, &f->in.P, 0);
     oc_filter_def(f->cor, f->in.fidx, f->in.nf);
-    oc_axpy(f->sol, 1.0, f->cor, f->sol, f->n);
-    oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
-    oc_filter_def(f->def, f->in.fidx, f->in.nf);
-    richardson_apply(mg, f, f->cor, f->def);
-    oc_axpy(f->sol, 1.0, f->cor, f->sol, f->n);
+    double w = 1.0;
+    if(mg->cgc)
+    {
+      oc_csr_apply(f->tmp, 1.0, f->cor, 0.0, f->tmp, &f->in.A, 0);
+      oc_filter_def(f->tmp, f->in.fidx, f->in.nf);
+      if(mg->cgc == 1)
+        w = oc_dot(f->def, f->cor, n) / oc_dot(f->tmp, f->cor, n);
+      else
+        w = oc_dot(f->def, f->tmp, n) / oc_dot(f->tmp, f->tmp, n);
+    }
+    oc_axpy(f->sol, w, f->cor, f->sol, n);
+    if(smooth || i > cur)
+    {
+      if(mg->cgc)
+        oc_axpy(f->def, -w, f->tmp, f->def, n);
+      else
+      {
+        oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+        oc_filter_def(f->def, f->in.fidx, f->in.nf);
+      }
+      richardson_apply(mg, f, f->cor, f->def);
+      oc_axpy(f->sol, 1.0, f->cor, f->sol, n);
+    }
   }
+}
+
+/* MultiGrid::_apply_smooth_peak + _apply_smooth_def (multigrid.hpp:1591-1700) with the peak smoother */
+static void smooth_peak(oc_mg* mg, int l)
+{
+  oc_level* f = &mg->lv[l];
+  oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+  oc_filter_def(f->def, f->in.fidx, f->in.nf);
+  richardson_apply(mg, f, f->cor, f->def);
+  oc_filter_def(f->cor, f->in.fidx, f->in.nf);
+  oc_axpy(f->sol, 1.0, f->cor, f->sol, f->n);
+  oc_csr_apply(f->def, -1.0, f->sol, 1.0, f->rhs, &f->in.A, 0);
+  oc_filter_def(f->def, f->in.fidx, f->in.nf);
+}
+
+static void apply_coarse(oc_mg* mg)
+{
+  coarse_apply(mg, mg->lv[mg->nlevels - 1].sol, mg->lv[mg->nlevels - 1].rhs);
+}
+
+/* cor = MG(def): MultiGrid::_apply_cycle_v / _f / _w (multigrid.hpp:1335-1440) */
+int oc_mg_vcycle(oc_mg* mg, double* cor, const double* def)
+{
+  const int last = mg->nlevels - 1;
+  memcpy(mg->lv[0].rhs, def, sizeof(double) * mg->lv[0].n);
+  apply_rest(mg, 0, 1);
+  if(mg->cycle == 1)
+  {
+    for(int pk = last - 1; pk > 0; --pk)
+    {
+      apply_coarse(mg);
+      apply_prol(mg, pk, 0);
+      smooth_peak(mg, pk);
+      apply_rest(mg, pk, 0);
+    }
+  }
+  else if(mg->cycle == 2)
+  {
+    apply_coarse(mg);
+    int counters[64];
+    for(int i = 0; i <= last; ++i)
+      counters[i] = 0;
+    const long num_cgs = 1L << last;
+    for(long cgs = 1; cgs < num_cgs; ++cgs)
+    {
+      int pk = last;
+      while(pk > 0)
+        if(counters[--pk] == 0)
+          break;
+      for(int i = last - 1; i > pk; --i)
+        counters[i] = 0;
+      ++counters[pk];
+      apply_prol(mg, pk, 0);
+      smooth_peak(mg, pk);
+      apply_rest(mg, pk, 0);
+      apply_coarse(mg);
+    }
+  }
+  if(mg->cycle != 2)
+    apply_coarse(mg);
+  apply_prol(mg, 0, 1);
   memcpy(cor, mg->lv[0].sol, sizeof(double) * mg->lv[0].n);
+  return 0;
+}
+
+/* MultiGrid::set_cycle / set_adapt_cgc */
+int oc_mg_set_cycle(oc_mg* mg, int cycle, int cgc)
+{
+  if(cycle < 0 || cycle > 2 || cgc < 0 || cgc > 2 || mg->nlevels > 62)
+    return 1;
+  mg->cycle = cycle;
+  mg->cgc = cgc;
   return 0;
 }
 

@@ -65,6 +65,7 @@ def lib():
         L.oc_mg_create.restype = C.c_void_p
         L.oc_mg_destroy.argtypes = [C.c_void_p]
         L.oc_mg_vcycle.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oc_mg_set_cycle.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oc_pcg_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                    C.c_void_p, C.POINTER(C.c_int)]
         L.oc_pcg_jacobi.argtypes = [C.POINTER(_Csr), C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
@@ -119,9 +120,10 @@ def norm2(x):
 
 
 class MultigridPCG:
-    """The FP64 PCG + V(steps, steps) multigrid of the reference, restated in C."""
+    """The FP64 PCG + multigrid (V, F or W cycle with `steps` pre- and post-smoothing steps; fixed,
+    energy- or defect-minimising coarse-grid correction) of the reference, restated in C."""
 
-    def __init__(self, levels, omega=0.7, steps=2):
+    def __init__(self, levels, omega=0.7, steps=2, cycle="V", cgc="fixed"):
         self._keep = []
         arr = (_LevelIn * len(levels))()
         for i, lv in enumerate(levels):
@@ -140,6 +142,9 @@ class MultigridPCG:
         self._arr = arr
         self.n = levels[0]["A"].shape[0]
         self._h = lib().oc_mg_create(len(levels), arr, omega, steps)
+        if lib().oc_mg_set_cycle(self._h, {"V": 0, "F": 1, "W": 2}[cycle.upper()],
+                                 {"fixed": 0, "energy": 1, "defect": 2}[cgc]) != 0:
+            raise ValueError("unsupported cycle / coarse-grid correction")
 
     def vcycle(self, d):
         d = np.ascontiguousarray(d, dtype=np.float64)
