@@ -315,3 +315,26 @@ def test_diagonal_storage_3d_against_oracle(featlib, cuda, oracle_lib, graph):
         assert np.array_equal(s.apply_precond(fb.DenseVector(b)).elements, z_ref), tma
         assert st == fb.Status.success and s.get_num_iter() == info["iters"]
         assert rel_err(x, x_ref) <= PARITY
+
+
+@pytest.mark.parametrize("cycle", ["F", "W"])
+@pytest.mark.parametrize("cgc", ["fixed", "energy"])
+def test_cycles_diagonal_storage_against_oracle(featlib, cuda, oracle_lib, cycle, cgc):
+    """F and W cycles, fixed and adaptive coarse-grid correction, on a lexicographically numbered
+    problem (diagonal storage) against the C restatement: bitwise with the fixed correction, to
+    1e-12 with the adaptive one (its step length sums dot products in another order)."""
+    from featb200 import assembly as AS
+    fb = featlib
+    levels, b = AS.poisson_hierarchy(6, 2, rhs="gauss", gauss=AS.gauss_params(3, 2))
+    mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2, cycle=cycle, cgc=cgc)
+    x_ref, info = mg.solve(b)
+    z_ref = mg.vcycle(b)
+    mode = {"fixed": "Fixed", "energy": "MinEnergy"}[cgc]
+    s, x, st = _solve(fb, levels, b, cycle=cycle, adapt_cgc=mode, tma_rows=64)
+    z = s.apply_precond(fb.DenseVector(b)).elements
+    if cgc == "fixed":
+        assert np.array_equal(z, z_ref)
+    else:
+        assert rel_err(z, z_ref) <= 1e-12
+    assert st == fb.Status.success and s.get_num_iter() == info["iters"]
+    assert rel_err(x, x_ref) <= 1e-11
