@@ -5,7 +5,9 @@
 Default workload (the configuration the headline metric is quoted on): 2D Poisson, Q1 on the unit
 square, level 10 (1,050,625 DOFs, 9,443,329 nnz), right-hand side a sum of 8 seeded Gaussians,
 PCG preconditioned by one V(2,2) cycle (Richardson + Jacobi omega 0.7, exact coarse solve on level
-1) run in FP32 inside FP64 PCG (iterative refinement), relative residual 1e-8.
+1) run in FP32 inside FP64 PCG (iterative refinement), relative residual 1e-8.  The problem is
+numbered lexicographically and solved in that order (--ordering native), so its system matrices
+are held as diagonals; --ordering rcm gives the sliced-ELL form.
 
 One step = one complete solve from a zero initial guess with the matrices resident in HBM.  Each
 step is timed with CUDA events on the stream of the call; the L2 is overwritten between steps
