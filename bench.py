@@ -58,10 +58,9 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "poisson2d_l10_mixed"
 
-# DRAM bytes of one launch of the roofline kernel, from one ncu capture (summarised in profiles/):
-# (workload, ordering) -> bytes read + written
-MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "rcm"): 104.055808e6 + 4.434432e6,
-                    ("poisson2d_l10_mixed", "native"): 85.146368e6 + 3.247616e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch, from an ncu capture of
+# the kernel as built from the current sources: (workload, ordering, kernel) -> bytes
+MEASURED_TRAFFIC = {("poisson2d_l10_mixed", "native", "pcg_spmv"): 85.146368e6 + 3.247616e6}
 
 
 def dist_env():
@@ -147,39 +146,43 @@ def build_problem(dim, level, rhs_kind):
     return levels, b, gauss
 
 
+def batch_levels(count=256):
+    from featb200 import assembly as AS
+    return AS.batch_family_levels(count)
+
+
 def _batch_instance(args):
-    level, k = args
     sys.path.insert(0, os.path.join(ROOT, "feat3.doxytest_b200"))
     from featb200 import assembly as AS
-    lv, b = AS.poisson_hierarchy(level, 2, rhs="gauss", gauss=AS.gauss_params(10_000 + 2 * k, 2),
-                                 field=AS.field_params(10_001 + 2 * k))
-    return lv, b
+    level, k = args
+    return AS.batch_instance(level, k)
 
 
-def batch_levels(count=256, seed=7):
-    return [int(v) for v in np.random.default_rng(seed).integers(5, 10, size=count)]
+def start_batch_build(count=256):
+    """Config-4 family assembled on a spawn-started process pool (host set-up, no CUDA in the
+    workers); returns (levels, pool, async result)."""
+    import multiprocessing as mp
+    levels = batch_levels(count)
+    pool = mp.get_context("spawn").Pool(min(32, os.cpu_count() or 1))
+    res = pool.map_async(_batch_instance, [(L, k) for k, L in enumerate(levels)])
+    return levels, pool, res
+
+
+def finish_batch_build(started):
+    levels, pool, res = started
+    inst = res.get()
+    pool.close()
+    pool.join()
+    return levels, inst
 
 
 def build_batch_problem(count=256):
-    """Config-4 family generated on a spawn-started process pool (before any CUDA use)."""
-    import multiprocessing as mp
-    levels = batch_levels(count)
-    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-        inst = pool.map(_batch_instance, [(L, k) for k, L in enumerate(levels)])
-    return levels, inst
+    return finish_batch_build(start_batch_build(count))
 
 
 def build_rhs64_problem():
     from featb200 import assembly as AS
-    levels, _ = AS.poisson_hierarchy(6, 3, rhs="sine")
-    fidx = levels[0]["filter"].indices.astype(np.int64)
-    B = np.zeros((levels[0]["matrix"].rows(), 64))
-    for j in range(64):
-        g = AS.gauss_params(100 + j, 3, width=(0.03, 0.12))
-        b = AS.load_vector(6, lambda *xs: AS.gauss_eval(g, *xs), 3)
-        b[fidx] = 0.0
-        B[:, j] = b
-    return levels, B
+    return AS.rhs64_family(6, 3, 64)
 
 
 class L2Flush:
@@ -471,6 +474,117 @@ def run_reference(args):
     return 0
 
 
+PASS_KERNELS = {
+    "pcg_spmv": "k_tma_pass<OpPcgQ>: FP64 q = F(A p) and q.p (PCG)",
+    "mg_smooth": "k_tma_pass<OpSmooth>: pre-smoothing step 2",
+    "mg_defect": "k_tma_pass<OpDefect>: defect d = F(b - A x) before restriction",
+    "mg_restrict": "k_tma_pass<OpRestrict>: b_c = F(R d), sol1_c = F(D_c b_c)",
+    "mg_prolong": "k_tma_pass<OpProlong>: x += F(P x_c)",
+    "mg_post1": "k_tma_pass<OpPost1>: post-smoothing step 1 (defect, Jacobi correction, norm)",
+    "mg_post2": "k_tma_pass<OpPost2>: post-smoothing step 2 with the PCG's z and r.z",
+}
+
+
+def pass_table(solver, levels, precision, reps=20):
+    """Each finest-level pass of a solve timed alone (cold L2) with its CSR-algorithmic bytes (the
+    survey's definition: nnz * (value + 4 B index) + (rows + 1) * 4 B + the vectors it reads and
+    writes) and the bytes it moves as stored on the device (solver's count)."""
+    sv = {"f64": 8, "f32": 4, "f32_bf16": 2}[precision]
+    sx = 8 if precision == "f64" else 4
+    A = levels[0]["matrix"]
+    n = int(A.rows())
+    nnz = int(A.used_elements())
+    tr = levels[0]["transfer"]
+    nc = int(tr.rest.rows())
+    nnz_r, nnz_p = int(tr.rest.used_elements()), int(tr.prol.used_elements())
+
+    def csr(nz, rows, sval):
+        return nz * (sval + 4) + (rows + 1) * 4
+
+    alg = {
+        "pcg_spmv": (csr(nnz, n, 8) + 2 * n * 8, "CSR FP64: nnz*(8+4) + (n+1)*4 + n*8 gathered p + n*8 q written"),
+        "mg_smooth": (csr(nnz, n, sv) + n * sx * 4, "CSR: nnz*(s_v+4) + (n+1)*4 + x gathered, x' written, b and D read"),
+        "mg_defect": (csr(nnz, n, sv) + n * sx * 3, "CSR: nnz*(s_v+4) + (n+1)*4 + x gathered, d written, b read"),
+        "mg_post1": (csr(nnz, n, sv) + n * sx * 5, "CSR: nnz*(s_v+4) + (n+1)*4 + x gathered, b and D read, d and c written"),
+        "mg_post2": (csr(nnz, n, sv) + n * sx * 4 + n * 16,
+                     "CSR: nnz*(s_v+4) + (n+1)*4 + c gathered, d, D, x read (s_x), r read and z written (FP64)"),
+        "mg_restrict": (csr(nnz_r, nc, sv) + n * sx + nc * sx * 3,
+                        "CSR of R: nnz_R*(s_v+4) + (n_c+1)*4 + d gathered, b_c and sol1_c written, D_c read"),
+        "mg_prolong": (csr(nnz_p, n, sv) + nc * sx + 2 * n * sx,
+                       "CSR of P: nnz_P*(s_v+4) + (n+1)*4 + x_c gathered, x read and written"),
+    }
+    out = {}
+    for k, (by, definition) in alg.items():
+        ms, stored = solver.time_kernel(k, reps=reps, flush_l2=True)
+        out[k] = {"kernel": PASS_KERNELS[k], "us": ms * 1e3, "csr_bytes": by, "csr_definition": definition,
+                  "csr_gbs": by / (ms * 1e-3) / 1e9, "stored_bytes": stored, "stored_gbs": stored / (ms * 1e-3) / 1e9}
+    return out
+
+
+def run_target(args, batch, flush, torch, fb, stream):
+    """The method's target measured on the uneven-instance family (256 instances, levels 5..9,
+    kappa fields): arm A = the plain FP64 drop-in solver on every instance one after the other (a
+    solver per instance, each solve timed alone on the device with a cold L2); arm B = the same
+    instances in one FP32-in-FP64 batched solve.  Both stop at 1e-8 relative residual per instance.
+    Returns the comparison (ms per set, ratio, largest error of arm B against arm A's FP64
+    solution)."""
+    levels, inst = batch
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    xs_a, t_a, it_a, ok_a = [], [], [], True
+    for lv, b in inst:
+        s = fb.build_pcg_multigrid(lv, precision="f64", ordering="native")
+        rhs = torch.tensor(b, device="cuda")
+        x = torch.zeros_like(rhs)
+        s.correct_device(x, rhs, stream)                  # warm-up (untimed)
+        flush()
+        x.zero_()
+        ev0.record(stream)
+        st = s.correct_device(x, rhs, stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        t_a.append(ev0.elapsed_time(ev1))
+        it_a.append(s.get_num_iter())
+        ok_a = ok_a and st == fb.Status.success
+        xs_a.append(x.cpu().numpy())
+        s.done()
+    hs = [fb.build_hierarchy(lv) for lv, _ in inst]
+    bat = fb.BatchPCG(hs, precision="f32", ordering="native")
+    rhs = torch.tensor(np.concatenate([b for _, b in inst]), device="cuda")
+    sol = torch.zeros_like(rhs)
+    for _ in range(args.warmup):
+        sol.zero_()
+        bat.solve_device(sol, rhs, stream)
+    t_b = []
+    for _ in range(max(3, min(args.steps, 10))):
+        flush()
+        sol.zero_()
+        ev0.record(stream)
+        bat.solve_device(sol, rhs, stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        t_b.append(ev0.elapsed_time(ev1))
+    xb = bat.split(sol.cpu().numpy())
+    err = max(float(np.linalg.norm(xb[k] - xs_a[k]) / np.linalg.norm(xs_a[k])) for k in range(len(inst)))
+    its_b = bat.iterations()
+    ok_b = all(st == fb.Status.success for st in bat.statuses())
+    bat.done()
+    ms_a, ms_b = float(np.sum(t_a)), float(np.mean(t_b))
+    return {"family": f"{len(inst)} -div(kappa grad u)=f instances, levels uniform in 5..9 (seed 7), kappa = "
+                      "exp(16x16-mode field), 8-Gaussian f; stop at 1e-8 relative residual per instance",
+            "instances": len(inst), "dofs": int(sum(b.size for _, b in inst)),
+            "plain_fp64_ms": ms_a, "plain_fp64_definition": "sum over the instances of one FP64 PCG-multigrid solve "
+                                                            "each (device time, cold L2, solver set-up excluded)",
+            "batched_mixed_ms": ms_b, "batched_mixed_definition": "one FP32-in-FP64 batched solve of all instances "
+                                                                  "(device time, cold L2, mean of the timed repeats)",
+            "ratio": ms_a / ms_b, "plain_solves_per_s": len(inst) * 1e3 / ms_a,
+            "batched_solves_per_s": len(inst) * 1e3 / ms_b,
+            "max_rel_err_vs_fp64": err, "error_reference": "arm A's FP64 solutions (the plain path, pinned to the "
+                                                           "FP64 oracle within 1e-12 by the tests)",
+            "iterations_plain": [int(min(it_a)), int(max(it_a))], "iterations_batched": [int(min(its_b)), int(max(its_b))],
+            "all_success": bool(ok_a and ok_b), "warm_start": "not used (it does not pay at this accuracy)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -500,6 +614,9 @@ def main():
     ap.add_argument("--ws-train", type=int, default=20000, help="training instances (learned warm start)")
     ap.add_argument("--ws-epochs", type=int, default=20)
     ap.add_argument("--ws-eval", type=int, default=1000, help="unseen evaluation instances")
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the plain-FP64 vs batched-mixed comparison on the uneven-instance family")
+    ap.add_argument("--target-count", type=int, default=256, help="instances of that comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -509,6 +626,12 @@ def main():
         return run_warmstart(args)
     if args.workload in ("poisson2d_batch256_mixed", "poisson3d_l6_rhs64_mixed"):
         return run_multi(args, "batch" if "batch" in args.workload else "rhs64")
+
+    # the target comparison's instances are assembled on host worker processes while the main
+    # workload's problem is assembled (single-GPU runs of the default workload only)
+    started = None
+    if not args.no_target and not args.profile_solves and dist_env()[1] == 1 and args.workload == DEFAULT_WORKLOAD:
+        started = start_batch_build(args.target_count)
 
     import torch
     rank, world, local = dist_env()
@@ -524,6 +647,8 @@ def main():
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
     levels, b, gauss = build_problem(dim, level, rhs_kind)
     n = b.size
+    # every timed region runs with idle host cores: the instance build finishes first
+    batch = finish_batch_build(started) if started is not None else None
     # a profiler cannot see the kernels of a graph with a device-side loop: profile runs launch per kernel
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
@@ -615,25 +740,26 @@ def main():
         extra["error_vs_fp64"] = float(np.abs(x - x64).max() / np.abs(x64).max())
         plain.done()
 
-    # roofline of the dominant kernel, timed alone on the solver's stream with a cold L2
+    # every finest-level pass timed alone on the solver's stream with a cold L2: the roofline kernel
+    # is the one with the largest time per solve (each runs once per V-cycle / PCG iteration)
     peak, peak_kind = read_peaks()
-    kern = "pcg_spmv"
-    ms_k, by_k = solver.time_kernel(kern, reps=20, flush_l2=True)
-    ms_d, by_d = solver.time_kernel("mg_defect", reps=20, flush_l2=True)
-    # algorithmic bytes of the CSR operation (independent of the device storage): FP64 q = A p with
-    # u32 indices; the V-cycle defect in its precision, reading b as well
-    nnz0, n0 = int(levels[0]["matrix"].used_elements()), int(n)
-    alg_k = csr_alg_bytes(nnz0, n0, n0, 8, 4, 8)
-    sv = {"f64": 8, "f32": 4, "f32_bf16": 2}[precision]
-    sx = 8 if precision == "f64" else 4
-    alg_d = csr_alg_bytes(nnz0, n0, n0, sv, 4, sx, row_vectors=1)
-    achieved = alg_k / (ms_k * 1e-3) / 1e9
-    spmv_gbs = {"pcg_spmv_f64": achieved, "mg_defect_" + precision: alg_d / (ms_d * 1e-3) / 1e9}
+    passes = pass_table(solver, levels, precision)
+    dom = max(passes, key=lambda k: passes[k]["us"])
+    dp = passes[dom]
+    traffic = MEASURED_TRAFFIC.get((args.workload, args.ordering, dom))
+    spmv_gbs = {"pcg_spmv_f64": passes["pcg_spmv"]["csr_gbs"],
+                "mg_defect_" + precision: passes["mg_defect"]["csr_gbs"]}
     # where a preconditioner application goes: one whole cycle, and its coarse-level tail kernel
     breakdown = {"mg_cycle_us": solver.time_kernel("mg_cycle", reps=20, flush_l2=False)[0] * 1e3}
     if args.tail_rows != 0 and args.cluster_rows in (None, 0):
         breakdown["mg_tail_us"] = solver.time_kernel("mg_tail", reps=20, flush_l2=False)[0] * 1e3
         breakdown["mg_tail_us_cold_l2"] = solver.time_kernel("mg_tail", reps=20, flush_l2=True)[0] * 1e3
+    # the whole solve: bytes the launched kernels move as stored (solver's own count) / device time
+    solve_bytes = float(solver.info.bytes_moved)
+    solve_gbs = solve_bytes / (ms_per_step * 1e-3) / 1e9
+    whole_solve = {"bytes_stored": solve_bytes, "ms": ms_per_step, "gbs": solve_gbs, "frac": solve_gbs / peak,
+                   "definition": "sum over the solve's launches of the matrix bytes as stored + gathered vector + "
+                                 "row-wise vectors + masks, divided by the device time of the solve"}
 
     # end to end through the C ABI with host buffers (copies inside the timed region)
     pin_rhs = torch.tensor(b).pin_memory()
@@ -651,6 +777,8 @@ def main():
             e2e_t.append((t1 - t0) * 1e3)
     e2e_ms = float(np.mean(e2e_t))
 
+    target = run_target(args, batch, flush, torch, fb, stream) if batch is not None else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         res = cpu_reference_times(dim, level, rhs_kind, gauss, 5)
@@ -664,26 +792,29 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if precision != "f64" else "f64", "data": "synthetic",
-                "config": {"workload": args.workload + ": " + desc, "dofs": int(n), "nnz": int(info_lv[0][1]),
+                "config": {"workload": args.workload + ": " + desc, "dofs": int(n),
+                           "nnz": int(levels[0]["matrix"].used_elements()), "nnz_stored": int(info_lv[0][1]),
                            "levels": int(info_lv.shape[0]), "ordering": args.ordering, "precision": precision,
                            "cycle": args.cycle, "parallelism": f"replicas x{world}", "l2": L2Flush.DESC,
                            "iterations": int(np.median(iters))},
                 "spmv_gbs": spmv_gbs, "rel_residual": rel_res, "breakdown": breakdown,
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": MEASURED_TRAFFIC.get((args.workload, args.ordering)),
-                             "traffic_source": "profiles/k_tma_pass_OpPcgQ_l10_f64.md (ncu dram__bytes_read.sum + "
-                                               "dram__bytes_write.sum of one launch)",
-                             "kernel": "k_tma_pass<OpPcgQ> (FP64 SpMV + q.p, TMA-staged; diagonal storage "
-                                       "for native order, sliced ELL for rcm)",
-                             "peak_source": f"{peak_kind} hbm_gbs", "bytes_per_launch": alg_k,
-                             "bytes_definition": "CSR: nnz*(8+4) + (n+1)*4 + n*8 (gathered p) + n*8 (q written)",
-                             "stored_bytes_per_launch": by_k, "launch_ms": ms_k,
-                             "traffic_frac": (MEASURED_TRAFFIC[(args.workload, args.ordering)] / (ms_k * 1e-3) / 1e9 / peak
-                                              if (args.workload, args.ordering) in MEASURED_TRAFFIC else None)},
+                "roofline": {"bound": "hbm", "kernel": dom, "kernel_name": dp["kernel"],
+                             "achieved": dp["csr_gbs"], "peak": peak, "unit": "GB/s",
+                             "frac": dp["csr_gbs"] / peak, "traffic": traffic,
+                             "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of this "
+                                                "kernel at this workload, same kernel source" if traffic else None),
+                             "traffic_frac": (traffic / (dp["us"] * 1e-6) / 1e9 / peak if traffic else None),
+                             "peak_source": f"{peak_kind} hbm_gbs", "launch_us": dp["us"],
+                             "bytes_per_launch": dp["csr_bytes"], "bytes_definition": dp["csr_definition"],
+                             "stored_bytes_per_launch": dp["stored_bytes"],
+                             "stored_frac": dp["stored_gbs"] / peak},
+                "passes": passes, "whole_solve": whole_solve,
                 "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(2 * 8 * n),
                         "d2h_bytes_per_step": int(8 * n)},
                 "gpu_launches": int(launches), "clocks": clk}
         line.update(extra)
+        if target is not None:
+            line["target"] = target
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))

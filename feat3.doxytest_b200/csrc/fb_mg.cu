@@ -2994,11 +2994,85 @@ namespace fb
       else
         k_pcg_q<<<blocks(t.n), NT, A64.smem, st>>>(view<double>(A64), s->p, s->q, t.dm, s->slot, s->sc);
     }
-    else if(l.use_tma(t.A))
-      l.template tma<V, S>(t.A, t.x, OpDefect<V, S>{(const S*)t.b, (S*)t.d, t.dm, s->sc});
-    else
-      k_defect<V, S><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.b, (const S*)t.x, (S*)t.d, t.dm,
-        s->sc);
+    else if(which == FB_KERNEL_MG_DEFECT)
+    {
+      if(l.use_tma(t.A))
+        l.template tma<V, S>(t.A, t.x, OpDefect<V, S>{(const S*)t.b, (S*)t.d, t.dm, s->sc});
+      else
+        k_defect<V, S><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.b, (const S*)t.x, (S*)t.d, t.dm,
+          s->sc);
+    }
+    else if(which == FB_KERNEL_MG_SMOOTH)
+    {
+      if(l.use_tma(t.A))
+        l.template tma<V, S>(t.A, t.x, OpSmooth<V, S>{(const S*)t.b, (const S*)t.x, (S*)t.x2, (const S*)t.dinv, t.dm,
+          t.skip_pre, s->sc});
+      else
+        k_smooth<V, S><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.b, (const S*)t.x, (S*)t.x2,
+          (const S*)t.dinv, t.dm, t.skip_pre, s->sc);
+    }
+    else if(which == FB_KERNEL_MG_POST1)
+    {
+      if(l.use_tma(t.A))
+        l.template tma<V, S>(t.A, t.x, OpPost1<V, S>{(const S*)t.b, (S*)t.d, (S*)t.c, (const S*)t.dinv, t.dm,
+          t.skip_post, s->sc});
+      else
+        k_post1<V, S><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.b, (const S*)t.x, (S*)t.d, (S*)t.c,
+          (const S*)t.dinv, t.dm, t.skip_post, s->slot, s->sc);
+    }
+    else if(which == FB_KERNEL_MG_POST2)
+    {
+      // the finest level's last post-smoothing step as the solve runs it: it also forms z and r.z
+      if(l.use_tma(t.A))
+        l.template tma<V, S>(t.A, t.c, OpPost2<V, S, true, true>{(const S*)t.d, (const S*)t.c, (S*)t.c2, (S*)t.x, s->z,
+          s->r, (const S*)t.dinv, t.dm, t.skip_post, s->sc});
+      else
+        k_post2<V, S, true, true><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.d, (const S*)t.c,
+          (S*)t.c2, (S*)t.x, s->z, s->r, (const S*)t.dinv, t.dm, t.skip_post, s->slot, s->sc);
+    }
+    else if(which == FB_KERNEL_MG_RESTRICT)
+      l.restrict_to(0);
+    else if(which == FB_KERNEL_MG_PROLONG)
+    {
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      xcur[0] = t.x;
+      xcur[1] = s->lv[1].x;
+      l.prolong(0, xcur);
+    }
+  }
+
+  // algorithmic bytes of one launch of kernel `which` as stored on the device: the matrix as stored,
+  // the gathered vector, the row-wise vectors read and written and the Dirichlet mask (the same
+  // count the solve's bytes_moved uses); 0 for the multi-pass entries
+  template<typename V, typename S>
+  static double stored_bytes_one(const fb_solver* s, int which)
+  {
+    const DevLevel& t = s->lv[0];
+    const double n = double(t.n), sx = double(sizeof(S));
+    auto csr = [&](const DevMat& m, double vin, double vout)
+    {
+      return m.bytes + double(m.cols) * sx + double(m.rows) * sx * (vin + vout);
+    };
+    switch(which)
+    {
+      case FB_KERNEL_PCG_SPMV:
+      {
+        const DevMat& A64 = s->cfg.precision == FB_PREC_F64 ? t.A : t.A64;
+        return A64.bytes + n * 8.0 * 2.0 + n;
+      }
+      case FB_KERNEL_MG_DEFECT: return csr(t.A, 1, 1) + n;
+      case FB_KERNEL_MG_SMOOTH: return csr(t.A, 3, 1) + n;
+      case FB_KERNEL_MG_POST1: return csr(t.A, 2, 2) + n;
+      case FB_KERNEL_MG_POST2: return csr(t.A, 3, 1) + n + 16.0 * n;
+      case FB_KERNEL_MG_RESTRICT:
+      {
+        const bool coarsest = s->nlev == 2;
+        const double nc = double(s->lv[1].n);
+        return t.R.bytes + double(t.R.cols) * sx + nc * sx * (coarsest ? 1.0 : 3.0) + nc;
+      }
+      case FB_KERNEL_MG_PROLONG: return csr(t.P, 1, 1) + n;
+      default: return 0.0;
+    }
   }
 } // namespace fb
 
@@ -3007,8 +3081,10 @@ extern "C" {
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
   double* bytes_per_launch)
 {
-  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_CYCLE ||
-     (which == FB_KERNEL_MG_TAIL && s->tail_first < 0 && s->ctail_first < 0))
+  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_PROLONG ||
+     (which == FB_KERNEL_MG_TAIL && s->tail_first < 0 && s->ctail_first < 0) ||
+     (which >= FB_KERNEL_MG_SMOOTH && s->nlev < 2) ||
+     (which >= FB_KERNEL_MG_SMOOTH && (s->tail_first == 0 || s->ctail_first == 0)))
   {
     set_error("solver_time_kernel: bad arguments");
     return FB_ERR_ARG;
@@ -3025,14 +3101,14 @@ fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2,
     FB_TRY(dalloc(s, &s->flush, 2 * flush_bytes + 256));
     FB_CUDA(cudaMemsetAsync(s->flush, 0, 2 * flush_bytes + 256, st));
   }
-  const DevMat& A64 = f64 ? t.A : t.A64;
-  const double sv = double(vsize_of(s->cfg.precision));
-  if(which == FB_KERNEL_PCG_SPMV)
-    *bytes_per_launch = A64.bytes + double(t.n) * 8.0 * 2.0 + double(t.n);
-  else if(which == FB_KERNEL_MG_DEFECT)
-    *bytes_per_launch = t.A.bytes + double(t.n) * sv * 3.0 + double(t.n);
+  (void)t;
+  (void)f64;
+  if(s->cfg.precision == FB_PREC_F64)
+    *bytes_per_launch = stored_bytes_one<double, double>(s, which);
+  else if(s->cfg.precision == FB_PREC_F32)
+    *bytes_per_launch = stored_bytes_one<float, float>(s, which);
   else
-    *bytes_per_launch = 0.0;   // several passes: no single figure
+    *bytes_per_launch = stored_bytes_one<bf16_t, float>(s, which);
   k_set_status<<<1, 1, 0, st>>>(s->sc, FB_SOLVER_PROGRESS);
   FB_LAUNCHED(1);
   double total = 0.0;

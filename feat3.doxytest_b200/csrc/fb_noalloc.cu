@@ -4,18 +4,22 @@
 // whole device memory to their own pool allocator at start-up (MPI codes with a fixed per-rank
 // memory budget work this way), and loops that must not stall, since cudaMalloc and cudaFree can
 // synchronise the device.  fb_dot_f64 allocates its reduction scratch on first use; this variant
-// keeps its scratch in a fixed array of this file instead, allocated when the library is loaded.
+// keeps its scratch in a fixed array of this file instead.
 //
-// The scratch is a file-scope __device__ array: every GPU that loads the library holds it
+// The scratch is a file-scope __device__ array: every GPU that loads this file's module holds it
 // (NOALLOC_MAX_BLOCKS = 4096 partial sums, 32 KiB, plus a counter and the result) until the process
-// exits.  Each block of the kernel reduces NOALLOC_CHUNK = 4096 consecutive elements, so the largest
+// exits.  Under CUDA's lazy module loading (the default) the module, and with it the array, is
+// loaded by the first use on a device, and that load itself takes device memory.  A caller that
+// hands all device memory to its own pool should therefore make one set-up call per device before
+// its pool takes the memory: fb_dot_f64_noalloc with n = 0 (x and y may then be null) loads the
+// module and the kernel on the current device, resolves the array's address and launches nothing.
+// Each block of the kernel reduces NOALLOC_CHUNK = 4096 consecutive elements, so the largest
 // accepted vector has 4096 * 4096 = 16,777,216 elements (FB_DOT_NOALLOC_MAX_N); longer vectors are
 // rejected with FB_ERR_ARG.  All calls share the one array and it keeps the last
 // call's contents: the arrival counter is cleared at the start of every call, and calls that
 // overlap on the GPU (concurrent streams, several host threads) race on the array.
 #include "fb_common.cuh"
 
-#include <mutex>
 #include <string>
 
 namespace fb
@@ -55,31 +59,22 @@ namespace fb
       sc->result = total;
   }
 
-  // Device address of the scratch array on the current device, looked up by the first call on
-  // each device (with that device current) and kept in a fixed table.
-  constexpr int NOALLOC_MAX_DEVICES = 64;
-
+  // Device address of the scratch array in the current context, with that context's device
+  // current.  The address is looked up on every call rather than cached per device ordinal: after
+  // cudaDeviceReset, or under a context other than the primary one, a cached address would be
+  // stale.  Once the module is loaded the lookup allocates nothing.  The kernel's attributes are
+  // queried as well, so that under lazy loading the kernel is loaded here, not at its first launch.
   static fb_status noalloc_scratch_ptr(NoallocScratch*& out)
   {
-    static std::mutex mu;
-    static NoallocScratch* per_dev[NOALLOC_MAX_DEVICES] = {};
-    int dev = 0;
-    FB_CUDA(cudaGetDevice(&dev));
-    if(dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-    {
-      set_error("dot_noalloc: device ordinal out of range");
-      return FB_ERR_ARG;
-    }
-    std::lock_guard<std::mutex> lock(mu);
-    if(!per_dev[dev])
-    {
-      void* p = nullptr;
-      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-      if(e != cudaSuccess)
-        return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-      per_dev[dev] = static_cast<NoallocScratch*>(p);
-    }
-    out = per_dev[dev];
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if(e != cudaSuccess)
+      return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, k_dot_noalloc);
+    if(e != cudaSuccess)
+      return cuda_fail(e, "cudaFuncGetAttributes(k_dot_noalloc)");
+    out = static_cast<NoallocScratch*>(p);
     return FB_OK;
   }
 } // namespace fb
@@ -99,20 +94,22 @@ extern "C" fb_status fb_dot_f64_noalloc(double* result, const double* x, const d
               " elements of the fixed scratch array (use fb_dot_f64)");
     return FB_ERR_ARG;
   }
+  if(n != 0 && (!x || !y))
+  {
+    set_error("dot_noalloc: null pointer");
+    return FB_ERR_ARG;
+  }
+  // set-up on the current device (module and kernel loaded, array address resolved); n = 0 stops
+  // here, which is the set-up call for callers whose pool takes the device memory afterwards
+  NoallocScratch* sc = nullptr;
+  fb_status e = noalloc_scratch_ptr(sc);
+  if(e != FB_OK)
+    return e;
   if(n == 0)
   {
     *result = 0.0;
     return FB_OK;
   }
-  if(!x || !y)
-  {
-    set_error("dot_noalloc: null pointer");
-    return FB_ERR_ARG;
-  }
-  NoallocScratch* sc = nullptr;
-  fb_status e = noalloc_scratch_ptr(sc);
-  if(e != FB_OK)
-    return e;
   cudaStream_t st = as_stream(stream);
   // the array keeps the last call's contents: the arrival counter must start at zero
   FB_CUDA(cudaMemsetAsync(&sc->counter, 0, sizeof(unsigned int), st));

@@ -244,3 +244,40 @@ def poisson_hierarchy(level, dim=2, level_min=1, rhs="sine", gauss=None, field=N
 
 def vertex_coords(level, dim=2):
     return _vertex_coords(level, dim)
+
+
+# ------------------------------------------------------------------------------ named workload families
+def batch_family_levels(count=256, seed=7):
+    """Levels of the uneven-instance batch: `count` draws uniform in 5..9 (seeded PCG64)."""
+    return [int(v) for v in np.random.default_rng(seed).integers(5, 10, size=count)]
+
+
+def batch_instance_params(k):
+    """(Gaussian right-hand side, kappa field) of instance k of the uneven-instance batch."""
+    return gauss_params(10_000 + 2 * k, 2), field_params(10_001 + 2 * k)
+
+
+def batch_instance(level, k):
+    """Instance k of the uneven-instance batch at `level`: -div(kappa grad u) = f with
+    kappa = exp(16x16-mode random field) and an 8-Gaussian f; (levels, filtered rhs)."""
+    g, f = batch_instance_params(k)
+    return poisson_hierarchy(level, 2, rhs="gauss", gauss=g, field=f)
+
+
+def rhs64_params(j, dim=3):
+    """Gaussian right-hand side j (0..63) of the many-right-hand-side 3D set (seeds 100..163)."""
+    return gauss_params(100 + j, dim, width=(0.03, 0.12) if dim == 3 else (0.02, 0.1))
+
+
+def rhs64_family(level=6, dim=3, k=64):
+    """The many-right-hand-side set: the Q1 Poisson hierarchy at `level` and a [rows, k] array of
+    filtered 8-Gaussian load vectors (column j from rhs64_params(j))."""
+    levels, _ = poisson_hierarchy(level, dim, rhs="sine")
+    fidx = levels[0]["filter"].indices.astype(np.int64)
+    B = np.zeros((levels[0]["matrix"].rows(), k))
+    for j in range(k):
+        g = rhs64_params(j, dim)
+        b = load_vector(level, lambda *xs: gauss_eval(g, *xs), dim)
+        b[fidx] = 0.0
+        B[:, j] = b
+    return levels, B

@@ -372,9 +372,11 @@ class PCG:
         return Status(self.info.status)
 
     def time_kernel(self, which="pcg_spmv", reps=20, flush_l2=True):
-        """Mean launch time (ms) and algorithmic bytes of one solver kernel timed alone: pcg_spmv,
-        mg_defect, mg_tail (the coarse-level tail kernel) or mg_cycle (one whole multigrid cycle)."""
-        code = {"pcg_spmv": 0, "mg_defect": 1, "mg_tail": 2, "mg_cycle": 3}[which]
+        """Mean launch time (ms) and stored bytes per launch of one solver kernel timed alone:
+        pcg_spmv, mg_defect, mg_smooth, mg_post1, mg_post2, mg_restrict, mg_prolong (finest-level
+        passes), mg_tail (the coarse-level tail kernel) or mg_cycle (one whole multigrid cycle)."""
+        code = {"pcg_spmv": 0, "mg_defect": 1, "mg_tail": 2, "mg_cycle": 3, "mg_smooth": 4, "mg_post1": 5,
+                "mg_post2": 6, "mg_restrict": 7, "mg_prolong": 8}[which]
         ms, by = C.c_double(), C.c_double()
         _lib.check(_lib.lib().fb_solver_time_kernel(self._s, code, int(reps), 1 if flush_l2 else 0, C.byref(ms),
                                                      C.byref(by)), "fb_solver_time_kernel")

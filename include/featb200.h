@@ -93,9 +93,12 @@ fb_status fb_dot_f32(float* result, const float* x, const float* y, uint64_t n, 
  * own pool allocator at start-up, and loops that must not stall on cudaMalloc/cudaFree, which can
  * synchronise the device.  Its scratch is a fixed 32 KiB array in the library's device image, held
  * by every GPU that loads the library; n may be at most FB_DOT_NOALLOC_MAX_N (longer vectors are
- * rejected with FB_ERR_ARG).  The first call on a device looks up the array's device address (with
- * that device current).  All calls share the array: calls that overlap on the GPU race.
- * No counterpart in the reference: an addition of this library. */
+ * rejected with FB_ERR_ARG).  Every call looks up the array's device address in the current
+ * context.  Under CUDA's lazy module loading the first call on a device loads the library's module,
+ * which takes device memory: call it once per device with n = 0 (x and y may be null; nothing is
+ * launched) before a pool takes the device memory, and before any stream capture.  All calls share
+ * the array and it keeps the last call's contents: calls that overlap on the GPU (several streams or
+ * host threads) race.  No counterpart in the reference: an addition of this library. */
 #define FB_DOT_NOALLOC_MAX_N 16777216ull
 fb_status fb_dot_f64_noalloc(double* result, const double* x, const double* y, uint64_t n, void* stream);
 
@@ -266,13 +269,19 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
 #define FB_KERNEL_MG_DEFECT 1  /* d = F(b - A x), finest level, in the V-cycle's precision */
 #define FB_KERNEL_MG_TAIL 2    /* the coarse-level tail kernel (one launch; needs a tail level) */
 #define FB_KERNEL_MG_CYCLE 3   /* one whole multigrid cycle from the finest level (all its launches) */
+#define FB_KERNEL_MG_SMOOTH 4  /* pre-smoothing step 2 x' = x + F(D F(b - A x)), finest level */
+#define FB_KERNEL_MG_POST1 5   /* post-smoothing step 1: d = F(b - A x), c = F(D d), ||d||, finest level */
+#define FB_KERNEL_MG_POST2 6   /* post-smoothing step 2 with the PCG's z = x + c' and r.z, finest level */
+#define FB_KERNEL_MG_RESTRICT 7 /* restriction b_c = F(R d) with sol1_c = F(D_c b_c), finest to next level */
+#define FB_KERNEL_MG_PROLONG 8 /* prolongation x += F(P x_c), next level to finest */
 
 /* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
- * on that stream; with flush_l2 != 0 a 256 MiB buffer is overwritten and another 256 MiB buffer read
+ * on that stream (the finest level's pass kernels need a finest level above the coarse-level tail);
+ * with flush_l2 != 0 a 256 MiB buffer is overwritten and another 256 MiB buffer read
  * before each launch (outside the timed interval), so every launch starts with an L2 that holds
  * none of its data and no dirty lines.  Returns the mean launch time and the
- * kernel's algorithmic bytes per launch (matrix values + indices + row pointers + vector reads and
- * writes).  No counterpart in the reference: a measurement aid for the SpMV roofline. */
+ * kernel's bytes per launch as stored on the device (matrix as stored + gathered vector + row-wise
+ * vector reads and writes + Dirichlet mask; 0 for the tail and the whole cycle).  No counterpart in the reference: a measurement aid for the SpMV roofline. */
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
                                 double* bytes_per_launch);
 

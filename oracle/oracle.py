@@ -23,6 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIB_PATH = os.path.join(REF_DIR, "libmgoracle.so")
 FEAT_BIN = os.path.join(REF_DIR, "feat_oracle")
+# the reference source tree the reference binary is compiled from (only where it exists)
+REF_SRC = os.environ.get("FEAT_REF", "/root/reference")
 
 STATUS = {0: "progress", 1: "success", 2: "aborted", 3: "diverged", 4: "max_iter"}
 
@@ -40,9 +42,9 @@ class _LevelIn(C.Structure):
 def build():
     """Compile the C restatement (and the reference driver when the reference tree exists)."""
     targets = ["port"]
-    if os.path.isdir("/root/reference"):
+    if os.path.isdir(REF_SRC):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"FEAT_REF={REF_SRC}"] + targets, check=True)
 
 
 _lib = None

@@ -12,6 +12,20 @@ CASES_3D = ["c3d_L3", "gauss3d_L3"]
 CASES = CASES_2D + CASES_3D
 
 
+def require_reference_binary():
+    """Skip the calling test when the reference binary (oracle/_ref/feat_oracle, built from the
+    reference's sources by oracle/Makefile) is absent; with FEATB200_REQUIRE_REF=1 in the
+    environment its absence fails the test instead, so a run that expects the binary cannot pass on
+    skipped pins."""
+    import pytest
+    import oracle as O
+    if O.feat_available():
+        return
+    if os.environ.get("FEATB200_REQUIRE_REF") == "1":
+        pytest.fail("reference binary oracle/_ref/feat_oracle not built (FEATB200_REQUIRE_REF=1)")
+    pytest.skip("reference binary oracle/_ref/feat_oracle not built")
+
+
 def load_golden(name):
     """A golden fixture as a dict: levels (finest first), rhs, sol, vcycle, iterates, defects, summary."""
     import oracle as O

@@ -7,14 +7,15 @@ import sys
 
 import pytest
 
+from helpers import require_reference_binary
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def test_reference_arm_json_line():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    if not O.feat_available():
-        pytest.skip("reference binary oracle/_ref/feat_oracle not built")
+    require_reference_binary()
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                           "--warmup", "3", "--workload", "poisson2d_l7_fp64"], capture_output=True, text=True,
                          timeout=600, cwd=ROOT)

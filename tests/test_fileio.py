@@ -7,6 +7,8 @@ import os
 import numpy as np
 import pytest
 
+from helpers import require_reference_binary
+
 from featb200 import assembly as AS
 from featb200 import fileio
 from featb200.lafem import DenseVector, SparseMatrixCSR
@@ -35,8 +37,7 @@ def test_binary_roundtrip_here(tmp_path):
 
 def test_reference_reads_and_rewrites_identically(tmp_path, oracle_lib):
     O = oracle_lib
-    if not O.feat_available():
-        pytest.skip("reference binary oracle/_ref/feat_oracle not built")
+    require_reference_binary()
     A = _matrix()
     v = DenseVector(np.random.default_rng(1).standard_normal(A.rows()))
     p, q = str(tmp_path / "a.csr"), str(tmp_path / "v.dv")

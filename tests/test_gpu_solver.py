@@ -10,7 +10,7 @@ import tempfile
 import numpy as np
 import pytest
 
-from helpers import CASES, load_golden, rel_err, to_lafem_levels, to_oracle_levels
+from helpers import CASES, load_golden, rel_err, to_lafem_levels, to_oracle_levels, require_reference_binary
 
 pytestmark = pytest.mark.gpu
 
@@ -53,8 +53,7 @@ def test_fp64_matches_reference(featlib, cuda, name, ordering, graph, tail, clus
 
 def _live_reference(tmp, level, dim=2, **kw):
     import oracle as O
-    if not O.feat_available():
-        pytest.skip("reference binary oracle/_ref/feat_oracle not built")
+    require_reference_binary()
     summ = O.feat_solve(tmp, dim=dim, level=level, dump_levels=True, vcycle=True, iterates=2, **kw)
     levels = O.load_dump(tmp, level)
     return summ, levels
@@ -318,9 +317,9 @@ def test_diagonal_storage_3d_against_oracle(featlib, cuda, oracle_lib, graph):
 
 
 @pytest.mark.parametrize("cycle", ["F", "W"])
-@pytest.mark.parametrize("cgc", ["fixed", "energy"])
+@pytest.mark.parametrize("cgc", ["fixed", "energy", "defect"])
 def test_cycles_diagonal_storage_against_oracle(featlib, cuda, oracle_lib, cycle, cgc):
-    """F and W cycles, fixed and adaptive coarse-grid correction, on a lexicographically numbered
+    """F and W cycles, fixed and both adaptive coarse-grid corrections, on a lexicographically numbered
     problem (diagonal storage) against the C restatement: bitwise with the fixed correction, to
     1e-12 with the adaptive one (its step length sums dot products in another order)."""
     from featb200 import assembly as AS
@@ -329,7 +328,7 @@ def test_cycles_diagonal_storage_against_oracle(featlib, cuda, oracle_lib, cycle
     mg = oracle_lib.MultigridPCG(to_oracle_levels(levels), 0.7, 2, cycle=cycle, cgc=cgc)
     x_ref, info = mg.solve(b)
     z_ref = mg.vcycle(b)
-    mode = {"fixed": "Fixed", "energy": "MinEnergy"}[cgc]
+    mode = {"fixed": "Fixed", "energy": "MinEnergy", "defect": "MinDefect"}[cgc]
     s, x, st = _solve(fb, levels, b, cycle=cycle, adapt_cgc=mode, tma_rows=64)
     z = s.apply_precond(fb.DenseVector(b)).elements
     if cgc == "fixed":

@@ -20,6 +20,10 @@ def _dot(lib, name, xd, yd, n):
 def test_dot_noalloc_matches_dot(featlib, cuda):
     torch = cuda
     lib = featlib.lib()
+    # the set-up call a caller makes before its pool takes the device memory: n = 0, null vectors
+    out = C.c_double(1.0)
+    assert lib.fb_dot_f64_noalloc(C.byref(out), None, None, 0, None) == 0, lib.fb_last_error()
+    assert out.value == 0.0
     rng = np.random.default_rng(7)
     for n in (1, 4095, 4096, 4097, 1_000_003):
         x = rng.standard_normal(n)
