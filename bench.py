@@ -284,7 +284,7 @@ def run_multi(args, kind):
     the whole set).  With N ranks the batch's instances are sharded by a longest-processing-time
     assignment on DOF count (no collective on the data path; total work fixed: strong scaling);
     the 64-RHS set is solved as a replica on every rank (weak scaling)."""
-    pre = build_batch_problem() if kind == "batch" else None
+    pre = build_batch_problem(args.batch_count) if kind == "batch" else None
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -303,12 +303,13 @@ def run_multi(args, kind):
         mine = sharding.shard([b.size for _, b in inst], rank, world)
         inst = [inst[i] for i in mine]
         hs = [fb.build_hierarchy(lv) for lv, _ in inst]
-        solver = fb.BatchPCG(hs, precision=precision, ordering=args.ordering)
+        solver = fb.BatchPCG(hs, precision=precision, ordering=args.ordering, use_graph=not args.profile_solves)
         rhs = np.concatenate([b for _, b in inst])
         units, dofs = len(inst), int(rhs.size)
     else:
         lv, B = build_rhs64_problem()
-        solver = fb.MultiRhsPCG(fb.build_hierarchy(lv), 64, precision=precision, ordering=args.ordering)
+        solver = fb.MultiRhsPCG(fb.build_hierarchy(lv), 64, precision=precision, ordering=args.ordering,
+                                use_graph=not args.profile_solves)
         rhs = B.ravel()
         units, dofs = 64, int(B.shape[0])
     stream = torch.cuda.current_stream()
@@ -319,6 +320,13 @@ def run_multi(args, kind):
         sol_d.zero_()
         solver.solve_device(sol_d, rhs_d, stream)
     torch.cuda.synchronize()
+    if args.profile_solves:
+        for _ in range(args.profile_solves):
+            sol_d.zero_()
+            solver.solve_device(sol_d, rhs_d, stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_solves": args.profile_solves, "iterations_max": int(max(solver.iterations()))}))
+        return 0
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
@@ -596,6 +604,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
+    ap.add_argument("--profile-kernel", default=None, choices=sorted(PASS_KERNELS),
+                    help="only launch this finest-level pass a few times alone (for a profiler), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
     ap.add_argument("--tma-rows", type=int, default=None,
                     help="levels with at least this many rows use the TMA-staged passes")
@@ -617,6 +627,7 @@ def main():
     ap.add_argument("--no-target", action="store_true",
                     help="skip the plain-FP64 vs batched-mixed comparison on the uneven-instance family")
     ap.add_argument("--target-count", type=int, default=256, help="instances of that comparison")
+    ap.add_argument("--batch-count", type=int, default=256, help="instances of the batch workload")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -630,7 +641,8 @@ def main():
     # the target comparison's instances are assembled on host worker processes while the main
     # workload's problem is assembled (single-GPU runs of the default workload only)
     started = None
-    if not args.no_target and not args.profile_solves and dist_env()[1] == 1 and args.workload == DEFAULT_WORKLOAD:
+    if (not args.no_target and not args.profile_solves and not args.profile_kernel and dist_env()[1] == 1
+            and args.workload == DEFAULT_WORKLOAD):
         started = start_batch_build(args.target_count)
 
     import torch
@@ -655,6 +667,10 @@ def main():
                                     cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle,
                                     diagonal=args.diagonal, pdl=args.pdl)
     info_lv = solver.level_info()
+    if args.profile_kernel:
+        ms_k, by_k = solver.time_kernel(args.profile_kernel, reps=3, flush_l2=True)
+        print(json.dumps({"profile_kernel": args.profile_kernel, "us": ms_k * 1e3, "stored_bytes": by_k}))
+        return 0
 
     stream = torch.cuda.current_stream()
     rhs_d = torch.tensor(b, device="cuda")

@@ -173,6 +173,24 @@ namespace fb
       r[i] = mul(x[i], s);
   }
 
+  template<typename DT>
+  __global__ void k_set_memory(DT* r, DT v, uint64_t n)
+  {
+    for(uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+      r[i] = v;
+  }
+  // one thread per row: every entry of the row scaled by the row's factor
+  template<typename DT, typename IT>
+  __global__ void k_scale_rows(DT* r, const DT* a, const IT* rp, const DT* x, uint64_t rows)
+  {
+    for(uint64_t row = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; row < rows; row += uint64_t(gridDim.x) * blockDim.x)
+    {
+      const DT s = x[row];
+      for(uint64_t k = uint64_t(rp[row]); k < uint64_t(rp[row + 1]); ++k)
+        r[k] = mul(a[k], s);
+    }
+  }
+
   // Dot products reduce in FP64 per thread (grid-stride), per block, then in the last block over
   // the block partials in block order: deterministic for a given launch shape.
   constexpr int RED_NT = 256;
@@ -426,6 +444,34 @@ fb_status fb_diagonal_csr_u64(uint64_t* diag, const uint64_t* col_ind, const uin
 {
   if(rows && (!diag || !col_ind || !row_ptr)) { set_error("diagonal: null pointer"); return FB_ERR_ARG; }
   FB_ELEMENTWISE(k_diagonal<uint64_t>, rows, diag, col_ind, row_ptr, rows);
+}
+
+fb_status fb_set_memory_f64(double* r, double value, uint64_t n, void* stream)
+{
+  if(n && !r) { set_error("set_memory: null pointer"); return FB_ERR_ARG; }
+  FB_ELEMENTWISE(k_set_memory<double>, n, r, value, n);
+}
+fb_status fb_set_memory_f32(float* r, float value, uint64_t n, void* stream)
+{
+  if(n && !r) { set_error("set_memory: null pointer"); return FB_ERR_ARG; }
+  FB_ELEMENTWISE(k_set_memory<float>, n, r, value, n);
+}
+fb_status fb_set_memory_u64(uint64_t* r, uint64_t value, uint64_t n, void* stream)
+{
+  if(n && !r) { set_error("set_memory: null pointer"); return FB_ERR_ARG; }
+  FB_ELEMENTWISE(k_set_memory<uint64_t>, n, r, value, n);
+}
+fb_status fb_set_memory_u32(uint32_t* r, uint32_t value, uint64_t n, void* stream)
+{
+  if(n && !r) { set_error("set_memory: null pointer"); return FB_ERR_ARG; }
+  FB_ELEMENTWISE(k_set_memory<uint32_t>, n, r, value, n);
+}
+
+fb_status fb_scale_rows_csr_f64_u64(double* r, const double* val, const uint64_t* row_ptr, const double* x,
+                                    uint64_t rows, void* stream)
+{
+  if(rows && (!r || !val || !row_ptr || !x)) { set_error("scale_rows: null pointer"); return FB_ERR_ARG; }
+  FB_ELEMENTWISE((k_scale_rows<double, uint64_t>), rows, r, val, row_ptr, x, rows);
 }
 
 fb_status fb_convert_f64_to_f32(float* dst, const double* src, uint64_t n, void* stream)

@@ -1601,6 +1601,7 @@ struct fb_solver
   uint8_t* tail_prog = nullptr;             // tail kernel programs: events op << 4 | tail level
   std::vector<uint32_t> seg_off, seg_len;   // program of each tail segment of `events`, in order
   double* cgc_omega = nullptr;   // step length of the adaptive coarse-grid correction
+  int max_iter_cap = 0;   // max_iter at creation: the defect history holds max_iter + 2 entries
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
   double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
@@ -2753,6 +2754,7 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   h0.div_abs = 1.0 / (EPS64 * EPS64);
   h0.min_iter = cfg.min_iter;
   h0.max_iter = cfg.max_iter;
+  s->max_iter_cap = cfg.max_iter;
   h0.mg_scale = 1.0;
   h0.mg_inv_scale = 1.0;
   FB_CUDA(cudaMemcpy(s->sc, &h0, sizeof(h0), cudaMemcpyHostToDevice));
@@ -3342,6 +3344,23 @@ fb_status fb_solver_set_tolerances(fb_solver* s, double tol_rel, double tol_abs)
   const double t[2] = {tol_rel, tol_abs};
   static_assert(offsetof(Scalars, tol_abs) == offsetof(Scalars, tol_rel) + sizeof(double), "Scalars layout");
   FB_CUDA(cudaMemcpy(reinterpret_cast<char*>(s->sc) + offsetof(Scalars, tol_rel), t, sizeof(t),
+                     cudaMemcpyHostToDevice));
+  return FB_OK;
+}
+
+fb_status fb_solver_set_iteration_limits(fb_solver* s, int min_iter, int max_iter)
+{
+  if(!s || min_iter < 0 || max_iter < 0 || max_iter > s->max_iter_cap)
+  {
+    set_error("solver_set_iteration_limits: bad arguments (max_iter may not exceed the value the solver was created with)");
+    return FB_ERR_ARG;
+  }
+  FB_CUDA(cudaStreamSynchronize(s->stream));
+  s->cfg.min_iter = min_iter;
+  s->cfg.max_iter = max_iter;
+  const int t[2] = {min_iter, max_iter};
+  static_assert(offsetof(Scalars, max_iter) == offsetof(Scalars, min_iter) + sizeof(int), "Scalars layout");
+  FB_CUDA(cudaMemcpy(reinterpret_cast<char*>(s->sc) + offsetof(Scalars, min_iter), t, sizeof(t),
                      cudaMemcpyHostToDevice));
   return FB_OK;
 }

@@ -68,6 +68,12 @@ _PROTOS = {
     "fb_dot_f64": (I, [P, P, P, U64, P]),
     "fb_dot_f32": (I, [P, P, P, U64, P]),
     "fb_dot_f64_noalloc": (I, [P, P, P, U64, P]),
+    "fb_solver_set_iteration_limits": (I, [P, I, I]),
+    "fb_set_memory_f64": (I, [P, D, U64, P]),
+    "fb_set_memory_f32": (I, [P, F, U64, P]),
+    "fb_set_memory_u64": (I, [P, U64, U64, P]),
+    "fb_set_memory_u32": (I, [P, C.c_uint32, U64, P]),
+    "fb_scale_rows_csr_f64_u64": (I, [P, P, P, P, U64, P]),
     "fb_norm2_f64": (I, [P, P, U64, P]),
     "fb_norm2_f32": (I, [P, P, U64, P]),
     "fb_component_product_f64": (I, [P, P, P, U64, P]),

@@ -131,6 +131,18 @@ fb_status fb_unit_filter_def_f32_u32(float* v, const uint32_t* idx, uint64_t ue,
 fb_status fb_diagonal_csr_u64(uint64_t* diag, const uint64_t* col_ind, const uint64_t* row_ptr,
                               uint64_t rows, void* stream);
 
+/* r_i = value for i < n.  Replaces Util::cuda_set_memory (cuda_util.cu:202-219), which
+ * MemoryPool::set_memory calls for the cuda backend (memory_pool.hpp:179-199). */
+fb_status fb_set_memory_f64(double* r, double value, uint64_t n, void* stream);
+fb_status fb_set_memory_f32(float* r, float value, uint64_t n, void* stream);
+fb_status fb_set_memory_u64(uint64_t* r, uint64_t value, uint64_t n, void* stream);
+fb_status fb_set_memory_u32(uint32_t* r, uint32_t value, uint64_t n, void* stream);
+
+/* r[k] = val[k] * x[row] for every entry k of every row (r may alias val).  Replaces
+ * Arch::ScaleRows::csr (scale_row_col.hpp, generic semantics scale_row_col_generic.hpp:19-31). */
+fb_status fb_scale_rows_csr_f64_u64(double* r, const double* val, const uint64_t* row_ptr, const double* x,
+                                    uint64_t rows, void* stream);
+
 /* Precision conversion (MemoryPool::convert / Util::cuda_convert, cuda_util.cu:228-262). */
 fb_status fb_convert_f64_to_f32(float* dst, const double* src, uint64_t n, void* stream);
 fb_status fb_convert_f32_to_f64(double* dst, const float* src, uint64_t n, void* stream);
@@ -326,6 +338,11 @@ fb_status fb_multigrid_cycle_events(int cycle, int adapt_cgc, int num_levels, ui
 /* New stopping tolerances for the following solves (IterativeSolver::set_tol_rel/set_tol_abs,
  * kernel/solver/iterative.hpp): converged when ||d|| <= tol_abs and ||d|| <= tol_rel * ||d_0||. */
 fb_status fb_solver_set_tolerances(fb_solver* s, double tol_rel, double tol_abs);
+
+/* New iteration limits for the following solves (IterativeSolver::set_min_iter / set_max_iter,
+ * kernel/solver/iterative.hpp): max_iter may not exceed the max_iter of the configuration the
+ * solver was created with. */
+fb_status fb_solver_set_iteration_limits(fb_solver* s, int min_iter, int max_iter);
 
 /* New values for the system matrix of `level` (0 = finest): `values` is a DEVICE array of the
  * level's used_elements doubles in the pattern and entry order passed to fb_hierarchy_set_level

@@ -15,6 +15,14 @@
 // CoarseInverseSolver below; the reference offers no third-party-free direct solver).
 //
 // Usage:
+// Built a second time with -DFEAT_HAVE_CUDA -DFEATB200_BACKEND and the library's FEAT binding
+// (feat3.doxytest_b200/feat/featb200_backend.cpp in place of FEAT's CUDA backend, linked with
+// libfeatb200.so) into oracle/_ref/feat_b200: the same program, where FEAT's containers hold managed
+// memory and two more options exist:
+//   --backend b200   FEAT's own PCG + MultiGrid with every LAFEM op dispatched to the CUDA backend
+//                    (Backend::set_preferred_backend(PreferredBackend::cuda)), i.e. to the library
+//   --b200-solver    the whole solve handed to the library's solver object (featb200_solver.hpp)
+//
 //   feat_oracle fd M D DIR     (the reference's basic_solver-test problem, see run_fd)
 //   feat_oracle solve --dim D --level L --out DIR [--rhs sine|gauss] [--params FILE]
 //                     [--kappa FILE] [--omega W] [--steps S] [--tol T] [--iterates K]
@@ -53,6 +61,10 @@
 #include <kernel/solver/richardson.hpp>
 #include <kernel/solver/jacobi_precond.hpp>
 #include <kernel/solver/multigrid.hpp>
+#ifdef FEATB200_BACKEND
+#include <kernel/backend.hpp>
+#include <featb200_solver.hpp>
+#endif
 
 #include <algorithm>
 #include <chrono>
@@ -351,6 +363,8 @@ namespace Oracle
     bool dump_levels = false;
     bool dump = true;
     int time_reps = 0;
+    std::string backend = "generic";   // generic | b200 (FEATB200_BACKEND builds only)
+    bool b200_solver = false;          // FEATB200_BACKEND builds only
   };
 
   template<int dim_>
@@ -521,7 +535,19 @@ namespace Oracle
       multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinEnergy);
     else if(opt.cgc == "defect")
       multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinDefect);
+#ifdef FEATB200_BACKEND
+    // every LAFEM op from here on (smoother set-up, solve) goes to the CUDA backend = the library
+    if(opt.backend == "b200")
+      Backend::set_preferred_backend(PreferredBackend::cuda);
+    std::shared_ptr<Solver::IterativeSolver<VectorType>> solver;
+    if(opt.b200_solver)
+      solver = std::make_shared<FEATB200::MultiGridPCG<MatrixType, FilterType, TransferType>>(hierarchy,
+        double(opt.omega), int(opt.steps));
+    else
+      solver = Solver::new_pcg(top.matrix, top.filter, multigrid);
+#else
     auto solver = Solver::new_pcg(top.matrix, top.filter, multigrid);
+#endif
     solver->set_tol_rel(DataType(opt.tol));
     solver->set_max_iter(100);
     hierarchy->init();
@@ -557,7 +583,7 @@ namespace Oracle
     }
 
     // one V-cycle applied to the fine rhs
-    if(opt.vcycle && opt.dump)
+    if(opt.vcycle && opt.dump && !opt.b200_solver)
     {
       VectorType z = top.matrix.create_vector_r();
       multigrid->apply(z, vec_rhs);
@@ -622,10 +648,10 @@ namespace Oracle
 
     std::printf("{\"dim\": %d, \"level\": %lu, \"dofs\": %lu, \"nnz\": %lu, \"status\": \"%s\", \"iters\": %lu, "
       "\"def_init\": %.17g, \"def_final\": %.17g, \"setup_s\": %.3f, \"solve_ms_median\": %.6f, \"reps\": %zu, "
-      "\"times_ms\": %s}\n",
+      "\"times_ms\": %s, \"backend\": \"%s\", \"solver\": \"%s\"}\n",
       dim_, (unsigned long)opt.level, (unsigned long)top.matrix.rows(), (unsigned long)top.matrix.used_elements(),
       Solver::status_success(st) ? "success" : "failure", (unsigned long)iters, def_init, def_final, setup_s,
-      median, times.size(), times_json.c_str());
+      median, times.size(), times_json.c_str(), opt.backend.c_str(), opt.b200_solver ? "b200" : "feat");
     return 0;
   }
   // The reference's own solver test problem (kernel/solver/basic_solver-test.cpp:98-140): the
@@ -727,6 +753,10 @@ int main(int argc, char* argv[])
     else if(a == "--dump-levels") opt.dump_levels = true;
     else if(a == "--no-dump") opt.dump = false;
     else if(a == "--time") opt.time_reps = std::stoi(next());
+#ifdef FEATB200_BACKEND
+    else if(a == "--backend") opt.backend = next();
+    else if(a == "--b200-solver") opt.b200_solver = true;
+#endif
     else
     {
       std::fprintf(stderr, "unknown option %s\n", a.c_str());

@@ -23,6 +23,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIB_PATH = os.path.join(REF_DIR, "libmgoracle.so")
 FEAT_BIN = os.path.join(REF_DIR, "feat_oracle")
+# the same driver built as a FEAT CUDA build on the library's FEAT binding
+FEAT_B200_BIN = os.path.join(REF_DIR, "feat_b200")
 # the reference source tree the reference binary is compiled from (only where it exists)
 REF_SRC = os.environ.get("FEAT_REF", "/root/reference")
 
@@ -44,6 +46,9 @@ def build():
     targets = ["port"]
     if os.path.isdir(REF_SRC):
         targets.append("ref")
+        # the FEAT build on the library's binding links the built library
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "feat3.doxytest_b200", "featb200", "libfeatb200.so")):
+            targets.append("b200")
     subprocess.run(["make", "-s", "-C", HERE, f"FEAT_REF={REF_SRC}"] + targets, check=True)
 
 
@@ -186,11 +191,19 @@ def feat_available():
     return os.path.exists(FEAT_BIN)
 
 
+def feat_b200_available():
+    return os.path.exists(FEAT_B200_BIN)
+
+
 def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, omega=0.7, steps=2,
                tol=1e-8, iterates=0, vcycle=False, dump_levels=False, time_reps=0, dump=True,
-               level_min=1, timeout=3600, cycle="v", cgc="fixed"):
-    """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary."""
-    cmd = [FEAT_BIN, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
+               level_min=1, timeout=3600, cycle="v", cgc="fixed", b200=None):
+    """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary.
+    b200 = "ops" or "solver": the same program built as a FEAT CUDA build on the library's FEAT
+    binding (oracle/_ref/feat_b200), with every LAFEM op on the library ("ops") or the whole solve
+    handed to the library's solver object ("solver")."""
+    exe = FEAT_BIN if b200 is None else FEAT_B200_BIN
+    cmd = [exe, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
            "--out", out_dir, "--rhs", rhs, "--omega", repr(omega), "--steps", str(steps), "--tol",
            repr(tol), "--iterates", str(iterates), "--time", str(time_reps), "--cycle", cycle, "--cgc", cgc]
     if params:
@@ -203,6 +216,12 @@ def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, ome
         cmd.append("--dump-levels")
     if not dump:
         cmd.append("--no-dump")
+    if b200 == "ops":
+        cmd += ["--backend", "b200"]
+    elif b200 == "solver":
+        cmd.append("--b200-solver")
+    elif b200 is not None:
+        raise ValueError(b200)
     os.makedirs(out_dir, exist_ok=True)
     res = subprocess.run(cmd, check=True, capture_output=True, text=True, timeout=timeout)
     return json.loads(res.stdout.strip().splitlines()[-1])
