@@ -490,7 +490,10 @@ PASS_KERNELS = {
     "mg_prolong": "k_tma_pass<OpProlong>: x += F(P x_c)",
     "mg_post1": "k_tma_pass<OpPost1>: post-smoothing step 1 (defect, Jacobi correction, norm)",
     "mg_post2": "k_tma_pass<OpPost2>: post-smoothing step 2 with the PCG's z and r.z",
+    "mg_down": "k_fz_down: fused pre-smoothing step 2 + defect + restriction (structured 2D level)",
+    "mg_up": "k_fz_up: fused prolongation + post-smoothing with the PCG's z and r.z (structured 2D level)",
 }
+FUSED_PASSES = ("mg_down", "mg_up")
 
 
 def pass_table(solver, levels, precision, reps=20):
@@ -520,12 +523,26 @@ def pass_table(solver, levels, precision, reps=20):
                         "CSR of R: nnz_R*(s_v+4) + (n_c+1)*4 + d gathered, b_c and sol1_c written, D_c read"),
         "mg_prolong": (csr(nnz_p, n, sv) + nc * sx + 2 * n * sx,
                        "CSR of P: nnz_P*(s_v+4) + (n+1)*4 + x_c gathered, x read and written"),
+        "mg_down": (csr(nnz, n, sv) + n * sx * 4 + csr(nnz_r, nc, sv) + nc * sx * 3,
+                    "CSR of A once + x read, x2 written, b and D read + CSR of R + b_c, sol1_c written, D_c read"),
+        "mg_up": (csr(nnz, n, sv) + csr(nnz_p, n, sv) + nc * sx + n * sx * 3 + n * 16,
+                  "CSR of A once + CSR of P + x_c gathered + x2, b, D read (s_x) + r read and z written (FP64)"),
     }
     out = {}
+    fused = True
     for k, (by, definition) in alg.items():
-        ms, stored = solver.time_kernel(k, reps=reps, flush_l2=True)
+        try:
+            ms, stored = solver.time_kernel(k, reps=reps, flush_l2=True)
+        except Exception:
+            if k in FUSED_PASSES:        # the finest level is not a structured grid: no fused passes
+                fused = False
+                continue
+            raise
         out[k] = {"kernel": PASS_KERNELS[k], "us": ms * 1e3, "csr_bytes": by, "csr_definition": definition,
                   "csr_gbs": by / (ms * 1e-3) / 1e9, "stored_bytes": stored, "stored_gbs": stored / (ms * 1e-3) / 1e9}
+    # which of them the solve launches on the finest level
+    for k in out:
+        out[k]["in_solve"] = k == "pcg_spmv" or ((k in FUSED_PASSES) == (fused and solver.cfg.fused >= n))
     return out
 
 
@@ -615,6 +632,9 @@ def main():
                     help="gathered-vector window of a TMA chunk: 2 prefetch into L2, 1 stage in shared memory, 0 none")
     ap.add_argument("--diagonal", type=int, choices=[0, 1], default=1,
                     help="diagonal storage of system matrices on at most 27 diagonals (1) or sliced ELL (0)")
+    ap.add_argument("--fused-rows", type=int, default=None,
+                    help="structured 2D levels with at most this many rows run fused V(2,2) passes "
+                         "(default: the library's threshold; 0 = one pass per step everywhere)")
     ap.add_argument("--pdl", type=int, choices=[0, 1], default=1,
                     help="programmatic dependent launch of the solve's kernels (1) or plain stream order (0)")
     ap.add_argument("--cycle", choices=["V", "F", "W"], default="V",
@@ -665,7 +685,7 @@ def main():
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
                                     cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle,
-                                    diagonal=args.diagonal, pdl=args.pdl)
+                                    diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows)
     info_lv = solver.level_info()
     if args.profile_kernel:
         ms_k, by_k = solver.time_kernel(args.profile_kernel, reps=3, flush_l2=True)
@@ -738,7 +758,7 @@ def main():
     extra = {}
     if not args.no_plain and precision != "f64":
         plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window,
-                                       diagonal=args.diagonal, pdl=args.pdl)
+                                       diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush()
@@ -760,7 +780,7 @@ def main():
     # is the one with the largest time per solve (each runs once per V-cycle / PCG iteration)
     peak, peak_kind = read_peaks()
     passes = pass_table(solver, levels, precision)
-    dom = max(passes, key=lambda k: passes[k]["us"])
+    dom = max((k for k in passes if passes[k]["in_solve"]), key=lambda k: passes[k]["us"])
     dp = passes[dom]
     traffic = MEASURED_TRAFFIC.get((args.workload, args.ordering, dom))
     spmv_gbs = {"pcg_spmv_f64": passes["pcg_spmv"]["csr_gbs"],

@@ -512,6 +512,12 @@ namespace fb
   template<typename V, typename S> struct OnSystem<OpRestrict<V, S>> { static constexpr bool value = false; };
   template<typename V, typename S> struct OnSystem<OpProlong<V, S>> { static constexpr bool value = false; };
 
+} // namespace fb
+
+#include "fb_fused.cuh"
+
+namespace fb
+{
   // ------------------------------------------------------------------ coarse-level tail
   // The part of a multigrid cycle below the tail threshold (levels whose row count is at most the
   // threshold, down to the coarsest) in ONE block of TAIL_NT threads: block-stride loops separated
@@ -1468,6 +1474,51 @@ namespace fb
     int32_t* doff = nullptr;                // diagonal storage: the diagonals' offsets
   };
 
+  // Grid width W when A is the 9-point operator of a lexicographically numbered W x W vertex grid
+  // in diagonal storage with all nine diagonals: every stored entry couples a vertex with itself
+  // or one of its eight neighbours (so no entry wraps around a grid line); 0 otherwise.
+  static uint32_t grid2d_width(const HostCsr& A, const DevMat& D)
+  {
+    if(!D.doff || D.kw != 9 || A.rows != A.cols)
+      return 0;
+    const uint32_t w = uint32_t(std::llround(std::sqrt(double(A.rows))));
+    if(w < 3 || uint64_t(w) * w != A.rows)
+      return 0;
+    for(uint32_t i = 0; i < A.rows; ++i)
+    {
+      const int x = int(i % w), y = int(i / w);
+      for(uint32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      {
+        const int cx = int(A.col[k] % w), cy = int(A.col[k] / w);
+        if(std::abs(cx - x) > 1 || std::abs(cy - y) > 1)
+          return 0;
+      }
+    }
+    return w;
+  }
+
+  // R (coarse grid (w+1)/2 squared <- fine grid w squared): every stored entry of coarse row
+  // (I, J) couples a fine vertex within one step of (2I, 2J)
+  static bool restriction_local(const HostCsr& R, uint32_t w)
+  {
+    if(w % 2 == 0)
+      return false;
+    const uint32_t wc = (w + 1) / 2;
+    if(R.rows != wc * wc || R.cols != w * w)
+      return false;
+    for(uint32_t j = 0; j < R.rows; ++j)
+    {
+      const int I = int(j % wc), J = int(j / wc);
+      for(uint32_t k = R.rp[j]; k < R.rp[j + 1]; ++k)
+      {
+        const int cx = int(R.col[k] % w), cy = int(R.col[k] / w);
+        if(std::abs(cx - 2 * I) > 1 || std::abs(cy - 2 * J) > 1)
+          return false;
+      }
+    }
+    return true;
+  }
+
   template<typename V> DCsr<V> view(const DevMat& m)
   {
     return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw, m.doff};
@@ -1483,6 +1534,9 @@ namespace fb
     void *b = nullptr, *x = nullptr, *x2 = nullptr, *d = nullptr, *c = nullptr, *c2 = nullptr;
     int* skip_pre = nullptr;
     int* skip_post = nullptr;
+    uint32_t gw = 0;         // grid width when the level is a structured 2D grid (fused passes), else 0
+    bool fz_down = false;    // the fused down pass applies (structured A and restriction)
+    bool fz_up = false;      // the fused up pass applies (structured A)
   };
 
   // _apply_rest(from, smooth_first) down to level stop: pre-smoothing and defect on every level
@@ -1602,6 +1656,8 @@ struct fb_solver
   std::vector<uint32_t> seg_off, seg_len;   // program of each tail segment of `events`, in order
   double* cgc_omega = nullptr;   // step length of the adaptive coarse-grid correction
   int max_iter_cap = 0;   // max_iter at creation: the defect history holds max_iter + 2 entries
+  void* vc_top = nullptr; // buffer that holds the finest level's result after a standalone V-cycle
+  uint32_t slot_cap = 0;  // blocks whose (two) partial sums the reduction slot holds
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
   double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
@@ -2034,6 +2090,67 @@ namespace fb
       bytes += csr_bytes(f.P, 1, 1) + f.n;
     }
 
+    // grid sizes of the fused passes of level l
+    uint32_t fused_down_grid(int l) const
+    {
+      const uint32_t t = ((s->lv[size_t(l)].gw + 1) / 2 + FZ_DOWN_TILE - 1) / FZ_DOWN_TILE;
+      return t * t;
+    }
+    uint32_t fused_up_grid(int l) const
+    {
+      const uint32_t t = (s->lv[size_t(l)].gw + FZ_UP_TILE - 1) / FZ_UP_TILE;
+      return t * t;
+    }
+    // the fused passes apply to levels of at most cfg.fused rows (structured ones, checked at
+    // creation) in V(2,2) cycles with the fixed coarse-grid correction
+    bool fused_level(int l) const
+    {
+      return s->cfg.fused > 0 && s->lv[size_t(l)].n <= uint32_t(s->cfg.fused) && s->cfg.cycle == FB_CYCLE_V &&
+             s->cfg.adapt_cgc == FB_CGC_FIXED && s->cfg.smooth_steps == 2;
+    }
+
+    // pre-smoothing step 2, defect and restriction of level l in one pass (k_fz_down): sol1 in x,
+    // the smoothed iterate to x2, b / sol1 / skip flag of level l + 1
+    void fused_down(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      DevLevel& c = L(l + 1);
+      const bool coarsest = (l + 2 == s->nlev);
+      const uint32_t wc = (f.gw + 1) / 2;
+      if(!dry)
+        go(k_fz_down<V, S>, fused_down_grid(l), FZ_NT, 0, view<V>(f.A), view<V>(f.R), f.gw, wc, (const S*)f.b,
+          (const S*)f.x, (S*)f.x2, (const S*)f.dinv, f.dm, (const int*)f.skip_pre, (S*)c.b,
+          coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, (const Scalars*)s->sc);
+      ++launches;
+      bytes += f.A.bytes + f.R.bytes + double(f.n) * (4.0 * sizeof(S) + 1.0) +
+               double(c.n) * ((coarsest ? 1.0 : 3.0) * sizeof(S) + 1.0);
+      xcur[size_t(l)] = f.x2;
+    }
+
+    // prolongation and both post-smoothing steps of level l in one pass (k_fz_up); the result
+    // goes to the level's other x buffer (top: the PCG's z and r.z)
+    void fused_up(int l, bool top, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      void* xin = xcur[size_t(l)];
+      void* xout = (xin == f.x) ? f.x2 : f.x;
+      const S* xc = (const S*)xcur[size_t(l + 1)];
+      if(dry)
+        ;
+      else if(top)
+        go(k_fz_up<V, S, true>, fused_up_grid(l), FZ_NT, 0, view<V>(f.A), view<V>(f.P), f.gw, (const S*)xin, xc,
+          (S*)nullptr, (const S*)f.b, (const S*)f.dinv, f.dm, f.skip_post, s->z, (const double*)s->r, s->slot, s->sc);
+      else
+        go(k_fz_up<V, S, false>, fused_up_grid(l), FZ_NT, 0, view<V>(f.A), view<V>(f.P), f.gw, (const S*)xin, xc,
+          (S*)xout, (const S*)f.b, (const S*)f.dinv, f.dm, f.skip_post, (double*)nullptr, (const double*)nullptr,
+          s->slot, s->sc);
+      ++launches;
+      bytes += f.A.bytes + f.P.bytes + double(f.P.cols) * sizeof(S) + double(f.n) * (4.0 * sizeof(S) + 1.0) +
+               (top ? 16.0 * double(f.n) : 0.0);
+      if(!top)
+        xcur[size_t(l)] = xout;
+    }
+
     // adaptive coarse-grid correction of level l: cor = F(P x_{l+1}) in c, tmp = F(A cor) in c2,
     // the step length w, x += w cor, d += -w tmp
     void prolong_cgc(int l, std::vector<void*>& xcur)
@@ -2225,6 +2342,25 @@ namespace fb
           i = j;
           continue;
         }
+        // V(2,2) on a structured level: pre-smoothing, defect and restriction in one pass, and
+        // prolongation and post-smoothing in one pass
+        // (every fused grid's partial sums fit the reduction slot, which is sized for them)
+        if(e.op == EV_PRE && fused_level(l) && L(l).fz_down && fused_down_grid(l) <= s->slot_cap && i + 2 < e1 &&
+           ev[i + 1].op == EV_DEF &&
+           ev[i + 1].lvl == l && ev[i + 2].op == EV_RES && ev[i + 2].lvl == l)
+        {
+          fused_down(l, xcur);
+          i += 3;
+          continue;
+        }
+        if(e.op == EV_PRO && fused_level(l) && L(l).fz_up && fused_up_grid(l) <= s->slot_cap && i + 1 < e1 &&
+           ev[i + 1].lvl == l &&
+           (ev[i + 1].op == EV_POST || ev[i + 1].op == EV_POST_TOP))
+        {
+          fused_up(l, ev[i + 1].op == EV_POST_TOP && pcg_top, xcur);
+          i += 2;
+          continue;
+        }
         switch(e.op)
         {
           case EV_PRE: pre_smooth(l, xcur); break;
@@ -2250,6 +2386,8 @@ namespace fb
       xcur[0] = L(0).x;
       const int lt = s->ctail_first >= 0 ? s->ctail_first : s->tail_first;
       run_events(0, s->events.size(), pcg_top, lt, xcur);
+      if(!dry && !pcg_top)
+        s->vc_top = xcur[0];
     }
 
     const DevMat& A64() { return s->cfg.precision == FB_PREC_F64 ? L(0).A : L(0).A64; }
@@ -2479,6 +2617,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->diagonal = 1;
   c->pdl = 1;
   c->adapt_cgc = FB_CGC_FIXED;
+  c->fused = 70000;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -2632,6 +2771,14 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       FB_TRY(upload_mat(s.get(), D.P, permute(H.P, pf, inv_c), prec, &dms[size_t(l)]));
       FB_TRY(upload_mat(s.get(), D.R, permute(H.R, pc, inv_f), prec, &dms[size_t(l + 1)]));
     }
+    if(l + 1 < s->nlev)
+    {
+      D.gw = grid2d_width(A, D.A);
+      D.fz_up = D.gw != 0 && D.P.col && !D.P.dcol && D.P.kmax <= uint32_t(FZ_KP);
+      const std::vector<uint32_t>& pc = s->perms[size_t(l + 1)];
+      D.fz_down = D.gw != 0 && D.R.col && !D.R.dcol && D.R.kmax <= uint32_t(FZ_KR) &&
+                  restriction_local(permute(H.R, pc, inv_f), D.gw);
+    }
     const std::vector<uint8_t>& dm = dms[size_t(l)];
     FB_TRY(dalloc(s.get(), (void**)&D.dm, D.n));
     FB_CUDA(cudaMemcpy(D.dm, dm.data(), D.n, cudaMemcpyHostToDevice));
@@ -2693,6 +2840,17 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     FB_CUDA(cudaGetDevice(&dev));
     FB_CUDA(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev));
   }
+  // the fused passes' grids: ceil(W / 16)^2 (up, 16 x 16 fine tiles) and ceil(Wc / 8)^2 (down,
+  // 8 x 8 coarse tiles) blocks, each with two partial sums
+  for(int l = 0; l + 1 < s->nlev; ++l)
+  {
+    const DevLevel& D = s->lv[size_t(l)];
+    if(!D.gw)
+      continue;
+    const uint32_t tu = (D.gw + FZ_UP_TILE - 1) / FZ_UP_TILE, td = ((D.gw + 1) / 2 + FZ_DOWN_TILE - 1) / FZ_DOWN_TILE;
+    max_blocks = std::max(max_blocks, std::max(tu * tu, td * td));
+  }
+  s->slot_cap = max_blocks;
   FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * 2 * (max_blocks + 1)));
   FB_TRY(dalloc(s.get(), (void**)&s->cgc_omega, sizeof(double)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
@@ -2943,7 +3101,7 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def)
   // the top level's solution: the buffer the last post-smoothing step wrote (x or x2 by parity)
   const DevLevel& t = s->lv[0];
   const int steps = std::max(1, s->cfg.smooth_steps);
-  void* xtop = ((steps - 1) % 2 == 0) ? t.x : t.x2;
+  void* xtop = s->vc_top ? s->vc_top : (((steps - 1) % 2 == 0) ? t.x : t.x2);
   if(s->cfg.precision == FB_PREC_F64)
     FB_TRY(from_device_order(s, s->tmp_out, (const double*)xtop));
   else
@@ -3032,6 +3190,19 @@ namespace fb
         k_post2<V, S, true, true><<<blocks(t.n), NT, t.A.smem, st>>>(view<V>(t.A), (const S*)t.d, (const S*)t.c,
           (S*)t.c2, (S*)t.x, s->z, s->r, (const S*)t.dinv, t.dm, t.skip_post, s->slot, s->sc);
     }
+    else if(which == FB_KERNEL_MG_DOWN)
+    {
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      l.fused_down(0, xcur);
+    }
+    else if(which == FB_KERNEL_MG_UP)
+    {
+      // the finest level's pass as the solve runs it: it also forms z and r.z
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      xcur[0] = t.x2;
+      xcur[1] = s->lv[1].x2;
+      l.fused_up(0, true, xcur);
+    }
     else if(which == FB_KERNEL_MG_RESTRICT)
       l.restrict_to(0);
     else if(which == FB_KERNEL_MG_PROLONG)
@@ -3073,6 +3244,12 @@ namespace fb
         return t.R.bytes + double(t.R.cols) * sx + nc * sx * (coarsest ? 1.0 : 3.0) + nc;
       }
       case FB_KERNEL_MG_PROLONG: return csr(t.P, 1, 1) + n;
+      case FB_KERNEL_MG_DOWN:
+      {
+        const bool coarsest = s->nlev == 2;
+        return t.A.bytes + t.R.bytes + n * (4.0 * sx + 1.0) + double(s->lv[1].n) * ((coarsest ? 1.0 : 3.0) * sx + 1.0);
+      }
+      case FB_KERNEL_MG_UP: return t.A.bytes + t.P.bytes + double(t.P.cols) * sx + n * (4.0 * sx + 1.0) + 16.0 * n;
       default: return 0.0;
     }
   }
@@ -3083,7 +3260,9 @@ extern "C" {
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
   double* bytes_per_launch)
 {
-  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_PROLONG ||
+  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_UP ||
+     (which == FB_KERNEL_MG_DOWN && (s->nlev < 2 || !s->lv[0].fz_down)) ||
+     (which == FB_KERNEL_MG_UP && (s->nlev < 2 || !s->lv[0].fz_up)) ||
      (which == FB_KERNEL_MG_TAIL && s->tail_first < 0 && s->ctail_first < 0) ||
      (which >= FB_KERNEL_MG_SMOOTH && s->nlev < 2) ||
      (which >= FB_KERNEL_MG_SMOOTH && (s->tail_first == 0 || s->ctail_first == 0)))

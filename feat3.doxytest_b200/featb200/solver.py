@@ -285,6 +285,12 @@ class PCG:
         stream order (0)."""
         self.cfg.pdl = int(bool(on))
 
+    def set_fused(self, rows):
+        """Fused V(2,2) passes on structured 2D levels of at most `rows` rows (default 70000;
+        True = every level, False / 0 = none): one pass for pre-smoothing, defect and restriction,
+        one for prolongation and post-smoothing."""
+        self.cfg.fused = (2 ** 31 - 1) if rows is True else int(rows)
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -374,9 +380,10 @@ class PCG:
     def time_kernel(self, which="pcg_spmv", reps=20, flush_l2=True):
         """Mean launch time (ms) and stored bytes per launch of one solver kernel timed alone:
         pcg_spmv, mg_defect, mg_smooth, mg_post1, mg_post2, mg_restrict, mg_prolong (finest-level
-        passes), mg_tail (the coarse-level tail kernel) or mg_cycle (one whole multigrid cycle)."""
+        passes), mg_down / mg_up (the fused passes of a structured finest level), mg_tail (the
+        coarse-level tail kernel) or mg_cycle (one whole multigrid cycle)."""
         code = {"pcg_spmv": 0, "mg_defect": 1, "mg_tail": 2, "mg_cycle": 3, "mg_smooth": 4, "mg_post1": 5,
-                "mg_post2": 6, "mg_restrict": 7, "mg_prolong": 8}[which]
+                "mg_post2": 6, "mg_restrict": 7, "mg_prolong": 8, "mg_down": 9, "mg_up": 10}[which]
         ms, by = C.c_double(), C.c_double()
         _lib.check(_lib.lib().fb_solver_time_kernel(self._s, code, int(reps), 1 if flush_l2 else 0, C.byref(ms),
                                                      C.byref(by)), "fb_solver_time_kernel")
@@ -400,7 +407,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed"):
+                        cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed", fused=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -431,6 +438,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_diagonal(diagonal)
     if pdl is not None:
         s.set_pdl(pdl)
+    if fused is not None:
+        s.set_fused(fused)
     h.init()
     s.init()
     return s

@@ -238,6 +238,12 @@ typedef struct
                            coarse-grid correction is scaled by the step length that minimises the
                            energy or the defect, and the post-smoother starts from the defect
                            updated with A P x_c (MultiGrid::_apply_prol, multigrid.hpp:1880-1960) */
+  int fused;            /* levels with at most this many rows (default 70000; 0 = never) that are
+                           structured 2D grids (lexicographic 9-point operator in diagonal storage,
+                           local restriction) run, in a V(2,2) cycle with the fixed coarse-grid
+                           correction, pre-smoothing + defect + restriction as one pass and
+                           prolongation + post-smoothing as another (tiles with halos recomputed in
+                           shared memory); results are bitwise those of one pass per step */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
@@ -286,6 +292,9 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
 #define FB_KERNEL_MG_POST2 6   /* post-smoothing step 2 with the PCG's z = x + c' and r.z, finest level */
 #define FB_KERNEL_MG_RESTRICT 7 /* restriction b_c = F(R d) with sol1_c = F(D_c b_c), finest to next level */
 #define FB_KERNEL_MG_PROLONG 8 /* prolongation x += F(P x_c), next level to finest */
+#define FB_KERNEL_MG_DOWN 9    /* fused pre-smoothing step 2 + defect + restriction, finest level (structured grids,
+                                  whatever the `fused` row threshold) */
+#define FB_KERNEL_MG_UP 10     /* fused prolongation + post-smoothing with the PCG's z and r.z, finest level */
 
 /* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
  * on that stream (the finest level's pass kernels need a finest level above the coarse-level tail);
