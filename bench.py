@@ -621,7 +621,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison solve")
     ap.add_argument("--profile-solves", type=int, default=0,
                     help="only run warm-up + this many solves (for a profiler's launch list), print nothing else")
-    ap.add_argument("--profile-kernel", default=None, choices=sorted(PASS_KERNELS),
+    ap.add_argument("--profile-kernel", default=None, choices=sorted(PASS_KERNELS) + ["mg_tail"],
                     help="only launch this finest-level pass a few times alone (for a profiler), print nothing else")
     ap.add_argument("--tail-rows", type=int, default=None)
     ap.add_argument("--tma-rows", type=int, default=None,

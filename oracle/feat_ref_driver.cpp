@@ -27,7 +27,7 @@
 //   feat_oracle solve --dim D --level L --out DIR [--rhs sine|gauss] [--params FILE]
 //                     [--kappa FILE] [--omega W] [--steps S] [--tol T] [--iterates K]
 //                     [--vcycle] [--dump-levels] [--time REPS] [--no-dump] [--cycle v|f|w]
-//                     [--cgc fixed|energy|defect]
+//                     [--cgc fixed|energy|defect] [--smoother jacobi|sor|ssor] [--sor-omega W]
 //
 // The params files are written by the caller (tests/bench) so that the reference and the GPU
 // path consume exactly the same Gaussian and random-field coefficients.
@@ -60,6 +60,8 @@
 #include <kernel/solver/pcg.hpp>
 #include <kernel/solver/richardson.hpp>
 #include <kernel/solver/jacobi_precond.hpp>
+#include <kernel/solver/sor_precond.hpp>
+#include <kernel/solver/ssor_precond.hpp>
 #include <kernel/solver/multigrid.hpp>
 #ifdef FEATB200_BACKEND
 #include <kernel/backend.hpp>
@@ -363,6 +365,8 @@ namespace Oracle
     bool dump_levels = false;
     bool dump = true;
     int time_reps = 0;
+    std::string smoother = "jacobi";   // the Richardson smoother's preconditioner: jacobi | sor | ssor
+    double sor_omega = 1.0;            // SOR / SSOR damping
     std::string backend = "generic";   // generic | b200 (FEATB200_BACKEND builds only)
     bool b200_solver = false;          // FEATB200_BACKEND builds only
   };
@@ -512,13 +516,20 @@ namespace Oracle
     top.filter.filter_rhs(vec_rhs);
     const double setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_setup).count();
 
-    // hierarchy: fine levels with Richardson(1) + Jacobi(omega), min = max = steps; coarse: exact inverse
+    // hierarchy: fine levels with Richardson(1) + Jacobi(omega) (or SOR / SSOR with the generic
+    // backend), min = max = steps; coarse: exact inverse
     auto hierarchy = std::make_shared<Solver::MultiGridHierarchy<MatrixType, FilterType, TransferType>>(levels.size());
     for(std::size_t i = 0; (i + 1) < levels.size(); ++i)
     {
       LevelType& lvl = *levels.at(i);
-      auto jacobi = Solver::new_jacobi_precond(lvl.matrix, lvl.filter, DataType(opt.omega));
-      auto smoother = Solver::new_richardson(lvl.matrix, lvl.filter, DataType(1), jacobi);
+      std::shared_ptr<Solver::SolverBase<VectorType>> precond;
+      if(opt.smoother == "sor")
+        precond = Solver::new_sor_precond(PreferredBackend::generic, lvl.matrix, lvl.filter, DataType(opt.sor_omega));
+      else if(opt.smoother == "ssor")
+        precond = Solver::new_ssor_precond(PreferredBackend::generic, lvl.matrix, lvl.filter, DataType(opt.sor_omega));
+      else
+        precond = Solver::new_jacobi_precond(lvl.matrix, lvl.filter, DataType(opt.omega));
+      auto smoother = Solver::new_richardson(lvl.matrix, lvl.filter, DataType(1), precond);
       smoother->set_min_iter(opt.steps);
       smoother->set_max_iter(opt.steps);
       hierarchy->push_level(lvl.matrix, lvl.filter, lvl.transfer, smoother, smoother, smoother);
@@ -753,6 +764,8 @@ int main(int argc, char* argv[])
     else if(a == "--dump-levels") opt.dump_levels = true;
     else if(a == "--no-dump") opt.dump = false;
     else if(a == "--time") opt.time_reps = std::stoi(next());
+    else if(a == "--smoother") opt.smoother = next();
+    else if(a == "--sor-omega") opt.sor_omega = std::stod(next());
 #ifdef FEATB200_BACKEND
     else if(a == "--backend") opt.backend = next();
     else if(a == "--b200-solver") opt.b200_solver = true;

@@ -22,6 +22,13 @@
  *   oc_pcg_solve        kernel/solver/pcg.hpp:159-286 (correct + _apply_intern) with the stopping
  *                       logic of kernel/solver/iterative.hpp (defaults: tol_abs = 1/eps^2,
  *                       div_rel = 1/eps, div_abs = 1/eps^2, no stagnation check)
+ *   sor_generic         kernel/solver/sor_precond.hpp:179-224 (SORPrecondWithBackend<generic, CSR>)
+ *   ssor_generic        kernel/solver/ssor_precond.hpp (SSORPrecondWithBackend<generic, CSR>: forward
+ *                       and backward insertion, scaling by omega (2 - omega))
+ *   sor_coloured,       the coloured sweeps of the reference's CUDA backend (kernel/solver/sor_precond.cu:
+ *   ssor_coloured       26-41 and :294-315, kernel/solver/ssor_precond.cu:25-60 and :182-230): y = 0,
+ *                       then colour by colour, colours by ascending row count; the colouring itself
+ *                       (greedy_colours below, first fit in row order) replaces cusparseDcsrcolor
  * The coarse-grid solve is an exact inverse of the matrix restricted to the free DOFs, formed by
  * Gauss-Jordan elimination with partial pivoting and applied in ascending column order (the same
  * coarse solver the reference-side driver oracle/feat_ref_driver.cpp plugs into the reference).
@@ -162,6 +169,12 @@ typedef struct
   double* cinv;
   /* PCG vectors on the finest level */
   double *r, *p, *t;
+  int smoother;          /* 0 Jacobi, 1 SOR, 2 SSOR: the Richardson smoother's preconditioner */
+  double sor_omega;      /* SOR / SSOR damping */
+  int coloured;          /* 1: the reference's coloured (CUDA) sweeps with greedy_colours */
+  uint32_t** corder;     /* per level: rows colour by colour; cofs: colour offsets */
+  uint32_t** cofs;
+  int* ncol;
   int cycle;             /* 0 V, 1 F, 2 W (MultiGridCycle) */
   int cgc;               /* 0 fixed, 1 energy minimisation, 2 defect minimisation (MultiGridAdaptCGC) */
 } oc_mg;
@@ -285,6 +298,13 @@ void oc_mg_destroy(oc_mg* mg)
     free(v->rhs); free(v->sol); free(v->def); free(v->cor); free(v->tmp);
     free(v->inv_diag); free(v->sm_def); free(v->sm_cor);
   }
+  if(mg->corder)
+    for(int l = 0; l < mg->nlevels; ++l)
+    {
+      free(mg->corder[l]);
+      free(mg->cofs[l]);
+    }
+  free(mg->corder); free(mg->cofs); free(mg->ncol);
   free(mg->lv);
   free(mg->free_dofs);
   free(mg->cinv);
@@ -292,7 +312,175 @@ void oc_mg_destroy(oc_mg* mg)
   free(mg);
 }
 
-/* Richardson(omega = 1) with Jacobi preconditioner, min_iter = max_iter = steps:
+/* SORPrecond (generic): out = copy(in), forward insertion out_i = w (in_i - sum_{j<i} a_ij out_j) / a_ii
+ * over the row's entries left of the diagonal in stored order */
+static void sor_generic(const oc_csr* A, double* out, const double* in, double w)
+{
+  const uint64_t n = A->rows;
+  memcpy(out, in, sizeof(double) * n);
+  for(uint64_t i = 0; i < n; ++i)
+  {
+    uint64_t col;
+    double d = 0.0;
+    for(col = A->row_ptr[i]; A->col_ind[col] < i; ++col)
+      d += A->val[col] * out[A->col_ind[col]];
+    out[i] = w * (in[i] - d) / A->val[col];
+  }
+}
+
+/* SSORPrecond (generic): forward insertion out_i = (in_i - w d) / a_ii, backward insertion
+ * out_i -= w d / a_ii with d over the entries right of the diagonal from the row's end, then
+ * out *= w (2 - w) */
+static void ssor_generic(const oc_csr* A, double* out, const double* in, double w)
+{
+  const uint64_t n = A->rows;
+  memcpy(out, in, sizeof(double) * n);
+  for(uint64_t i = 0; i < n; ++i)
+  {
+    uint64_t col;
+    double d = 0.0;
+    for(col = A->row_ptr[i]; A->col_ind[col] < i; ++col)
+      d += A->val[col] * out[A->col_ind[col]];
+    out[i] = (in[i] - w * d) / A->val[col];
+  }
+  for(uint64_t i = n; i > 0;)
+  {
+    --i;
+    uint64_t col;
+    double d = 0.0;
+    for(col = A->row_ptr[i + 1] - 1; A->col_ind[col] > i; --col)
+      d += A->val[col] * out[A->col_ind[col]];
+    out[i] -= w * d / A->val[col];
+  }
+  const double sc = w * (2.0 - w);
+  for(uint64_t i = 0; i < n; ++i)
+    out[i] = out[i] * sc;
+}
+
+/* the coloured sweeps: out = 0, then colour by colour (rows of one colour are not coupled) */
+static void sor_coloured(const oc_csr* A, double* out, const double* in, double w, const uint32_t* order,
+  const uint32_t* cofs, int ncol, int ssor)
+{
+  memset(out, 0, sizeof(double) * A->rows);
+  for(int c = 0; c < ncol; ++c)
+    for(uint32_t k = cofs[c]; k < cofs[c + 1]; ++k)
+    {
+      const uint64_t row = order[k];
+      uint64_t col;
+      double d = 0.0;
+      for(col = A->row_ptr[row]; A->col_ind[col] < row; ++col)
+        d += A->val[col] * out[A->col_ind[col]];
+      out[row] = ssor ? (in[row] - w * d) / A->val[col] : w * (in[row] - d) / A->val[col];
+    }
+  if(!ssor)
+    return;
+  for(int c = 0; c < ncol; ++c)
+    for(uint32_t k = cofs[c]; k < cofs[c + 1]; ++k)
+    {
+      const uint64_t row = order[k];
+      uint64_t col;
+      double d = 0.0;
+      for(col = A->row_ptr[row + 1] - 1; A->col_ind[col] > row; --col)
+        d += A->val[col] * out[A->col_ind[col]];
+      out[row] -= w * d / A->val[col];
+    }
+  const double sc = w * (2.0 - w);
+  for(uint64_t i = 0; i < A->rows; ++i)
+    out[i] = out[i] * sc;
+}
+
+/* Greedy colouring of the symmetric pattern of A: rows in ascending order take the smallest colour
+ * no already coloured neighbour (a_ij or a_ji stored, j != i) has; colours are then ordered by
+ * ascending row count (ties: colour number) and each colour lists its rows in ascending order. */
+static int greedy_colours(const oc_csr* A, uint32_t** order_out, uint32_t** cofs_out)
+{
+  const uint64_t n = A->rows;
+  /* transpose pattern */
+  uint64_t* tp = (uint64_t*)calloc(n + 1, sizeof(uint64_t));
+  const uint64_t nnz = A->row_ptr[n];
+  uint64_t* tc = (uint64_t*)malloc(sizeof(uint64_t) * (nnz ? nnz : 1));
+  for(uint64_t k = 0; k < nnz; ++k)
+    ++tp[A->col_ind[k] + 1];
+  for(uint64_t i = 0; i < n; ++i)
+    tp[i + 1] += tp[i];
+  uint64_t* fill = (uint64_t*)malloc(sizeof(uint64_t) * (n ? n : 1));
+  memcpy(fill, tp, sizeof(uint64_t) * n);
+  for(uint64_t i = 0; i < n; ++i)
+    for(uint64_t k = A->row_ptr[i]; k < A->row_ptr[i + 1]; ++k)
+      tc[fill[A->col_ind[k]]++] = i;
+  int* colour = (int*)malloc(sizeof(int) * (n ? n : 1));
+  int* mark = (int*)malloc(sizeof(int) * (n + 1));
+  for(uint64_t i = 0; i <= n; ++i)
+    mark[i] = -1;
+  int ncol = 0;
+  for(uint64_t i = 0; i < n; ++i)
+  {
+    for(uint64_t k = A->row_ptr[i]; k < A->row_ptr[i + 1]; ++k)
+      if(A->col_ind[k] < i)
+        mark[colour[A->col_ind[k]]] = (int)i;
+    for(uint64_t k = tp[i]; k < tp[i + 1]; ++k)
+      if(tc[k] < i)
+        mark[colour[tc[k]]] = (int)i;
+    int c = 0;
+    while(mark[c] == (int)i)
+      ++c;
+    colour[i] = c;
+    if(c + 1 > ncol)
+      ncol = c + 1;
+  }
+  uint64_t* cnt = (uint64_t*)calloc((size_t)ncol, sizeof(uint64_t));
+  for(uint64_t i = 0; i < n; ++i)
+    ++cnt[colour[i]];
+  int* rank = (int*)malloc(sizeof(int) * (size_t)ncol);   /* colours by ascending (count, number) */
+  for(int c = 0; c < ncol; ++c)
+    rank[c] = c;
+  for(int a = 1; a < ncol; ++a)
+  {
+    const int v = rank[a];
+    int b = a - 1;
+    while(b >= 0 && (cnt[rank[b]] > cnt[v] || (cnt[rank[b]] == cnt[v] && rank[b] > v)))
+    {
+      rank[b + 1] = rank[b];
+      --b;
+    }
+    rank[b + 1] = v;
+  }
+  uint32_t* order = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+  uint32_t* cofs = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)ncol + 1));
+  uint32_t pos = 0;
+  for(int r = 0; r < ncol; ++r)
+  {
+    cofs[r] = pos;
+    for(uint64_t i = 0; i < n; ++i)
+      if(colour[i] == rank[r])
+        order[pos++] = (uint32_t)i;
+  }
+  cofs[ncol] = pos;
+  free(tp); free(tc); free(fill); free(colour); free(mark); free(cnt); free(rank);
+  *order_out = order;
+  *cofs_out = cofs;
+  return ncol;
+}
+
+/* the smoother's preconditioner: cor = M(def), filtered (JacobiPrecond / SORPrecond / SSORPrecond) */
+static void precond_apply(const oc_mg* mg, const oc_level* v, int l, double* cor, const double* def)
+{
+  const uint64_t n = v->n;
+  if(mg->smoother == 0)
+  {
+    for(uint64_t i = 0; i < n; ++i)
+      cor[i] = v->inv_diag[i] * def[i];
+  }
+  else if(mg->coloured)
+    sor_coloured(&v->in.A, cor, def, mg->sor_omega, mg->corder[l], mg->cofs[l], mg->ncol[l], mg->smoother == 2);
+  else if(mg->smoother == 1)
+    sor_generic(&v->in.A, cor, def, mg->sor_omega);
+  else
+    ssor_generic(&v->in.A, cor, def, mg->sor_omega);
+  oc_filter_def(cor, v->in.fidx, v->in.nf);
+}
+
+/* Richardson(omega = 1) with the smoother's preconditioner, min_iter = max_iter = steps:
  * out = smoother(in), out starts at zero (richardson.hpp:160-228). */
 static void richardson_apply(const oc_mg* mg, const oc_level* v, double* out, const double* in)
 {
@@ -306,10 +494,8 @@ static void richardson_apply(const oc_mg* mg, const oc_level* v, double* out, co
     return;                                   /* Status::success */
   for(int it = 1;; ++it)
   {
-    /* JacobiPrecond::apply: cor = inv_diag .* def, filter_cor */
-    for(uint64_t i = 0; i < n; ++i)
-      v->sm_cor[i] = v->inv_diag[i] * v->sm_def[i];
-    oc_filter_def(v->sm_cor, v->in.fidx, v->in.nf);
+    /* JacobiPrecond / SORPrecond / SSORPrecond::apply, filter_cor */
+    precond_apply(mg, v, (int)(v - mg->lv), v->sm_cor, v->sm_def);
     oc_axpy(out, 1.0, v->sm_cor, out, n);
     oc_csr_apply(v->sm_def, -1.0, out, 1.0, in, &v->in.A, 0);
     oc_filter_def(v->sm_def, v->in.fidx, v->in.nf);
@@ -455,6 +641,39 @@ int oc_mg_vcycle(oc_mg* mg, double* cor, const double* def)
   apply_prol(mg, 0, 1);
   memcpy(cor, mg->lv[0].sol, sizeof(double) * mg->lv[0].n);
   return 0;
+}
+
+/* the smoother's preconditioner: kind 0 Jacobi (the default), 1 SOR, 2 SSOR with damping omega;
+ * coloured != 0: the reference's coloured sweeps with greedy_colours (on every level but the coarsest) */
+int oc_mg_set_smoother(oc_mg* mg, int kind, double omega, int coloured)
+{
+  if(kind < 0 || kind > 2)
+    return 1;
+  mg->smoother = kind;
+  mg->sor_omega = omega;
+  mg->coloured = kind != 0 && coloured;
+  if(mg->coloured && !mg->corder)
+  {
+    mg->corder = (uint32_t**)calloc((size_t)mg->nlevels, sizeof(uint32_t*));
+    mg->cofs = (uint32_t**)calloc((size_t)mg->nlevels, sizeof(uint32_t*));
+    mg->ncol = (int*)calloc((size_t)mg->nlevels, sizeof(int));
+    for(int l = 0; l < mg->nlevels; ++l)
+      mg->ncol[l] = greedy_colours(&mg->lv[l].in.A, &mg->corder[l], &mg->cofs[l]);
+  }
+  return 0;
+}
+
+/* the colouring of level l (greedy_colours): ncol colours, order[n] rows, cofs[ncol + 1] offsets;
+ * returns the colour count, or -1 without a coloured smoother */
+int oc_mg_colours(const oc_mg* mg, int l, uint32_t* order, uint32_t* cofs)
+{
+  if(!mg->corder || l < 0 || l >= mg->nlevels)
+    return -1;
+  if(order)
+    memcpy(order, mg->corder[l], sizeof(uint32_t) * mg->lv[l].n);
+  if(cofs)
+    memcpy(cofs, mg->cofs[l], sizeof(uint32_t) * ((size_t)mg->ncol[l] + 1));
+  return mg->ncol[l];
 }
 
 /* MultiGrid::set_cycle / set_adapt_cgc */

@@ -73,6 +73,8 @@ def lib():
         L.oc_mg_destroy.argtypes = [C.c_void_p]
         L.oc_mg_vcycle.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.oc_mg_set_cycle.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.oc_mg_set_smoother.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int]
+        L.oc_mg_colours.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.oc_pcg_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                    C.c_void_p, C.POINTER(C.c_int)]
         L.oc_pcg_jacobi.argtypes = [C.POINTER(_Csr), C.c_void_p, C.c_uint64, C.c_double, C.c_void_p,
@@ -130,7 +132,8 @@ class MultigridPCG:
     """The FP64 PCG + multigrid (V, F or W cycle with `steps` pre- and post-smoothing steps; fixed,
     energy- or defect-minimising coarse-grid correction) of the reference, restated in C."""
 
-    def __init__(self, levels, omega=0.7, steps=2, cycle="V", cgc="fixed"):
+    def __init__(self, levels, omega=0.7, steps=2, cycle="V", cgc="fixed", smoother="jacobi", sor_omega=1.0,
+                 coloured=False):
         self._keep = []
         arr = (_LevelIn * len(levels))()
         for i, lv in enumerate(levels):
@@ -148,10 +151,24 @@ class MultigridPCG:
             arr[i].nf = fidx.size
         self._arr = arr
         self.n = levels[0]["A"].shape[0]
+        self.sizes = [lv["A"].shape[0] for lv in levels]
         self._h = lib().oc_mg_create(len(levels), arr, omega, steps)
         if lib().oc_mg_set_cycle(self._h, {"V": 0, "F": 1, "W": 2}[cycle.upper()],
                                  {"fixed": 0, "energy": 1, "defect": 2}[cgc]) != 0:
             raise ValueError("unsupported cycle / coarse-grid correction")
+        if lib().oc_mg_set_smoother(self._h, {"jacobi": 0, "sor": 1, "ssor": 2}[smoother], float(sor_omega),
+                                    1 if coloured else 0) != 0:
+            raise ValueError("unsupported smoother")
+
+    def colours(self, level):
+        """(order, offsets) of the greedy colouring of `level` (coloured smoothers only)."""
+        nc = lib().oc_mg_colours(self._h, level, None, None)
+        if nc < 0:
+            raise ValueError("no colouring")
+        order = np.zeros(self.sizes[level], dtype=np.uint32)
+        cofs = np.zeros(nc + 1, dtype=np.uint32)
+        lib().oc_mg_colours(self._h, level, _ptr(order), _ptr(cofs))
+        return order, cofs
 
     def vcycle(self, d):
         d = np.ascontiguousarray(d, dtype=np.float64)
@@ -197,7 +214,7 @@ def feat_b200_available():
 
 def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, omega=0.7, steps=2,
                tol=1e-8, iterates=0, vcycle=False, dump_levels=False, time_reps=0, dump=True,
-               level_min=1, timeout=3600, cycle="v", cgc="fixed", b200=None):
+               level_min=1, timeout=3600, cycle="v", cgc="fixed", b200=None, smoother="jacobi", sor_omega=1.0):
     """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary.
     b200 = "ops" or "solver": the same program built as a FEAT CUDA build on the library's FEAT
     binding (oracle/_ref/feat_b200), with every LAFEM op on the library ("ops") or the whole solve
@@ -206,6 +223,8 @@ def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, ome
     cmd = [exe, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
            "--out", out_dir, "--rhs", rhs, "--omega", repr(omega), "--steps", str(steps), "--tol",
            repr(tol), "--iterates", str(iterates), "--time", str(time_reps), "--cycle", cycle, "--cgc", cgc]
+    if smoother != "jacobi":
+        cmd += ["--smoother", smoother, "--sor-omega", repr(float(sor_omega))]
     if params:
         cmd += ["--params", params]
     if kappa:
