@@ -515,6 +515,7 @@ namespace fb
 } // namespace fb
 
 #include "fb_fused.cuh"
+#include "fb_sor.cuh"
 
 namespace fb
 {
@@ -1539,6 +1540,17 @@ namespace fb
     bool fz_up = false;      // the fused up pass applies (structured A)
   };
 
+  // a level's SOR / SSOR sweep data: the full system matrix in CSR (stored order, Dirichlet rows
+  // included), the diagonal positions and the sweeps' colour orders (fb_sor.cuh)
+  struct DevSor
+  {
+    uint32_t *rp = nullptr, *col = nullptr, *posf = nullptr, *posb = nullptr;
+    void* val = nullptr;                 // the V-cycle's vector precision
+    uint32_t *of = nullptr, *cf = nullptr, *ob = nullptr, *cb = nullptr;   // forward / backward order, offsets
+    std::vector<uint32_t> hcf, hcb;      // the offsets on the host (one launch per colour)
+    uint64_t nnz = 0;
+  };
+
   // _apply_rest(from, smooth_first) down to level stop: pre-smoothing and defect on every level
   // but `from` when smooth_first is false (its defect is in place), restriction to the next level
   static void ev_down(std::vector<CycEv>& ev, int from, bool smooth_first, int stop)
@@ -1651,6 +1663,7 @@ struct fb_solver
   cudaGraph_t vgraph = nullptr;
   cudaGraphExec_t vexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<fb::DevSor> sor;              // per level (not the coarsest): SOR / SSOR sweep data
   std::vector<fb::CycEv> events;            // one multigrid cycle
   uint8_t* tail_prog = nullptr;             // tail kernel programs: events op << 4 | tail level
   std::vector<uint32_t> seg_off, seg_len;   // program of each tail segment of `events`, in order
@@ -1822,6 +1835,13 @@ namespace fb
     FB_TRY(dalloc(s, dst, sizeof(S) * std::max<size_t>(1, v.size())));
     std::vector<S> t(v.begin(), v.end());
     FB_CUDA(cudaMemcpy(*dst, t.data(), sizeof(S) * t.size(), cudaMemcpyHostToDevice));
+    return FB_OK;
+  }
+
+  static fb_status upload_u32(fb_solver* s, uint32_t** dst, const std::vector<uint32_t>& v)
+  {
+    FB_TRY(dalloc(s, (void**)dst, sizeof(uint32_t) * std::max<size_t>(1, v.size())));
+    FB_CUDA(cudaMemcpy(*dst, v.data(), sizeof(uint32_t) * v.size(), cudaMemcpyHostToDevice));
     return FB_OK;
   }
 
@@ -2105,7 +2125,8 @@ namespace fb
     // creation) in V(2,2) cycles with the fixed coarse-grid correction
     bool fused_level(int l) const
     {
-      return s->cfg.fused > 0 && s->lv[size_t(l)].n <= uint32_t(s->cfg.fused) && s->cfg.cycle == FB_CYCLE_V &&
+      return s->cfg.fused > 0 && s->cfg.smoother == FB_SMOOTHER_JACOBI && s->lv[size_t(l)].n <= uint32_t(s->cfg.fused) &&
+             s->cfg.cycle == FB_CYCLE_V &&
              s->cfg.adapt_cgc == FB_CGC_FIXED && s->cfg.smooth_steps == 2;
     }
 
@@ -2172,6 +2193,152 @@ namespace fb
       }
       launches += 3;
       bytes += csr_bytes(f.P, 1, 1) + f.n + csr_bytes(f.A, 2, 1) + f.n + double(f.n) * sizeof(S) * 6;
+    }
+
+    // ---- SOR / SSOR smoothing (fb_sor.cuh): each Richardson step sweeps its defect into y and
+    // adds the filtered (SSOR: scaled) result to the smoother's iterate
+
+    // out = F(b - A x) with explicit buffers
+    void defect_into(int l, const void* b, const void* x, void* out)
+    {
+      DevLevel& f = L(l);
+      if(dry)
+        ;
+      else if(use_tma(f.A))
+        tma<V, S>(f.A, x, OpDefect<V, S>{(const S*)b, (S*)out, f.dm, s->sc});
+      else
+        go(k_defect<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)b, (const S*)x, (S*)out, f.dm, s->sc);
+      ++launches;
+      bytes += csr_bytes(f.A, 1, 1) + f.n;
+    }
+
+    template<int KIND>
+    void sweep_colours(const DevSor& q, const uint32_t* order, const uint32_t* dcofs, const std::vector<uint32_t>& hcofs,
+      const void* in, void* y)
+    {
+      const SorCsr<S> M{q.rp, q.col, (const S*)q.val, q.posf, q.posb};
+      const S w = S(s->cfg.smoother_omega);
+      const uint32_t ncol = uint32_t(hcofs.size()) - 1u;
+      if(ncol <= SWEEP_LAUNCH_MAX)
+      {
+        for(uint32_t c = 0; c < ncol; ++c)
+        {
+          const uint32_t cnt = hcofs[c + 1] - hcofs[c];
+          if(!dry && cnt)
+            go(k_sweep_colour<S, KIND>, blocks(cnt), NT, 0, M, (const S*)in, (S*)y, order + hcofs[c], cnt, w,
+              (const Scalars*)s->sc);
+          launches += cnt ? 1 : 0;
+        }
+      }
+      else
+      {
+        if(!dry)
+          go(k_sweep_block<S, KIND>, 1, SWEEP_BLOCK_NT, 0, M, (const S*)in, (S*)y, order, dcofs, ncol, w,
+            (const Scalars*)s->sc);
+        ++launches;
+      }
+    }
+
+    // y = the sweep(s) of the level's smoother applied to `in` (y zeroed first, as the coloured
+    // sweeps require)
+    void sweep(int l, const void* in, void* y)
+    {
+      const DevSor& q = s->sor[size_t(l)];
+      const uint32_t n = L(l).n;
+      if(!dry)
+        go(k_sweep_zero<S>, blocks(n), NT, 0, (S*)y, n, (const Scalars*)s->sc);
+      ++launches;
+      if(s->cfg.smoother == FB_SMOOTHER_SOR)
+        sweep_colours<SW_SOR>(q, q.of, q.cf, q.hcf, in, y);
+      else
+      {
+        sweep_colours<SW_SSOR_FWD>(q, q.of, q.cf, q.hcf, in, y);
+        sweep_colours<SW_SSOR_BWD>(q, q.ob, q.cb, q.hcb, in, y);
+      }
+      const double nsw = s->cfg.smoother == FB_SMOOTHER_SOR ? 1.0 : 2.0;
+      bytes += nsw * (double(q.nnz) * (4.0 + sizeof(S)) + double(n) * (12.0 + 2.0 * sizeof(S)));
+    }
+
+    // out = (skip ? 0 : F(scale * y) + base)
+    void sweep_finish(int l, const void* y, const void* base, void* out, const int* skip)
+    {
+      DevLevel& f = L(l);
+      const double w = s->cfg.smoother_omega;
+      const bool ssor = s->cfg.smoother == FB_SMOOTHER_SSOR;
+      if(!dry)
+        go(k_sweep_finish<S>, blocks(f.n), NT, 0, (const S*)y, (const S*)base, (S*)out, f.dm, skip,
+          S(ssor ? S(w) * (S(2.0) - S(w)) : S(1)), ssor ? 1 : 0, f.n, (const Scalars*)s->sc);
+      ++launches;
+      bytes += double(f.n) * ((base ? 3.0 : 2.0) * sizeof(S) + 1.0);
+    }
+
+    // pre-smoothing of level l with SOR / SSOR: x_1 = F(M b), x_k = x_{k-1} + F(M F(b - A x_{k-1}))
+    void sor_pre(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      const int steps = std::max(1, s->cfg.smooth_steps);
+      void* xa = nullptr;
+      void* xb = f.x;
+      for(int k = 1; k <= steps; ++k)
+      {
+        const void* in = f.b;
+        if(k > 1)
+        {
+          defect_into(l, f.b, xa, f.d);
+          in = f.d;
+        }
+        sweep(l, in, f.c);
+        sweep_finish(l, f.c, xa, xb, f.skip_pre);
+        xa = xb;
+        xb = (xb == f.x) ? f.x2 : f.x;
+      }
+      xcur[size_t(l)] = xa;
+    }
+
+    // post-smoothing of level l with SOR / SSOR as a correction of x: d = F(b - A x) (with the
+    // smoother's skip test), c_1 = F(M d), c_k = c_{k-1} + F(M F(d - A c_{k-1})), x += c
+    // (top: the PCG's z and r.z)
+    void sor_post(int l, bool top, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      const int steps = std::max(1, s->cfg.smooth_steps);
+      void* xf = xcur[size_t(l)];
+      void* y = (xf == f.x) ? f.x2 : f.x;
+      if(dry)
+        ;
+      else if(use_tma(f.A))
+        tma<V, S>(f.A, xf, OpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc});
+      else
+        go(k_post1<V, S>, blocks(f.n), NT, f.A.smem, view<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+          (const S*)f.dinv, f.dm, f.skip_post, s->slot, s->sc);
+      ++launches;
+      bytes += csr_bytes(f.A, 2, 2) + f.n;
+      void* ca = nullptr;
+      void* cb = f.c;
+      for(int k = 1; k <= steps; ++k)
+      {
+        const void* in = f.d;
+        if(k > 1)
+        {
+          defect_into(l, f.d, ca, cb);
+          in = cb;
+        }
+        sweep(l, in, y);
+        sweep_finish(l, y, ca, cb, f.skip_post);
+        ca = cb;
+        cb = (cb == f.c) ? f.c2 : f.c;
+      }
+      if(!dry)
+      {
+        if(top)
+          go(k_post_final<S, true>, blocks(f.n), NT, 0, (const S*)ca, (S*)xf, s->z, s->r, f.skip_post, f.n, s->slot,
+            s->sc);
+        else
+          go(k_post_final<S, false>, blocks(f.n), NT, 0, (const S*)ca, (S*)xf, nullptr, nullptr, f.skip_post, f.n,
+            s->slot, s->sc);
+      }
+      ++launches;
+      bytes += double(f.n) * sizeof(S) * 3;
     }
 
     // a smoother applied as a correction: d = F(b - A x), c = Richardson-Jacobi(d) from zero, x += c
@@ -2359,6 +2526,15 @@ namespace fb
         {
           fused_up(l, ev[i + 1].op == EV_POST_TOP && pcg_top, xcur);
           i += 2;
+          continue;
+        }
+        if(s->cfg.smoother != FB_SMOOTHER_JACOBI && (e.op == EV_PRE || e.op == EV_POST || e.op == EV_POST_TOP))
+        {
+          if(e.op == EV_PRE)
+            sor_pre(l, xcur);
+          else
+            sor_post(l, e.op == EV_POST_TOP && pcg_top, xcur);
+          ++i;
           continue;
         }
         switch(e.op)
@@ -2618,6 +2794,9 @@ void fb_solver_config_default(fb_solver_config* c)
   c->pdl = 1;
   c->adapt_cgc = FB_CGC_FIXED;
   c->fused = 70000;
+  c->smoother = FB_SMOOTHER_JACOBI;
+  c->smoother_omega = 1.0;
+  c->sweep_colouring = FB_SWEEP_SEQUENTIAL;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -2719,10 +2898,19 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
     fb_solver_config_default(&cfg);
   if(cfg.precision < FB_PREC_F64 || cfg.precision > FB_PREC_F32_BF16 || cfg.smooth_steps < 1 || cfg.max_iter < 0 ||
      cfg.cycle < FB_CYCLE_V || cfg.cycle > FB_CYCLE_W || cfg.adapt_cgc < FB_CGC_FIXED ||
-     cfg.adapt_cgc > FB_CGC_MIN_DEFECT)
+     cfg.adapt_cgc > FB_CGC_MIN_DEFECT || cfg.smoother < FB_SMOOTHER_JACOBI || cfg.smoother > FB_SMOOTHER_SSOR ||
+     (cfg.smoother != FB_SMOOTHER_JACOBI && !(cfg.smoother_omega > 0.0)) || cfg.sweep_colouring < FB_SWEEP_SEQUENTIAL ||
+     cfg.sweep_colouring > FB_SWEEP_COLOURED)
   {
     set_error("solver_create: bad configuration");
     return FB_ERR_ARG;
+  }
+  if(cfg.smoother != FB_SMOOTHER_JACOBI && (cfg.adapt_cgc != FB_CGC_FIXED || cfg.ordering != FB_ORDER_NATIVE))
+  {
+    // a sweep's result depends on the row numbering: it runs in the caller's numbering only
+    set_error("solver_create: SOR / SSOR smoothing needs the caller's numbering (FB_ORDER_NATIVE) and the fixed "
+              "coarse-grid correction");
+    return FB_ERR_UNSUPPORTED;
   }
   std::unique_ptr<fb_solver, void (*)(fb_solver*)> s(new fb_solver(), fb_solver_destroy);
   s->cfg = cfg;
@@ -2854,11 +3042,71 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
   FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * 2 * (max_blocks + 1)));
   FB_TRY(dalloc(s.get(), (void**)&s->cgc_omega, sizeof(double)));
   FB_TRY(dalloc(s.get(), (void**)&s->slot.counter, sizeof(unsigned int) * 4));
+  // SOR / SSOR sweeps: every level but the coarsest gets the full system matrix in CSR (stored
+  // order), the diagonal positions and the sweep orders
+  if(cfg.smoother != FB_SMOOTHER_JACOBI)
+  {
+    s->sor.resize(size_t(s->nlev));
+    for(int l = 0; l + 1 < s->nlev; ++l)
+    {
+      const HostCsr& A = h->levels[size_t(l)].A;
+      DevSor& q = s->sor[size_t(l)];
+      const uint32_t n = A.rows;
+      std::vector<uint32_t> posf(n), posb(n);
+      for(uint32_t i = 0; i < n; ++i)
+      {
+        uint32_t k = A.rp[i];
+        while(k < A.rp[i + 1] && A.col[k] < i)
+          ++k;
+        uint32_t kb = A.rp[i + 1];
+        while(kb > A.rp[i] && A.col[kb - 1] > i)
+          --kb;
+        if(k >= A.rp[i + 1] || A.col[k] != i || kb == A.rp[i] || A.col[kb - 1] != i)
+        {
+          set_error("solver_create: SOR / SSOR smoothing needs every row's diagonal entry, columns sorted");
+          return FB_ERR_UNSUPPORTED;
+        }
+        posf[i] = k;
+        posb[i] = kb - 1;
+      }
+      q.nnz = A.nnz();
+      FB_TRY(upload_u32(s.get(), &q.rp, A.rp));
+      FB_TRY(upload_u32(s.get(), &q.col, A.col));
+      FB_TRY(upload_u32(s.get(), &q.posf, posf));
+      FB_TRY(upload_u32(s.get(), &q.posb, posb));
+      if(prec == FB_PREC_F64)
+        FB_TRY(upload_vec<double>(s.get(), &q.val, A.val));
+      else
+      {
+        // the V-cycle's values: FP32, or BF16-rounded in the BF16-value mode
+        std::vector<double> v(A.val);
+        if(prec == FB_PREC_F32_BF16)
+          for(double& x : v)
+          {
+            const uint32_t u = uint32_t(to_bf16_rne(float(x))) << 16;
+            float f;
+            std::memcpy(&f, &u, sizeof(f));
+            x = double(f);
+          }
+        FB_TRY(upload_vec<float>(s.get(), &q.val, v));
+      }
+      const SweepOrder fw = cfg.sweep_colouring == FB_SWEEP_COLOURED ? greedy_colours(A) : sweep_levels(A, false);
+      const SweepOrder bw = cfg.sweep_colouring == FB_SWEEP_COLOURED ? fw : sweep_levels(A, true);
+      FB_TRY(upload_u32(s.get(), &q.of, fw.order));
+      FB_TRY(upload_u32(s.get(), &q.cf, fw.cofs));
+      FB_TRY(upload_u32(s.get(), &q.ob, bw.order));
+      FB_TRY(upload_u32(s.get(), &q.cb, bw.cofs));
+      q.hcf = fw.cofs;
+      q.hcb = bw.cofs;
+    }
+  }
   // the tail starts at the first level (below the top) with at most tail_rows rows, if it has a
-  // coarser level below it
+  // coarser level below it (Jacobi smoothing only: the tail kernels run no sweeps)
   s->tail_first = -1;
   s->ctail_first = -1;
-  if(cfg.cluster_rows > 0 && cfg.cycle == FB_CYCLE_V && cfg.adapt_cgc == FB_CGC_FIXED)
+  if(cfg.smoother != FB_SMOOTHER_JACOBI)
+    ;
+  else if(cfg.cluster_rows > 0 && cfg.cycle == FB_CYCLE_V && cfg.adapt_cgc == FB_CGC_FIXED)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.cluster_rows))
       {
@@ -2867,7 +3115,7 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       }
   if(s->ctail_first >= 0)
     FB_TRY(dalloc(s.get(), (void**)&s->cred, sizeof(double) * 2 * MAX_TAIL * CT_CS));
-  if(cfg.tail_rows > 0 && s->ctail_first < 0)
+  if(cfg.tail_rows > 0 && s->ctail_first < 0 && cfg.smoother == FB_SMOOTHER_JACOBI)
     for(int l = 1; l + 1 < s->nlev; ++l)
       if(s->lv[size_t(l)].n <= uint32_t(cfg.tail_rows))
       {

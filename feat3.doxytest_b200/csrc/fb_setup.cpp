@@ -378,4 +378,95 @@ namespace fb
       }
     }
   }
+
+  SweepOrder sweep_levels(const HostCsr& A, bool backward)
+  {
+    const uint32_t n = A.rows;
+    std::vector<uint32_t> lvl(n, 0);
+    uint32_t top = 0;
+    auto visit = [&](uint32_t i)
+    {
+      uint32_t l = 0;
+      for(uint32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      {
+        const uint32_t j = A.col[k];
+        if(backward ? j > i : j < i)
+          l = std::max(l, lvl[j] + 1u);
+      }
+      lvl[i] = l;
+      top = std::max(top, l);
+    };
+    if(backward)
+      for(uint32_t i = n; i > 0; --i)
+        visit(i - 1);
+    else
+      for(uint32_t i = 0; i < n; ++i)
+        visit(i);
+    SweepOrder so;
+    const uint32_t nl = n ? top + 1 : 0;
+    so.cofs.assign(size_t(nl) + 1, 0u);
+    for(uint32_t i = 0; i < n; ++i)
+      ++so.cofs[size_t(lvl[i]) + 1];
+    for(uint32_t l = 0; l < nl; ++l)
+      so.cofs[size_t(l) + 1] += so.cofs[l];
+    so.order.resize(n);
+    std::vector<uint32_t> fill(so.cofs.begin(), so.cofs.end() - 1);
+    for(uint32_t i = 0; i < n; ++i)
+      so.order[fill[lvl[i]]++] = i;
+    return so;
+  }
+
+  SweepOrder greedy_colours(const HostCsr& A)
+  {
+    const uint32_t n = A.rows;
+    // coupled rows of the symmetric pattern that precede row i: row i's own entries j < i and the
+    // rows j < i that store an entry in column i
+    std::vector<uint32_t> tp(size_t(n) + 1, 0u);
+    for(uint32_t c : A.col)
+      if(c < n)
+        ++tp[size_t(c) + 1];
+    for(uint32_t i = 0; i < n; ++i)
+      tp[size_t(i) + 1] += tp[i];
+    std::vector<uint32_t> tc(tp[n]), fill(tp.begin(), tp.end() - 1);
+    for(uint32_t i = 0; i < n; ++i)
+      for(uint32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if(A.col[k] < n)
+          tc[fill[A.col[k]]++] = i;
+    std::vector<uint32_t> colour(n, 0u);
+    std::vector<uint32_t> mark(size_t(n) + 1, UINT32_MAX);
+    uint32_t ncol = 0;
+    for(uint32_t i = 0; i < n; ++i)
+    {
+      for(uint32_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if(A.col[k] < i)
+          mark[colour[A.col[k]]] = i;
+      for(uint32_t k = tp[i]; k < tp[size_t(i) + 1]; ++k)
+        if(tc[k] < i)
+          mark[colour[tc[k]]] = i;
+      uint32_t c = 0;
+      while(mark[c] == i)
+        ++c;
+      colour[i] = c;
+      ncol = std::max(ncol, c + 1u);
+    }
+    std::vector<uint32_t> cnt(ncol, 0u);
+    for(uint32_t i = 0; i < n; ++i)
+      ++cnt[colour[i]];
+    std::vector<uint32_t> rank(ncol);
+    for(uint32_t c = 0; c < ncol; ++c)
+      rank[c] = c;
+    std::stable_sort(rank.begin(), rank.end(), [&](uint32_t a, uint32_t b) { return cnt[a] < cnt[b]; });
+    std::vector<uint32_t> pos(ncol);
+    for(uint32_t r = 0; r < ncol; ++r)
+      pos[rank[r]] = r;
+    SweepOrder so;
+    so.cofs.assign(size_t(ncol) + 1, 0u);
+    for(uint32_t r = 0; r < ncol; ++r)
+      so.cofs[size_t(r) + 1] = so.cofs[r] + cnt[rank[r]];
+    so.order.resize(n);
+    std::vector<uint32_t> f2(so.cofs.begin(), so.cofs.end() - 1);
+    for(uint32_t i = 0; i < n; ++i)
+      so.order[f2[pos[colour[i]]]++] = i;
+    return so;
+  }
 } // namespace fb

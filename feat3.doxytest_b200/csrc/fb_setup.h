@@ -49,6 +49,23 @@ namespace fb
 
   std::vector<uint32_t> inverse_perm(const std::vector<uint32_t>& perm);
 
+  // Order of a triangular sweep (SOR / SSOR): the rows of colour c are order[cofs[c] .. cofs[c+1]),
+  // colours processed in ascending order, rows of one colour independent of each other.
+  struct SweepOrder
+  {
+    std::vector<uint32_t> order, cofs;
+    uint32_t colours() const { return uint32_t(cofs.size()) - 1u; }
+  };
+  // Dependency levels of the sequential sweep over the entries left of the diagonal (forward) or
+  // right of it (backward): a row's level is one more than the highest level among the rows its
+  // entries couple it to on that side.  Sweeping level after level gives every row the same inputs
+  // as the sequential sweep, so the result is identical.
+  SweepOrder sweep_levels(const HostCsr& A, bool backward);
+  // Greedy colouring of the symmetric pattern (rows in ascending order take the smallest colour no
+  // coupled, already coloured row has), colours ordered by ascending row count, ties by number:
+  // the colouring of the coloured sweeps.
+  SweepOrder greedy_colours(const HostCsr& A);
+
   // A matrix in the device layout of the solvers: sliced ELL with 32-row slices (entry k of row
   // 32s+lane at soff[s] + 32k + lane, stored order kept), or plain ELL (uniform width kw, when it
   // stores at most 12.5% more entries).  Rows flagged in `empty` are stored without entries;

@@ -34,7 +34,8 @@ class SolverConfig(C.Structure):
                 ("rows_per_block", C.c_int), ("tail_rows", C.c_int), ("tma_rows", C.c_int),
                 ("cluster_rows", C.c_int), ("cycle", C.c_int), ("tma_window", C.c_int),
                 ("diagonal", C.c_int), ("pdl", C.c_int),
-                ("adapt_cgc", C.c_int), ("fused", C.c_int)]
+                ("adapt_cgc", C.c_int), ("fused", C.c_int), ("smoother", C.c_int),
+                ("smoother_omega", C.c_double), ("sweep_colouring", C.c_int)]
 
 
 class StoragePlan(C.Structure):

@@ -291,6 +291,15 @@ class PCG:
         one for prolongation and post-smoothing."""
         self.cfg.fused = (2 ** 31 - 1) if rows is True else int(rows)
 
+    def set_smoother(self, kind="jacobi", omega=1.0, sweep="sequential"):
+        """The Richardson smoother's preconditioner: "jacobi" (JacobiPrecond with the hierarchy's
+        damping), "sor" or "ssor" (SORPrecond / SSORPrecond with damping `omega`); SOR / SSOR sweep
+        in the rows' dependency levels ("sequential": the reference's generic sweep, bit for bit) or
+        in greedy colours ("coloured": the reference's coloured CUDA sweeps)."""
+        self.cfg.smoother = {"jacobi": 0, "sor": 1, "ssor": 2}[kind]
+        self.cfg.smoother_omega = float(omega)
+        self.cfg.sweep_colouring = {"sequential": 0, "coloured": 1}[sweep]
+
     def set_tail_rows(self, rows):
         """Levels with at most `rows` rows (below the finest) run in one single-block kernel."""
         self.cfg.tail_rows = int(rows)
@@ -407,7 +416,8 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
-                        cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed", fused=None):
+                        cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed", fused=None,
+                        smoother="jacobi", smoother_omega=1.0, sweep="sequential"):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -440,6 +450,7 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_pdl(pdl)
     if fused is not None:
         s.set_fused(fused)
+    s.set_smoother(smoother, smoother_omega, sweep)
     h.init()
     s.init()
     return s

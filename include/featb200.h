@@ -196,6 +196,14 @@ void fb_hierarchy_destroy(fb_hierarchy* h);
 #define FB_CGC_FIXED 0        /* x += P x_c */
 #define FB_CGC_MIN_ENERGY 1   /* x += w P x_c, w = (d, c) / (A c, c) */
 #define FB_CGC_MIN_DEFECT 2   /* x += w P x_c, w = (d, A c) / (A c, A c) */
+/* the preconditioner of the Richardson smoother (JacobiPrecond, SORPrecond, SSORPrecond:
+ * kernel/solver/jacobi_precond.hpp, sor_precond.hpp:179-224, ssor_precond.hpp) */
+#define FB_SMOOTHER_JACOBI 0
+#define FB_SMOOTHER_SOR 1
+#define FB_SMOOTHER_SSOR 2
+/* the order of the SOR / SSOR sweeps */
+#define FB_SWEEP_SEQUENTIAL 0 /* the rows' dependency levels: the reference's generic sequential sweep, bit for bit */
+#define FB_SWEEP_COLOURED 1   /* greedy colours by ascending size: the reference's coloured CUDA sweeps (sor_precond.cu:26-41) */
 
 typedef struct
 {
@@ -244,6 +252,11 @@ typedef struct
                            correction, pre-smoothing + defect + restriction as one pass and
                            prolongation + post-smoothing as another (tiles with halos recomputed in
                            shared memory); results are bitwise those of one pass per step */
+  int smoother;         /* FB_SMOOTHER_JACOBI (default; damping `omega`), FB_SMOOTHER_SOR or FB_SMOOTHER_SSOR:
+                           the Richardson smoother's preconditioner; SOR / SSOR need FB_ORDER_NATIVE and the
+                           fixed coarse-grid correction, and run without the tail kernels */
+  double smoother_omega;/* SOR / SSOR damping (SORPrecond omega; default 1) */
+  int sweep_colouring;  /* FB_SWEEP_SEQUENTIAL (default) or FB_SWEEP_COLOURED */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
