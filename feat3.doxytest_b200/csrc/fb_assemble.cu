@@ -1,4 +1,5 @@
-// Q1 assembly on the uniformly refined unit square, on the device: the set-up step before the
+// Q1 assembly on the uniformly refined unit square (and, for the Laplacian, the unit cube), on
+// the device: the set-up step before the
 // solve path (the reference assembles on the host: kernel/assembly/domain_assembler_helpers.hpp,
 // kernel/assembly/common_operators.hpp:36, common_functionals.hpp:33, with the 3x3 Gauss rule that
 // "auto-degree:5" selects).  Vertices are numbered lexicographically ((2^L+1)^2 of them); the
@@ -238,6 +239,181 @@ namespace as
       }
   }
 
+  // ---------------------------------------------------------------- 3D (unit cube, hexahedra)
+  // Trilinear Q1 on [-1,1]^3 with the 3x3x3 Gauss rule (q = 9 qx + 3 qy + qz), local vertex
+  // v = bx + 2 by + 4 bz; the Laplace element matrix is the same for every cell (h/2 times the
+  // reference one), so only the load vector needs per-cell work.
+  struct Ref3
+  {
+    double xq[3], wq[3];
+    double val[27][8];      // phi_v at quad point q
+    double kloc[8][8];      // element stiffness of the reference element scaled to cells of size h = 1
+  };
+  __constant__ Ref3 c_ref3;
+
+  // per cell: the 8 load-vector contributions of a sum of Gaussians (rows c_x, c_y, c_z, w, a)
+  __global__ void k_cells3(int N, double h, int ng, const double* __restrict__ gauss, double* __restrict__ fe)
+  {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(c >= (long long)N * N * N)
+      return;
+    const int cx = int(c % N), cy = int((c / N) % N), cz = int(c / ((long long)N * N));
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for(int qx = 0; qx < 3; ++qx)
+      for(int qy = 0; qy < 3; ++qy)
+        for(int qz = 0; qz < 3; ++qz)
+        {
+          const int q = qx * 9 + qy * 3 + qz;
+          const double x = (double(cx) + (1.0 + c_ref3.xq[qx]) / 2.0) * h;
+          const double y = (double(cy) + (1.0 + c_ref3.xq[qy]) / 2.0) * h;
+          const double z = (double(cz) + (1.0 + c_ref3.xq[qz]) / 2.0) * h;
+          double f = 0.0;
+          for(int g = 0; g < ng; ++g)
+          {
+            const double dx = x - gauss[5 * g + 0], dy = y - gauss[5 * g + 1], dz = z - gauss[5 * g + 2];
+            const double w = gauss[5 * g + 3];
+            f += gauss[5 * g + 4] * exp(-(dx * dx + dy * dy + dz * dz) / (2.0 * w * w));
+          }
+          const double wf = f * (c_ref3.wq[qx] * c_ref3.wq[qy] * c_ref3.wq[qz]);
+          for(int a = 0; a < 8; ++a)
+            acc[a] += wf * c_ref3.val[q][a];
+        }
+    const double sc = (h / 2.0) * (h / 2.0) * (h / 2.0);
+    for(int a = 0; a < 8; ++a)
+      fe[size_t(c) * 8 + a] = sc * acc[a];
+  }
+
+  // per vertex: the 27-point stiffness row (sorted neighbours) and the load entry, cells in
+  // ascending index order
+  __global__ void k_vertices3(int N, double h, const double* __restrict__ fe, const uint64_t* __restrict__ rp,
+    double* __restrict__ vals, double* __restrict__ rhs)
+  {
+    const long long n1 = N + 1;
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if(v >= n1 * n1 * n1)
+      return;
+    const int ix = int(v % n1), iy = int((v / n1) % n1), iz = int(v / (n1 * n1));
+    if(vals)
+    {
+      uint64_t pos = rp[v];
+      for(int dz = -1; dz <= 1; ++dz)
+        for(int dy = -1; dy <= 1; ++dy)
+          for(int dx = -1; dx <= 1; ++dx)
+          {
+            const int jx = ix + dx, jy = iy + dy, jz = iz + dz;
+            if(jx < 0 || jy < 0 || jz < 0 || jx > N || jy > N || jz > N)
+              continue;
+            double s = 0.0;
+            for(int cz = max(max(iz, jz) - 1, 0); cz <= min(min(iz, jz), N - 1); ++cz)
+              for(int cy = max(max(iy, jy) - 1, 0); cy <= min(min(iy, jy), N - 1); ++cy)
+                for(int cx = max(max(ix, jx) - 1, 0); cx <= min(min(ix, jx), N - 1); ++cx)
+                {
+                  const int a = (ix - cx) + 2 * (iy - cy) + 4 * (iz - cz);
+                  const int b = (jx - cx) + 2 * (jy - cy) + 4 * (jz - cz);
+                  s += h * c_ref3.kloc[a][b];
+                }
+            vals[pos++] = s;
+          }
+    }
+    if(rhs)
+    {
+      double s = 0.0;
+      for(int cz = max(iz - 1, 0); cz <= min(iz, N - 1); ++cz)
+        for(int cy = max(iy - 1, 0); cy <= min(iy, N - 1); ++cy)
+          for(int cx = max(ix - 1, 0); cx <= min(ix, N - 1); ++cx)
+            s += fe[((size_t(cz) * N + cy) * N + cx) * 8 + (ix - cx) + 2 * (iy - cy) + 4 * (iz - cz)];
+      const bool boundary = ix == 0 || iy == 0 || iz == 0 || ix == N || iy == N || iz == N;
+      rhs[v] = boundary ? 0.0 : s;
+    }
+  }
+
+  // Q1 prolongation level-1 -> level on the lexicographic vertices of the cube: per direction an
+  // even fine coordinate takes coarse i/2 (weight 1), an odd one (i-1)/2 and (i+1)/2 (1/2 each);
+  // entries in ascending coarse index.  Row pointer in closed form with S(i) = i + i/2 the entries
+  // of the coordinates before i on one line and W = S(N + 1).
+  __global__ void k_prolongation3(int Nf, uint64_t* __restrict__ rp, uint64_t* __restrict__ col,
+    double* __restrict__ val)
+  {
+    const uint64_t n1 = uint64_t(Nf) + 1, nc1 = uint64_t(Nf) / 2 + 1;
+    const uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(v >= n1 * n1 * n1)
+      return;
+    const uint64_t ix = v % n1, iy = (v / n1) % n1, iz = v / (n1 * n1);
+    const uint64_t W = n1 + uint64_t(Nf) / 2;
+    const uint64_t cx = 1 + (ix & 1), cy = 1 + (iy & 1), cz = 1 + (iz & 1);
+    const uint64_t off = (iz + iz / 2) * W * W + cz * (iy + iy / 2) * W + cz * cy * (ix + ix / 2);
+    rp[v] = off;
+    if(v + 1 == n1 * n1 * n1)
+      rp[v + 1] = off + cx * cy * cz;
+    const uint64_t x0 = ix / 2, y0 = iy / 2, z0 = iz / 2;
+    uint64_t e = off;
+    for(uint64_t c = 0; c < cz; ++c)
+      for(uint64_t b = 0; b < cy; ++b)
+        for(uint64_t a = 0; a < cx; ++a)
+        {
+          col[e] = ((z0 + c) * nc1 + (y0 + b)) * nc1 + (x0 + a);
+          val[e] = (cx == 2 ? 0.5 : 1.0) * (cy == 2 ? 0.5 : 1.0) * (cz == 2 ? 0.5 : 1.0);
+          ++e;
+        }
+  }
+
+  static bool ref3_ready[64] = {};
+  static fb_status upload_ref3()
+  {
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    if(dev >= 0 && dev < 64 && ref3_ready[dev])
+      return FB_OK;
+    Ref3 r;
+    const double g = std::sqrt(3.0 / 5.0);
+    const double xs[3] = {-g, 0.0, g}, ws[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+    for(int k = 0; k < 3; ++k)
+    {
+      r.xq[k] = xs[k];
+      r.wq[k] = ws[k];
+    }
+    double gr[27][8][3];
+    for(int qx = 0; qx < 3; ++qx)
+      for(int qy = 0; qy < 3; ++qy)
+        for(int qz = 0; qz < 3; ++qz)
+        {
+          const int q = qx * 9 + qy * 3 + qz;
+          const double p[3] = {xs[qx], xs[qy], xs[qz]};
+          for(int v = 0; v < 8; ++v)
+          {
+            double f[3], sg[3];
+            for(int d = 0; d < 3; ++d)
+            {
+              sg[d] = ((v >> d) & 1) ? 1.0 : -1.0;
+              f[d] = 1.0 + p[d] * sg[d];
+            }
+            r.val[q][v] = f[0] * f[1] * f[2] / 8.0;
+            gr[q][v][0] = sg[0] * f[1] * f[2] / 8.0;
+            gr[q][v][1] = sg[1] * f[0] * f[2] / 8.0;
+            gr[q][v][2] = sg[2] * f[0] * f[1] / 8.0;
+          }
+        }
+    // (h/2)^3 (2/h)^2 = h/2: the reference element's matrix times 1/2, times h in the vertex kernel
+    for(int a = 0; a < 8; ++a)
+      for(int b = 0; b < 8; ++b)
+      {
+        double s = 0.0;
+        for(int qx = 0; qx < 3; ++qx)
+          for(int qy = 0; qy < 3; ++qy)
+            for(int qz = 0; qz < 3; ++qz)
+            {
+              const int q = qx * 9 + qy * 3 + qz;
+              const double gg = gr[q][a][0] * gr[q][b][0] + gr[q][a][1] * gr[q][b][1] + gr[q][a][2] * gr[q][b][2];
+              s += ws[qx] * ws[qy] * ws[qz] * gg;
+            }
+        r.kloc[a][b] = 0.5 * s;
+      }
+    FB_CUDA(cudaMemcpyToSymbol(c_ref3, &r, sizeof(Ref3)));
+    if(dev >= 0 && dev < 64)
+      ref3_ready[dev] = true;
+    return FB_OK;
+  }
+
   static bool ref_ready[64] = {};
   static fb_status upload_ref()
   {
@@ -378,6 +554,94 @@ fb_status fb_q1_prolongation_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uin
   }
   cudaStream_t st = as_stream(stream);
   as::k_prolongation<<<unsigned((n1 * n1 + 255) / 256), 256, 0, st>>>(int(Nf), row_ptr, col_ind, values);
+  FB_LAUNCHED(1);
+  FB_CUDA(cudaStreamSynchronize(st));
+  return FB_OK;
+}
+
+fb_status fb_q1_pattern_3d(int level, uint64_t* nnz_out, uint64_t* row_ptr, uint64_t* col_ind)
+{
+  if(level < 0 || level > 8 || !nnz_out)
+  {
+    set_error("q1_pattern_3d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const int64_t N = int64_t(1) << level, n1 = N + 1;
+  uint64_t pos = 0;
+  if(row_ptr)
+    row_ptr[0] = 0;
+  for(int64_t iz = 0; iz <= N; ++iz)
+    for(int64_t iy = 0; iy <= N; ++iy)
+      for(int64_t ix = 0; ix <= N; ++ix)
+      {
+        for(int64_t dz = -1; dz <= 1; ++dz)
+          for(int64_t dy = -1; dy <= 1; ++dy)
+            for(int64_t dx = -1; dx <= 1; ++dx)
+            {
+              const int64_t jx = ix + dx, jy = iy + dy, jz = iz + dz;
+              if(jx < 0 || jy < 0 || jz < 0 || jx > N || jy > N || jz > N)
+                continue;
+              if(col_ind)
+                col_ind[pos] = uint64_t((jz * n1 + jy) * n1 + jx);
+              ++pos;
+            }
+        if(row_ptr)
+          row_ptr[uint64_t((iz * n1 + iy) * n1 + ix) + 1] = pos;
+      }
+  *nnz_out = pos;
+  return FB_OK;
+}
+
+fb_status fb_q1_assemble_3d(int level, int ngauss, const double* gauss, const uint64_t* row_ptr, double* values,
+  double* rhs, void* stream)
+{
+  if(level < 0 || level > 8 || (ngauss && !gauss) || ngauss < 0 || (values && !row_ptr) || (!values && !rhs))
+  {
+    set_error("q1_assemble_3d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  fb_status e = as::upload_ref3();
+  if(e != FB_OK)
+    return e;
+  const int N = 1 << level;
+  const double h = 1.0 / N;
+  cudaStream_t st = as_stream(stream);
+  double* fe = nullptr;
+  const long long cells = (long long)N * N * N, verts = (long long)(N + 1) * (N + 1) * (N + 1);
+  if(rhs)
+  {
+    FB_CUDA(cudaMallocAsync((void**)&fe, sizeof(double) * 8 * size_t(cells), st));
+    as::k_cells3<<<unsigned((cells + 127) / 128), 128, 0, st>>>(N, h, ngauss, gauss, fe);
+    FB_LAUNCHED(1);
+  }
+  as::k_vertices3<<<unsigned((verts + 255) / 256), 256, 0, st>>>(N, h, fe, row_ptr, values, rhs);
+  FB_LAUNCHED(1);
+  if(fe)
+    FB_CUDA(cudaFreeAsync(fe, st));
+  FB_CUDA(cudaStreamSynchronize(st));
+  return FB_OK;
+}
+
+fb_status fb_q1_prolongation_3d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind, double* values,
+  void* stream)
+{
+  if(level < 1 || level > 8 || !nnz)
+  {
+    set_error("q1_prolongation_3d: bad arguments");
+    return FB_ERR_ARG;
+  }
+  const uint64_t Nf = uint64_t(1) << level, n1 = Nf + 1;
+  const uint64_t cnt = n1 + Nf / 2;   // entries per fine line
+  *nnz = cnt * cnt * cnt;
+  if(!row_ptr && !col_ind && !values)
+    return FB_OK;
+  if(!row_ptr || !col_ind || !values)
+  {
+    set_error("q1_prolongation_3d: row_ptr, col_ind and values are all needed");
+    return FB_ERR_ARG;
+  }
+  cudaStream_t st = as_stream(stream);
+  as::k_prolongation3<<<unsigned((n1 * n1 * n1 + 255) / 256), 256, 0, st>>>(int(Nf), row_ptr, col_ind, values);
   FB_LAUNCHED(1);
   FB_CUDA(cudaStreamSynchronize(st));
   return FB_OK;

@@ -70,6 +70,9 @@ _PROTOS = {
     "fb_dot_f32": (I, [P, P, P, U64, P]),
     "fb_dot_f64_noalloc": (I, [P, P, P, U64, P]),
     "fb_solver_set_iteration_limits": (I, [P, I, I]),
+    "fb_q1_pattern_3d": (I, [I, P, P, P]),
+    "fb_q1_assemble_3d": (I, [I, I, P, P, P, P, P]),
+    "fb_q1_prolongation_3d": (I, [I, C.POINTER(C.c_uint64), P, P, P, P]),
     "fb_set_memory_f64": (I, [P, D, U64, P]),
     "fb_set_memory_f32": (I, [P, F, U64, P]),
     "fb_set_memory_u64": (I, [P, U64, U64, P]),

@@ -455,6 +455,20 @@ fb_status fb_q1_assemble_2d(int level, int kmodes, const double* xi, const doubl
 fb_status fb_q1_prolongation_2d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind, double* values,
                                 void* stream);
 
+/* The 3D counterparts for the Laplacian on the unit cube refined to level L (hexahedral Q1, 3x3x3
+ * Gauss rule, (2^L+1)^3 vertices numbered lexicographically, x fastest; L <= 8): the row-sorted
+ * 27-point pattern (host), the stiffness values in that pattern and / or the load vector of a sum
+ * of Gaussians (DEVICE gauss[ngauss][5] = c_x, c_y, c_z, w, a; boundary entries zeroed), and the
+ * prolongation level L-1 -> L (weights 1, 1/2, 1/4, 1/8, DEVICE arrays of nnz entries).
+ * Replace the reference's host assembly on RefinedUnitCubeFactory meshes
+ * (kernel/assembly/common_operators.hpp:36, kernel/assembly/grid_transfer.hpp:353-430 in 3D) in
+ * lexicographic numbering. */
+fb_status fb_q1_pattern_3d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind);
+fb_status fb_q1_assemble_3d(int level, int ngauss, const double* gauss, const uint64_t* row_ptr, double* values,
+                            double* rhs, void* stream);
+fb_status fb_q1_prolongation_3d(int level, uint64_t* nnz, uint64_t* row_ptr, uint64_t* col_ind, double* values,
+                                void* stream);
+
 /* f (sum of Gaussians, as above) and g = log kappa at the vertices of level L (DEVICE arrays of
  * (2^L+1)^2 doubles, lexicographic; either may be NULL): the inputs of the learned warm start. */
 fb_status fb_q1_sample_2d(int level, int kmodes, const double* xi, const double* eta, double s, int ngauss,

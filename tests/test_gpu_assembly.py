@@ -140,3 +140,79 @@ def test_prolongation_matches_host(featlib, cuda, level):
     assert np.array_equal(rp.cpu().numpy(), P.indptr.astype(np.int64))
     assert np.array_equal(ci.cpu().numpy(), P.indices.astype(np.int64))
     assert np.array_equal(v.cpu().numpy(), P.data)
+
+
+def test_pattern_3d_matches_host_assembler(featlib):
+    from featb200.assembly_gpu import q1_pattern_3d
+    for level in (0, 1, 2, 4):
+        rp, ci = q1_pattern_3d(level)
+        A = AS.stiffness(level, 3)
+        assert np.array_equal(rp, A.indptr.astype(np.uint64))
+        assert np.array_equal(ci, A.indices.astype(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [1, 3, 5])
+def test_assembly_3d_matches_host(featlib, cuda, level):
+    """The hexahedral Q1 Laplacian and the Gaussian load vector on the unit cube against the host
+    assembler (pinned to the reference's assembly by test_assembly)."""
+    torch = cuda
+    from featb200.assembly_gpu import Q1Assembler3D
+    gp = AS.gauss_params(70 + level, 3, width=(0.03, 0.12))
+    vals, b = Q1Assembler3D(level).assemble(gp)
+    torch.cuda.synchronize()
+    A = AS.stiffness(level, 3)
+    b_ref = AS.load_vector(level, lambda *xs: AS.gauss_eval(gp, *xs), 3)
+    b_ref[AS.boundary_dofs(level, 3).astype(np.int64)] = 0.0
+    v = vals.cpu().numpy()
+    assert np.abs(v - A.data).max() <= TOL * np.abs(A.data).max()
+    bb = b.cpu().numpy()
+    assert np.abs(bb - b_ref).max() <= TOL * max(np.abs(b_ref).max(), 1e-300)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [1, 2, 4])
+def test_prolongation_3d_matches_host(featlib, cuda, level):
+    from featb200.assembly_gpu import q1_prolongation_3d
+    rp, ci, v = q1_prolongation_3d(level)
+    P = AS.prolongation(level, 3)
+    assert np.array_equal(rp.cpu().numpy(), P.indptr.astype(np.int64))
+    assert np.array_equal(ci.cpu().numpy(), P.indices.astype(np.int64))
+    assert np.array_equal(v.cpu().numpy(), P.data)
+
+
+@pytest.mark.gpu
+def test_device_assembled_3d_hierarchy_solves(featlib, cuda, oracle_lib):
+    """A 3D level-5 hierarchy assembled entirely on the device (stiffness, load vector and
+    prolongations; R = P^T) gives the solve of the host-assembled one."""
+    from featb200.assembly_gpu import Q1Assembler3D, q1_prolongation_3d
+    from helpers import rel_err
+    import scipy.sparse as sp
+    fb = featlib
+    L = 5
+    gp = AS.gauss_params(9, 3, width=(0.03, 0.12))
+    host_levels, b_host = AS.poisson_hierarchy(L, 3, rhs="gauss", gauss=gp)
+    levels = []
+    b_dev = None
+    for lv in range(L, 0, -1):
+        asm = Q1Assembler3D(lv)
+        vals, b = asm.assemble(gp if lv == L else None, rhs=(lv == L))
+        n = asm.n
+        A = sp.csr_matrix((vals.cpu().numpy(), asm.col_ind.astype(np.int64), asm.row_ptr.astype(np.int64)), shape=(n, n))
+        d = {"matrix": fb.SparseMatrixCSR.from_scipy(A), "filter": fb.UnitFilter(AS.boundary_dofs(lv, 3))}
+        if lv == L:
+            b_dev = b.cpu().numpy()
+        if lv > 1:
+            rp, ci, v = q1_prolongation_3d(lv)
+            nc = (2 ** (lv - 1) + 1) ** 3
+            P = sp.csr_matrix((v.cpu().numpy(), ci.cpu().numpy(), rp.cpu().numpy()), shape=(n, nc))
+            d["transfer"] = fb.Transfer(fb.SparseMatrixCSR.from_scipy(P), fb.SparseMatrixCSR.from_scipy(P.T.tocsr()))
+        levels.append(d)
+    assert rel_err(b_dev, b_host) <= 1e-12
+    s_dev = fb.build_pcg_multigrid(levels)
+    s_host = fb.build_pcg_multigrid(host_levels)
+    x_dev, x_host = fb.DenseVector(b_dev.size), fb.DenseVector(b_host.size)
+    assert fb.solve(s_dev, x_dev, fb.DenseVector(b_dev)) == fb.Status.success
+    assert fb.solve(s_host, x_host, fb.DenseVector(b_host)) == fb.Status.success
+    assert s_dev.get_num_iter() == s_host.get_num_iter()
+    assert rel_err(x_dev.elements, x_host.elements) <= 1e-10
