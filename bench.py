@@ -492,8 +492,11 @@ PASS_KERNELS = {
     "mg_post2": "k_tma_pass<OpPost2>: post-smoothing step 2 with the PCG's z and r.z",
     "mg_down": "k_fz_down: fused pre-smoothing step 2 + defect + restriction (structured 2D level)",
     "mg_up": "k_fz_up: fused prolongation + post-smoothing with the PCG's z and r.z (structured 2D level)",
+    "mg_sdown": "k_fs_down: the fused down pass streamed through bands of coarse rows (structured 2D level)",
+    "mg_sup": "k_fs_up: the fused up pass streamed through bands of coarse rows (structured 2D level)",
 }
 FUSED_PASSES = ("mg_down", "mg_up")
+STREAM_PASSES = ("mg_sdown", "mg_sup")
 
 
 def pass_table(solver, levels, precision, reps=20):
@@ -528,21 +531,26 @@ def pass_table(solver, levels, precision, reps=20):
         "mg_up": (csr(nnz, n, sv) + csr(nnz_p, n, sv) + nc * sx + n * sx * 3 + n * 16,
                   "CSR of A once + CSR of P + x_c gathered + x2, b, D read (s_x) + r read and z written (FP64)"),
     }
+    alg["mg_sdown"] = alg["mg_down"]
+    alg["mg_sup"] = alg["mg_up"]
     out = {}
     fused = True
     for k, (by, definition) in alg.items():
         try:
             ms, stored = solver.time_kernel(k, reps=reps, flush_l2=True)
         except Exception:
-            if k in FUSED_PASSES:        # the finest level is not a structured grid: no fused passes
+            if k in FUSED_PASSES or k in STREAM_PASSES:   # the finest level is not a structured grid
                 fused = False
                 continue
             raise
         out[k] = {"kernel": PASS_KERNELS[k], "us": ms * 1e3, "csr_bytes": by, "csr_definition": definition,
                   "csr_gbs": by / (ms * 1e-3) / 1e9, "stored_bytes": stored, "stored_gbs": stored / (ms * 1e-3) / 1e9}
     # which of them the solve launches on the finest level
+    tiled = fused and solver.cfg.fused >= n
+    streamed = fused and not tiled and 0 < solver.cfg.streamed <= n
     for k in out:
-        out[k]["in_solve"] = k == "pcg_spmv" or ((k in FUSED_PASSES) == (fused and solver.cfg.fused >= n))
+        kind = "tiled" if k in FUSED_PASSES else ("streamed" if k in STREAM_PASSES else "unfused")
+        out[k]["in_solve"] = k == "pcg_spmv" or kind == ("tiled" if tiled else ("streamed" if streamed else "unfused"))
     return out
 
 
@@ -635,6 +643,9 @@ def main():
     ap.add_argument("--fused-rows", type=int, default=None,
                     help="structured 2D levels with at most this many rows run fused V(2,2) passes "
                          "(default: the library's threshold; 0 = one pass per step everywhere)")
+    ap.add_argument("--streamed-rows", type=int, default=None,
+                    help="structured 2D levels above the fused threshold with at least this many rows run "
+                         "the streamed fused passes (default: the library's threshold; 0 = never)")
     ap.add_argument("--pdl", type=int, choices=[0, 1], default=1,
                     help="programmatic dependent launch of the solve's kernels (1) or plain stream order (0)")
     ap.add_argument("--cycle", choices=["V", "F", "W"], default="V",
@@ -685,7 +696,8 @@ def main():
     solver = fb.build_pcg_multigrid(levels, precision=precision, ordering=args.ordering, tail_rows=args.tail_rows,
                                     use_graph=not args.profile_solves, tma_window=args.tma_window,
                                     cluster_rows=args.cluster_rows, tma_rows=args.tma_rows, cycle=args.cycle,
-                                    diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows)
+                                    diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows,
+                                    streamed=args.streamed_rows)
     info_lv = solver.level_info()
     if args.profile_kernel:
         ms_k, by_k = solver.time_kernel(args.profile_kernel, reps=3, flush_l2=True)
@@ -758,7 +770,8 @@ def main():
     extra = {}
     if not args.no_plain and precision != "f64":
         plain = fb.build_pcg_multigrid(levels, precision="f64", ordering=args.ordering, tma_window=args.tma_window,
-                                       diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows)
+                                       diagonal=args.diagonal, pdl=args.pdl, fused=args.fused_rows,
+                                    streamed=args.streamed_rows)
         pt = []
         for k in range(args.warmup + max(3, args.steps // 2)):
             flush()

@@ -515,6 +515,7 @@ namespace fb
 } // namespace fb
 
 #include "fb_fused.cuh"
+#include "fb_stream.cuh"
 #include "fb_sor.cuh"
 
 namespace fb
@@ -1358,6 +1359,9 @@ namespace fb
       sc->alpha = sc->gamma / total;
   }
 
+  constexpr int PCGX_U = 4;        // rows per thread in flight in k_pcg_x
+  constexpr int PCGX_BPS = 4;      // its resident blocks per SM at 64 registers (grid = one wave)
+
   // x += alpha p; r -= alpha q; ||r||, stopping test (iterative.hpp:492-507,795-879); the next
   // V-cycle input (FP64: sol1 = F(D .* r); FP32: b = S(r * scale), sol1 = F(D .* b)).
   template<typename S, bool CONVERT>
@@ -1376,15 +1380,40 @@ namespace fb
     }
     const double alpha = sc->alpha;
     const double scale = CONVERT ? pow2_near_inverse(sc->def_cur) : 1.0;
-    const uint32_t i = blockIdx.x * NT + threadIdx.x;
+    // grid-stride over the rows, PCGX_U rows per thread in flight: all loads of a group go out
+    // before its arithmetic
+    const uint32_t stride = gridDim.x * NT;
     double sq = 0.0;
-    if(i < n)
+    for(uint32_t i0 = blockIdx.x * NT + threadIdx.x; i0 < n; i0 += PCGX_U * stride)
     {
-      x[i] = add(x[i], mul(alpha, p[i]));
-      const double rv = add(r[i], mul(-alpha, q[i]));
-      r[i] = rv;
-      mg_input<S>(i, rv, dm[i] != 0, scale, CONVERT ? bt : (S*)nullptr, x1, dinv);
-      sq = mul(rv, rv);
+      double xv[PCGX_U], rv[PCGX_U], pv[PCGX_U], qv[PCGX_U];
+      bool dd[PCGX_U];
+      #pragma unroll
+      for(int u = 0; u < PCGX_U; ++u)
+      {
+        const uint32_t i = i0 + uint32_t(u) * stride;
+        if(i < n)
+        {
+          xv[u] = x[i];
+          rv[u] = r[i];
+          pv[u] = p[i];
+          qv[u] = q[i];
+          dd[u] = dm[i] != 0;
+        }
+      }
+      #pragma unroll
+      for(int u = 0; u < PCGX_U; ++u)
+      {
+        const uint32_t i = i0 + uint32_t(u) * stride;
+        if(i < n)
+        {
+          x[i] = add(xv[u], mul(alpha, pv[u]));
+          const double rn = add(rv[u], mul(-alpha, qv[u]));
+          r[i] = rn;
+          mg_input<S>(i, rn, dd[u], scale, CONVERT ? bt : (S*)nullptr, x1, dinv);
+          sq += mul(rn, rn);
+        }
+      }
     }
     double total;
     if(grid_sum_last<NT>(sq, slot, sh, total))
@@ -1520,6 +1549,59 @@ namespace fb
     return true;
   }
 
+  // every entry of P's row (x, y) couples the coarse vertex (x / 2 + dx, y / 2 + dy), dx, dy in {0, 1}
+  // (integer halves), and the rows have at most FZ_KP entries: the streamed up pass stages the
+  // coarse rows y / 2 .. y / 2 + 1 around each fine row
+  static bool prolongation_local(const HostCsr& P, uint32_t w)
+  {
+    if(w % 2 == 0)
+      return false;
+    const uint32_t wc = (w + 1) / 2;
+    if(P.rows != w * w || P.cols != wc * wc)
+      return false;
+    for(uint32_t i = 0; i < P.rows; ++i)
+    {
+      const uint32_t x = i % w, y = i / w;
+      if(P.rp[i + 1] - P.rp[i] > uint32_t(FZ_KP))
+        return false;
+      for(uint32_t k = P.rp[i]; k < P.rp[i + 1]; ++k)
+      {
+        const uint32_t cx = P.col[k] % wc, cy = P.col[k] / wc;
+        if(cx < x / 2 || cx > x / 2 + 1 || cy < y / 2 || cy > y / 2 + 1)
+          return false;
+      }
+    }
+    return true;
+  }
+
+  // tiles of the streamed passes on a W x W level: at most FS_TC_MAX coarse columns, evened out
+  // across the grid, and bands of coarse rows sized so that the grid fills one wave of bps blocks
+  // per SM
+  static FsGeom fs_geom(uint32_t W, int nsm, int bps)
+  {
+    FsGeom g;
+    g.W = int(W);
+    g.Wc = int((W + 1) / 2);
+    g.ntx = (g.Wc + FS_TC_MAX - 1) / FS_TC_MAX;
+    g.TC = (g.Wc + g.ntx - 1) / g.ntx;
+    const int nby = std::max(1, std::max(1, nsm) * std::max(1, bps) / g.ntx);
+    g.TR = (g.Wc + nby - 1) / nby;
+    return g;
+  }
+  static uint32_t fs_grid(const FsGeom& g) { return uint32_t(g.ntx) * uint32_t((g.Wc + g.TR - 1) / g.TR); }
+
+  // every vertex on the boundary of the w x w grid is a Dirichlet vertex (the streamed passes read
+  // the out-of-grid neighbours of boundary rows unguarded and rely on the masks to discard them)
+  static bool boundary_dirichlet(const std::vector<uint8_t>& dm, uint32_t w)
+  {
+    if(w < 2 || dm.size() != size_t(w) * w)
+      return false;
+    for(uint32_t k = 0; k < w; ++k)
+      if(!dm[k] || !dm[size_t(w - 1) * w + k] || !dm[size_t(k) * w] || !dm[size_t(k) * w + w - 1])
+        return false;
+    return true;
+  }
+
   template<typename V> DCsr<V> view(const DevMat& m)
   {
     return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw, m.doff};
@@ -1538,6 +1620,8 @@ namespace fb
     uint32_t gw = 0;         // grid width when the level is a structured 2D grid (fused passes), else 0
     bool fz_down = false;    // the fused down pass applies (structured A and restriction)
     bool fz_up = false;      // the fused up pass applies (structured A)
+    bool fs_up = false;      // the streamed up pass applies (also a local prolongation)
+    bool fs_ok = false;      // the streamed passes apply (structured, Dirichlet boundary)
   };
 
   // a level's SOR / SSOR sweep data: the full system matrix in CSR (stored order, Dirichlet rows
@@ -1671,6 +1755,7 @@ struct fb_solver
   int max_iter_cap = 0;   // max_iter at creation: the defect history holds max_iter + 2 entries
   void* vc_top = nullptr; // buffer that holds the finest level's result after a standalone V-cycle
   uint32_t slot_cap = 0;  // blocks whose (two) partial sums the reduction slot holds
+  int fs_bps_down = 1, fs_bps_up = 1;   // resident blocks per SM of the streamed passes
   int tail_first = -1;    // first level handled by the single-block tail kernel, -1 = none
   int ctail_first = -1;   // first level handled by the cluster tail kernel, -1 = none
   double* cred = nullptr; // cluster tail: per-block partial sums (2 * MAX_TAIL * CT_CS)
@@ -1897,6 +1982,12 @@ namespace fb
       const cudaError_t e = cudaLaunchKernelEx(&lc, k, std::forward<A>(a)...);
       if(e != cudaSuccess && s->launch_err == cudaSuccess)
         s->launch_err = e;
+    }
+
+    // k_pcg_x: one wave of PCGX_BPS blocks per SM at most
+    unsigned int pcgx_grid(uint32_t n) const
+    {
+      return std::min(blocks(n), unsigned(std::max(1, s->nsm) * PCGX_BPS));
     }
 
     // column index bytes per entry
@@ -2165,6 +2256,63 @@ namespace fb
         go(k_fz_up<V, S, false>, fused_up_grid(l), FZ_NT, 0, view<V>(f.A), view<V>(f.P), f.gw, (const S*)xin, xc,
           (S*)xout, (const S*)f.b, (const S*)f.dinv, f.dm, f.skip_post, (double*)nullptr, (const double*)nullptr,
           s->slot, s->sc);
+      ++launches;
+      bytes += f.A.bytes + f.P.bytes + double(f.P.cols) * sizeof(S) + double(f.n) * (4.0 * sizeof(S) + 1.0) +
+               (top ? 16.0 * double(f.n) : 0.0);
+      if(!top)
+        xcur[size_t(l)] = xout;
+    }
+
+    // the streamed passes apply to structured levels above the fused threshold with at least
+    // cfg.streamed rows, in the cycles the fused passes serve
+    bool stream_level(int l) const
+    {
+      const uint32_t n = s->lv[size_t(l)].n;
+      return s->cfg.streamed > 0 && s->cfg.smoother == FB_SMOOTHER_JACOBI && n >= uint32_t(s->cfg.streamed) &&
+             (s->cfg.fused <= 0 || n > uint32_t(s->cfg.fused)) && s->cfg.cycle == FB_CYCLE_V &&
+             s->cfg.adapt_cgc == FB_CGC_FIXED && s->cfg.smooth_steps == 2;
+    }
+    FsGeom stream_geom(int l, bool up) const
+    {
+      return fs_geom(s->lv[size_t(l)].gw, s->nsm, up ? s->fs_bps_up : s->fs_bps_down);
+    }
+
+    // the down pass of level l in its streamed form (k_fs_down); buffers as in fused_down
+    void streamed_down(int l, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      DevLevel& c = L(l + 1);
+      const bool coarsest = (l + 2 == s->nlev);
+      const FsGeom g = stream_geom(l, false);
+      if(!dry)
+        go(k_fs_down<V, S>, fs_grid(g), FS_NT, FsLay<V, S, false, false>::SMEM, view<V>(f.A), view<V>(f.R), g,
+          (const S*)f.b, (const S*)f.x, (S*)f.x2, (const S*)f.dinv, f.dm, (const int*)f.skip_pre, (S*)c.b,
+          coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.skip_pre, s->slot, s->err,
+          (const Scalars*)s->sc);
+      ++launches;
+      bytes += f.A.bytes + f.R.bytes + double(f.n) * (4.0 * sizeof(S) + 1.0) +
+               double(c.n) * ((coarsest ? 1.0 : 3.0) * sizeof(S) + 1.0);
+      xcur[size_t(l)] = f.x2;
+    }
+
+    // the up pass of level l in its streamed form (k_fs_up); buffers as in fused_up
+    void streamed_up(int l, bool top, std::vector<void*>& xcur)
+    {
+      DevLevel& f = L(l);
+      void* xin = xcur[size_t(l)];
+      void* xout = (xin == f.x) ? f.x2 : f.x;
+      const S* xc = (const S*)xcur[size_t(l + 1)];
+      const FsGeom g = stream_geom(l, true);
+      if(dry)
+        ;
+      else if(top)
+        go(k_fs_up<V, S, true>, fs_grid(g), FS_NT, FsLay<V, S, true, true>::SMEM, view<V>(f.A), view<V>(f.P), g,
+          (const S*)xin, xc, (S*)nullptr, (const S*)f.b, (const S*)f.dinv, f.dm, f.skip_post, s->z,
+          (const double*)s->r, s->slot, s->err, s->sc);
+      else
+        go(k_fs_up<V, S, false>, fs_grid(g), FS_NT, FsLay<V, S, true, false>::SMEM, view<V>(f.A), view<V>(f.P), g,
+          (const S*)xin, xc, (S*)xout, (const S*)f.b, (const S*)f.dinv, f.dm, f.skip_post, (double*)nullptr,
+          (const double*)nullptr, s->slot, s->err, s->sc);
       ++launches;
       bytes += f.A.bytes + f.P.bytes + double(f.P.cols) * sizeof(S) + double(f.n) * (4.0 * sizeof(S) + 1.0) +
                (top ? 16.0 * double(f.n) : 0.0);
@@ -2528,6 +2676,21 @@ namespace fb
           i += 2;
           continue;
         }
+        // the same on the large structured levels, streamed
+        if(e.op == EV_PRE && stream_level(l) && L(l).fs_ok && L(l).fz_down && fs_grid(stream_geom(l, false)) <= s->slot_cap &&
+           i + 2 < e1 && ev[i + 1].op == EV_DEF && ev[i + 1].lvl == l && ev[i + 2].op == EV_RES && ev[i + 2].lvl == l)
+        {
+          streamed_down(l, xcur);
+          i += 3;
+          continue;
+        }
+        if(e.op == EV_PRO && stream_level(l) && L(l).fs_ok && L(l).fs_up && fs_grid(stream_geom(l, true)) <= s->slot_cap &&
+           i + 1 < e1 && ev[i + 1].lvl == l && (ev[i + 1].op == EV_POST || ev[i + 1].op == EV_POST_TOP))
+        {
+          streamed_up(l, ev[i + 1].op == EV_POST_TOP && pcg_top, xcur);
+          i += 2;
+          continue;
+        }
         if(s->cfg.smoother != FB_SMOOTHER_JACOBI && (e.op == EV_PRE || e.op == EV_POST || e.op == EV_POST_TOP))
         {
           if(e.op == EV_PRE)
@@ -2601,10 +2764,10 @@ namespace fb
       if(dry)
         ;
       else if(f64)
-        go(k_pcg_x<S, false>, blocks(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
+        go(k_pcg_x<S, false>, pcgx_grid(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
           (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
       else
-        go(k_pcg_x<S, true>, blocks(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)t.b, (S*)t.x,
+        go(k_pcg_x<S, true>, pcgx_grid(t.n), NT, 0, s->x, s->r, s->p, s->q, t.dm, (S*)t.b, (S*)t.x,
           (const S*)t.dinv, t.skip_pre, s->hist, t.n, s->slot, s->sc, cond);
       launches += 3;
       bytes += double(t.n) * 8 * (first ? 2 : 3);                                    // P
@@ -2612,6 +2775,23 @@ namespace fb
       bytes += double(t.n) * 8 * 6 + double(t.n) * (f64 ? 16 : 12) + t.n;             // X
     }
   };
+
+  // dynamic shared memory of the streamed passes and their resident blocks per SM
+  template<typename V, typename S>
+  static fb_status fs_occupancy(fb_solver* s)
+  {
+    typedef FsLay<V, S, false, false> LD;
+    typedef FsLay<V, S, true, true> LU;
+    typedef FsLay<V, S, true, false> LN;
+    FB_CUDA(cudaFuncSetAttribute(k_fs_down<V, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LD::SMEM)));
+    FB_CUDA(cudaFuncSetAttribute(k_fs_up<V, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LU::SMEM)));
+    FB_CUDA(cudaFuncSetAttribute(k_fs_up<V, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LN::SMEM)));
+    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->fs_bps_down, k_fs_down<V, S>, FS_NT, LD::SMEM));
+    FB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->fs_bps_up, k_fs_up<V, S, true>, FS_NT, LU::SMEM));
+    s->fs_bps_down = std::max(1, s->fs_bps_down);
+    s->fs_bps_up = std::max(1, s->fs_bps_up);
+    return FB_OK;
+  }
 
   template<typename V, typename S, class Op>
   static fb_status set_tma_attr_dg(int mx)
@@ -2797,6 +2977,7 @@ void fb_solver_config_default(fb_solver_config* c)
   c->smoother = FB_SMOOTHER_JACOBI;
   c->smoother_omega = 1.0;
   c->sweep_colouring = FB_SWEEP_SEQUENTIAL;
+  c->streamed = 0;
 }
 
 fb_status fb_hierarchy_create(fb_hierarchy** out, int num_levels)
@@ -2900,7 +3081,7 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
      cfg.cycle < FB_CYCLE_V || cfg.cycle > FB_CYCLE_W || cfg.adapt_cgc < FB_CGC_FIXED ||
      cfg.adapt_cgc > FB_CGC_MIN_DEFECT || cfg.smoother < FB_SMOOTHER_JACOBI || cfg.smoother > FB_SMOOTHER_SSOR ||
      (cfg.smoother != FB_SMOOTHER_JACOBI && !(cfg.smoother_omega > 0.0)) || cfg.sweep_colouring < FB_SWEEP_SEQUENTIAL ||
-     cfg.sweep_colouring > FB_SWEEP_COLOURED)
+     cfg.sweep_colouring > FB_SWEEP_COLOURED || cfg.streamed < 0)
   {
     set_error("solver_create: bad configuration");
     return FB_ERR_ARG;
@@ -2966,6 +3147,9 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       const std::vector<uint32_t>& pc = s->perms[size_t(l + 1)];
       D.fz_down = D.gw != 0 && D.R.col && !D.R.dcol && D.R.kmax <= uint32_t(FZ_KR) &&
                   restriction_local(permute(H.R, pc, inv_f), D.gw);
+      D.fs_up = D.fz_up &&
+                prolongation_local(permute(H.P, pf, pc.empty() ? std::vector<uint32_t>() : inverse_perm(pc)), D.gw);
+      D.fs_ok = D.gw != 0 && boundary_dirichlet(dms[size_t(l)], D.gw);
     }
     const std::vector<uint8_t>& dm = dms[size_t(l)];
     FB_TRY(dalloc(s.get(), (void**)&D.dm, D.n));
@@ -3037,6 +3221,26 @@ fb_status fb_solver_create(fb_solver** out, fb_hierarchy* h, const fb_solver_con
       continue;
     const uint32_t tu = (D.gw + FZ_UP_TILE - 1) / FZ_UP_TILE, td = ((D.gw + 1) / 2 + FZ_DOWN_TILE - 1) / FZ_DOWN_TILE;
     max_blocks = std::max(max_blocks, std::max(tu * tu, td * td));
+  }
+  // the streamed passes' grids (tiles sized for the resident blocks of one wave)
+  {
+    fb_status fe = FB_OK;
+    if(prec == FB_PREC_F64)
+      fe = fs_occupancy<double, double>(s.get());
+    else if(prec == FB_PREC_F32)
+      fe = fs_occupancy<float, float>(s.get());
+    else
+      fe = fs_occupancy<bf16_t, float>(s.get());
+    if(fe != FB_OK)
+      return fe;
+    for(int l = 0; l + 1 < s->nlev; ++l)
+    {
+      const DevLevel& D = s->lv[size_t(l)];
+      if(!D.gw)
+        continue;
+      max_blocks = std::max(max_blocks, fs_grid(fs_geom(D.gw, s->nsm, s->fs_bps_down)));
+      max_blocks = std::max(max_blocks, fs_grid(fs_geom(D.gw, s->nsm, s->fs_bps_up)));
+    }
   }
   s->slot_cap = max_blocks;
   FB_TRY(dalloc(s.get(), (void**)&s->slot.partials, sizeof(double) * 2 * (max_blocks + 1)));
@@ -3451,6 +3655,18 @@ namespace fb
       xcur[1] = s->lv[1].x2;
       l.fused_up(0, true, xcur);
     }
+    else if(which == FB_KERNEL_MG_SDOWN)
+    {
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      l.streamed_down(0, xcur);
+    }
+    else if(which == FB_KERNEL_MG_SUP)
+    {
+      std::vector<void*> xcur(static_cast<size_t>(s->nlev), nullptr);
+      xcur[0] = t.x2;
+      xcur[1] = s->lv[1].x2;
+      l.streamed_up(0, true, xcur);
+    }
     else if(which == FB_KERNEL_MG_RESTRICT)
       l.restrict_to(0);
     else if(which == FB_KERNEL_MG_PROLONG)
@@ -3493,11 +3709,13 @@ namespace fb
       }
       case FB_KERNEL_MG_PROLONG: return csr(t.P, 1, 1) + n;
       case FB_KERNEL_MG_DOWN:
+      case FB_KERNEL_MG_SDOWN:
       {
         const bool coarsest = s->nlev == 2;
         return t.A.bytes + t.R.bytes + n * (4.0 * sx + 1.0) + double(s->lv[1].n) * ((coarsest ? 1.0 : 3.0) * sx + 1.0);
       }
-      case FB_KERNEL_MG_UP: return t.A.bytes + t.P.bytes + double(t.P.cols) * sx + n * (4.0 * sx + 1.0) + 16.0 * n;
+      case FB_KERNEL_MG_UP:
+      case FB_KERNEL_MG_SUP: return t.A.bytes + t.P.bytes + double(t.P.cols) * sx + n * (4.0 * sx + 1.0) + 16.0 * n;
       default: return 0.0;
     }
   }
@@ -3508,9 +3726,11 @@ extern "C" {
 fb_status fb_solver_time_kernel(fb_solver* s, int which, int reps, int flush_l2, double* avg_ms,
   double* bytes_per_launch)
 {
-  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_UP ||
+  if(!s || !avg_ms || !bytes_per_launch || reps < 1 || which < FB_KERNEL_PCG_SPMV || which > FB_KERNEL_MG_SUP ||
      (which == FB_KERNEL_MG_DOWN && (s->nlev < 2 || !s->lv[0].fz_down)) ||
      (which == FB_KERNEL_MG_UP && (s->nlev < 2 || !s->lv[0].fz_up)) ||
+     (which == FB_KERNEL_MG_SDOWN && (s->nlev < 2 || !s->lv[0].fz_down || !s->lv[0].fs_ok)) ||
+     (which == FB_KERNEL_MG_SUP && (s->nlev < 2 || !s->lv[0].fs_up || !s->lv[0].fs_ok)) ||
      (which == FB_KERNEL_MG_TAIL && s->tail_first < 0 && s->ctail_first < 0) ||
      (which >= FB_KERNEL_MG_SMOOTH && s->nlev < 2) ||
      (which >= FB_KERNEL_MG_SMOOTH && (s->tail_first == 0 || s->ctail_first == 0)))

@@ -35,7 +35,8 @@ class SolverConfig(C.Structure):
                 ("cluster_rows", C.c_int), ("cycle", C.c_int), ("tma_window", C.c_int),
                 ("diagonal", C.c_int), ("pdl", C.c_int),
                 ("adapt_cgc", C.c_int), ("fused", C.c_int), ("smoother", C.c_int),
-                ("smoother_omega", C.c_double), ("sweep_colouring", C.c_int)]
+                ("smoother_omega", C.c_double), ("sweep_colouring", C.c_int),
+                ("streamed", C.c_int)]
 
 
 class StoragePlan(C.Structure):

@@ -291,6 +291,13 @@ class PCG:
         one for prolongation and post-smoothing."""
         self.cfg.fused = (2 ** 31 - 1) if rows is True else int(rows)
 
+    def set_streamed(self, rows):
+        """Streamed fused passes on structured 2D levels with more rows than the `fused` threshold
+        and at least `rows` rows (True = every such level, False / 0 = none): the same two fused
+        passes, swept row by row through bands of coarse rows with their rows staged in shared
+        memory."""
+        self.cfg.streamed = 1 if rows is True else int(rows)
+
     def set_smoother(self, kind="jacobi", omega=1.0, sweep="sequential"):
         """The Richardson smoother's preconditioner: "jacobi" (JacobiPrecond with the hierarchy's
         damping), "sor" or "ssor" (SORPrecond / SSORPrecond with damping `omega`); SOR / SSOR sweep
@@ -389,10 +396,12 @@ class PCG:
     def time_kernel(self, which="pcg_spmv", reps=20, flush_l2=True):
         """Mean launch time (ms) and stored bytes per launch of one solver kernel timed alone:
         pcg_spmv, mg_defect, mg_smooth, mg_post1, mg_post2, mg_restrict, mg_prolong (finest-level
-        passes), mg_down / mg_up (the fused passes of a structured finest level), mg_tail (the
+        passes), mg_down / mg_up (the fused passes of a structured finest level), mg_sdown / mg_sup
+        (the same in their streamed form), mg_tail (the
         coarse-level tail kernel) or mg_cycle (one whole multigrid cycle)."""
         code = {"pcg_spmv": 0, "mg_defect": 1, "mg_tail": 2, "mg_cycle": 3, "mg_smooth": 4, "mg_post1": 5,
-                "mg_post2": 6, "mg_restrict": 7, "mg_prolong": 8, "mg_down": 9, "mg_up": 10}[which]
+                "mg_post2": 6, "mg_restrict": 7, "mg_prolong": 8, "mg_down": 9, "mg_up": 10, "mg_sdown": 11,
+                "mg_sup": 12}[which]
         ms, by = C.c_double(), C.c_double()
         _lib.check(_lib.lib().fb_solver_time_kernel(self._s, code, int(reps), 1 if flush_l2 else 0, C.byref(ms),
                                                      C.byref(by)), "fb_solver_time_kernel")
@@ -417,7 +426,7 @@ def solve(solver, vec_sol, vec_rhs, matrix=None, filter=None):
 def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, precision="f64",
                         ordering="native", use_graph=True, tail_rows=None, tma_rows=None, tma_window=None,
                         cluster_rows=None, cycle="V", diagonal=None, pdl=None, adapt_cgc="Fixed", fused=None,
-                        smoother="jacobi", smoother_omega=1.0, sweep="sequential"):
+                        smoother="jacobi", smoother_omega=1.0, sweep="sequential", streamed=None):
     """Convenience set-up from a finest-first list of level dicts with keys matrix, filter,
     transfer (all but the coarsest)."""
     h = MultiGridHierarchy(len(levels))
@@ -450,6 +459,8 @@ def build_pcg_multigrid(levels, omega=0.7, steps=2, tol_rel=1e-8, max_iter=100, 
         s.set_pdl(pdl)
     if fused is not None:
         s.set_fused(fused)
+    if streamed is not None:
+        s.set_streamed(streamed)
     s.set_smoother(smoother, smoother_omega, sweep)
     h.init()
     s.init()

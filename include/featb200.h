@@ -257,6 +257,10 @@ typedef struct
                            fixed coarse-grid correction, and run without the tail kernels */
   double smoother_omega;/* SOR / SSOR damping (SORPrecond omega; default 1) */
   int sweep_colouring;  /* FB_SWEEP_SEQUENTIAL (default) or FB_SWEEP_COLOURED */
+  int streamed;         /* structured 2D levels with more rows than `fused` and at least this many
+                           (0 = never) run the same two fused passes swept row by row through
+                           tiles of whole coarse-row bands, their rows staged in shared memory by
+                           the bulk-copy engine; results are bitwise those of one pass per step */
 } fb_solver_config;
 
 /* Fill `cfg` with the reference's defaults: FP64, native order, omega 0.7, V(2,2), tol_rel 1e-8,
@@ -308,6 +312,8 @@ fb_status fb_solver_vcycle(fb_solver* s, double* cor, const double* def);
 #define FB_KERNEL_MG_DOWN 9    /* fused pre-smoothing step 2 + defect + restriction, finest level (structured grids,
                                   whatever the `fused` row threshold) */
 #define FB_KERNEL_MG_UP 10     /* fused prolongation + post-smoothing with the PCG's z and r.z, finest level */
+#define FB_KERNEL_MG_SDOWN 11  /* FB_KERNEL_MG_DOWN in its streamed form (whatever the `streamed` threshold) */
+#define FB_KERNEL_MG_SUP 12    /* FB_KERNEL_MG_UP in its streamed form */
 
 /* Launches kernel `which` `reps` times on the solver's stream, timing each launch with CUDA events
  * on that stream (the finest level's pass kernels need a finest level above the coarse-level tail);
