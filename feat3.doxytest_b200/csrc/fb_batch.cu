@@ -11,8 +11,10 @@
 //
 // Per instance: PCG scalars, stopping test (iterative.hpp:492-507,795-879), Richardson skip flags
 // per level, and a status word; converged instances skip all work.  Dot products and norms are
-// reduced per warp and added per instance with FP64 atomics; the last warp to arrive finalises all
-// instances (their summation order is not fixed; results agree with single solves to rounding).
+// reduced per warp, summed per instance within the block and added per instance with FP64 atomics;
+// the last block to arrive finalises all instances (their summation order is not fixed; results
+// agree with single solves to rounding).  System matrices of lexicographically numbered instances
+// are held in diagonal storage (values only), as in the single-system solver.
 #include "fb_common.cuh"
 #include "fb_rows.cuh"
 #include "fb_setup.h"
@@ -65,29 +67,50 @@ namespace bt
     return v;
   }
 
-  // Adds the warp's partial to acc[inst] (if inst >= 0) and counts the warp in; the last warp of
-  // the grid gets true (all lanes) and then finalises.  Every warp of the grid must call this.
-  __device__ __forceinline__ bool warp_arrive(double part, int inst, const BScal& sc)
+  // Adds the block's partials per instance to acc[inst] and counts the block in; returns true in
+  // warp 0 of the last block of the grid, which then finalises.  A warp's rows belong to one
+  // instance (inst < 0: the warp contributes nothing); each run of consecutive warps with the same
+  // instance is added by its first warp's lane with one atomic, so the grid's same-address arrival
+  // counter takes one atomic per block.  Every thread of the grid must call this.
+  __device__ __forceinline__ bool block_arrive(double part, int inst, const BScal& sc)
   {
+    __shared__ double ws[BNT_MAX / 32];
+    __shared__ int wi[BNT_MAX / 32];
+    __shared__ unsigned int prev_s;
     const double s = warp_sum(part);
-    const int lane = threadIdx.x & 31;
-    unsigned int prev = 0;
+    const int lane = int(threadIdx.x & 31u), warp = int(threadIdx.x >> 5), nw = int(blockDim.x >> 5);
     if(lane == 0)
     {
-      if(inst >= 0)
-        atomicAdd(&sc.acc[inst], s);
-      __threadfence();
-      prev = atomicAdd(sc.arrive, 1u);
+      ws[warp] = s;
+      wi[warp] = inst;
     }
-    prev = __shfl_sync(0xffffffffu, prev, 0);
-    const unsigned int total = gridDim.x * (blockDim.x >> 5);
-    if(prev != total - 1)
+    __syncthreads();
+    if(warp == 0)
+    {
+      if(lane < nw)
+      {
+        const int my = wi[lane];
+        if(my >= 0 && (lane == 0 || wi[lane - 1] != my))
+        {
+          double t = 0.0;
+          for(int k = lane; k < nw && wi[k] == my; ++k)
+            t += ws[k];
+          atomicAdd(&sc.acc[my], t);
+        }
+      }
+      __threadfence();
+      __syncwarp();
+      if(lane == 0)
+        prev_s = atomicAdd(sc.arrive, 1u);
+    }
+    __syncthreads();
+    if(prev_s != gridDim.x - 1)
       return false;
     __threadfence();
-    return true;
+    return warp == 0;
   }
 
-  // last warp: fin(j, total) for every instance j, accumulators cleared, counter reset
+  // warp 0 of the last block: fin(j, total) for every instance j, accumulators cleared, counter reset
   template<class Fin>
   __device__ __forceinline__ void finalize_all(const BScal& sc, Fin fin)
   {
@@ -157,7 +180,7 @@ namespace bt
     }
     if(!xc)
       return;
-    if(warp_arrive(sq, inst, sc))
+    if(block_arrive(sq, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         if(active(sc, j) && sc.top[j] > gc)
@@ -216,7 +239,7 @@ namespace bt
           sq = post1_row<V, S, true>(A, b, x, d, c, dinv, dm, i);
       }
     }
-    if(warp_arrive(sq, inst, sc))
+    if(block_arrive(sq, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         skip[j] = skip_from_norm<S>(sqrt(tot));
@@ -267,7 +290,7 @@ namespace bt
     }
     if(!LAST)
       return;
-    if(warp_arrive(rz, inst, sc))
+    if(block_arrive(rz, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         if(active(sc, j) && sc.top[j] == g)
@@ -337,7 +360,7 @@ namespace bt
         sq = mul(rv, rv);
       }
     }
-    if(warp_arrive(sq, inst, sc))
+    if(block_arrive(sq, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         const double d0 = sqrt(tot);
@@ -385,7 +408,7 @@ namespace bt
         }
       }
     }
-    if(warp_arrive(sq, inst, sc))
+    if(block_arrive(sq, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         if(!active(sc, j))
@@ -436,7 +459,7 @@ namespace bt
         }
       }
     }
-    if(warp_arrive(qp, inst, sc))
+    if(block_arrive(qp, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         if(active(sc, j))
@@ -478,7 +501,7 @@ namespace bt
         }
       }
     }
-    if(warp_arrive(sq, inst, sc))
+    if(block_arrive(sq, inst, sc))
       finalize_all(sc, [&](int j, double tot)
       {
         if(!active(sc, j))
@@ -533,6 +556,7 @@ struct fb_batch
     uint32_t* soff = nullptr;
     uint32_t* col = nullptr;
     int16_t* dcol = nullptr;
+    int32_t* doff = nullptr;   // diagonal storage: the offsets (no column indices)
     void* val = nullptr;
     double bytes = 0;
   };
@@ -620,9 +644,10 @@ namespace bt
     return uint16_t(u >> 16);
   }
 
-  static fb_status upload_mat(fb_batch* s, fb_batch::Mat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty)
+  static fb_status upload_mat(fb_batch* s, fb_batch::Mat& d, const HostCsr& M, int prec, const std::vector<uint8_t>* empty,
+    bool diag = false)
   {
-    const HostSell H = build_sell(M, empty);
+    const HostSell H = build_sell(M, empty, true, diag);
     const uint32_t ns = (H.rows + 31u) / 32u;
     d.rows = H.rows;
     d.cols = H.cols;
@@ -630,9 +655,12 @@ namespace bt
     d.nnz = H.nnz;
     d.entries = H.entries;
     const size_t vb = prec == FB_PREC_F64 ? 8 : (prec == FB_PREC_F32 ? 4 : 2);
-    d.bytes = double(H.entries) * double(vb + (H.narrow ? 2 : 4)) + (H.kw ? 0.0 : double(ns + 1) * 4.0);
+    d.bytes = double(H.entries) * double(vb + (!H.doff.empty() ? 0 : (H.narrow ? 2 : 4))) +
+              (H.kw ? 0.0 : double(ns + 1) * 4.0);
     BT_TRY(upload_vec(s, &d.soff, H.soff));
-    if(H.narrow)
+    if(!H.doff.empty())
+      BT_TRY(upload_vec(s, &d.doff, H.doff));
+    else if(H.narrow)
       BT_TRY(upload_vec(s, &d.dcol, H.dcol));
     else
       BT_TRY(upload_vec(s, &d.col, H.col));
@@ -662,7 +690,7 @@ namespace bt
 
   template<typename V> DCsr<V> bview(const fb_batch::Mat& m)
   {
-    return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw};
+    return DCsr<V>{m.kw ? nullptr : m.soff, m.col, m.dcol, static_cast<const V*>(m.val), m.rows, m.kw, m.doff};
   }
 
   static unsigned int nblk(uint32_t n) { return std::max(1u, (n + BNT - 1) / BNT); }
@@ -1199,7 +1227,7 @@ fb_status fb_batch_create(fb_batch** out, int num, fb_hierarchy* const* hs, cons
           R.rp[size_t(oc + r) + 1] = uint32_t(R.col.size());
       }
     }
-    BT_TRY(bt::upload_mat(s.get(), gl.A, A, prec, &dm));
+    BT_TRY(bt::upload_mat(s.get(), gl.A, A, prec, &dm, cfg.diagonal != 0));
     if(has_t)
     {
       BT_TRY(bt::upload_mat(s.get(), gl.P, P, prec, &dm));
@@ -1286,7 +1314,7 @@ fb_status fb_batch_create(fb_batch** out, int num, fb_hierarchy* const* hs, cons
       packed += Aj.rows;
     }
     s->packed = packed;
-    BT_TRY(bt::upload_mat(s.get(), s->Atop, A, FB_PREC_F64, &dm));
+    BT_TRY(bt::upload_mat(s.get(), s->Atop, A, FB_PREC_F64, &dm, cfg.diagonal != 0));
     BT_TRY(bt::upload_vec(s.get(), &s->dm_top, dm));
     BT_TRY(bt::upload_vec(s.get(), &s->sinst_top, sinst));
     BT_TRY(bt::upload_vec(s.get(), &s->mg_base_top, mgb));
