@@ -386,12 +386,13 @@ def run_multi(args, kind):
     return 0
 
 
-def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900, field=None):
+def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900, field=None, backend=None):
     """The reference's own CPU solver (oracle/_ref/feat_oracle, built from the reference's sources)
-    on the same problem; returns its JSON summary with per-solve times (1 warm-up + reps)."""
+    on the same problem; returns its JSON summary with per-solve times (1 warm-up + reps).
+    backend="cuda": the reference's own GPU backend instead (oracle/_ref/feat_cuda)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    if not O.feat_available():
+    if not (O.feat_cuda_available() if backend == "cuda" else O.feat_available()):
         return None
     from featb200 import assembly as AS
     with tempfile.TemporaryDirectory() as d:
@@ -403,7 +404,7 @@ def cpu_reference_times(dim, level, rhs_kind, gauss, reps, timeout=900, field=No
             kappa = os.path.join(d, "kappa.txt")
             AS.write_params(kappa, field=field)
         return O.feat_solve(d, dim=dim, level=level, rhs=rhs_kind, params=params, kappa=kappa, dump=False,
-                            time_reps=reps, timeout=timeout)
+                            time_reps=reps, timeout=timeout, b200=backend)
 
 
 def reference_sample(args):
@@ -460,10 +461,39 @@ def reference_sample(args):
     return None
 
 
+def run_reference_gpu(args):
+    """The reference's own GPU backend (FEAT built with its CUDA sources: cuSPARSE SpMV, cuBLAS
+    vector ops, managed memory, one synchronised launch per LAFEM op) on the default workload, FP64:
+    a timing column beside the library, not the driver's reference arm."""
+    dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
+    from featb200 import assembly as AS
+    if rhs_kind not in ("sine", "gauss"):
+        print(json.dumps({"impl": "reference", "reference_backend": "cuda",
+                          "unavailable": "timed for the single-system workloads only"}))
+        return 0
+    gauss = AS.gauss_params(1, dim) if rhs_kind == "gauss" else None
+    res = cpu_reference_times(dim, level, rhs_kind, gauss, max(1, min(args.warmup + args.steps, 20)), backend="cuda")
+    if res is None:
+        print(json.dumps({"impl": "reference", "reference_backend": "cuda",
+                          "unavailable": "oracle/_ref/feat_cuda is missing; build it with `make -C oracle cuda`"}))
+        return 0
+    t = res["times_ms"]
+    ms = float(np.mean(t))
+    print(json.dumps({"impl": "reference", "reference_backend": "cuda", "metric": METRIC, "value": ms, "unit": "ms",
+                      "n_gpus": 1, "steps": len(t), "warmup": 1, "ms_per_step": ms, "higher_is_better": False,
+                      "dtype": "f64", "data": "synthetic", "times_ms": t, "status": res["status"],
+                      "config": {"workload": args.workload + ": " + desc + " (the reference's GPU path is FP64)",
+                                 "dofs": res["dofs"], "nnz": res["nnz"], "iterations": res["iters"]},
+                      "timing": "host wall clock around Solver::solve (every op synchronises), after 1 warm-up solve"}))
+    return 0
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    if args.reference_backend == "cuda":
+        return run_reference_gpu(args)
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
     res = reference_sample(args)
     if res is None:
@@ -659,6 +689,9 @@ def main():
                     help="skip the plain-FP64 vs batched-mixed comparison on the uneven-instance family")
     ap.add_argument("--target-count", type=int, default=256, help="instances of that comparison")
     ap.add_argument("--batch-count", type=int, default=256, help="instances of the batch workload")
+    ap.add_argument("--reference-backend", choices=["generic", "cuda"], default="generic",
+                    help="with --impl reference: the reference's generic CPU backend (default) or its own CUDA "
+                         "backend (cuSPARSE / cuBLAS, built by `make -C oracle cuda`)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

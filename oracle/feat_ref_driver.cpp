@@ -22,6 +22,10 @@
 //   --backend b200   FEAT's own PCG + MultiGrid with every LAFEM op dispatched to the CUDA backend
 //                    (Backend::set_preferred_backend(PreferredBackend::cuda)), i.e. to the library
 //   --b200-solver    the whole solve handed to the library's solver object (featb200_solver.hpp)
+// And a third time with -DFEAT_HAVE_CUDA and FEAT's own CUDA backend (its kernel/util/cuda_util.cu and
+// kernel/lafem/arch/*.cu compiled by nvcc, cuSPARSE / cuBLAS) into oracle/_ref/feat_cuda, where
+//   --backend cuda   runs FEAT's own PCG + MultiGrid with every LAFEM op on FEAT's GPU kernels
+// (the reference's GPU path, for a timing column beside the library).
 //
 //   feat_oracle fd M D DIR     (the reference's basic_solver-test problem, see run_fd)
 //   feat_oracle solve --dim D --level L --out DIR [--rhs sine|gauss] [--params FILE]
@@ -367,7 +371,7 @@ namespace Oracle
     int time_reps = 0;
     std::string smoother = "jacobi";   // the Richardson smoother's preconditioner: jacobi | sor | ssor
     double sor_omega = 1.0;            // SOR / SSOR damping
-    std::string backend = "generic";   // generic | b200 (FEATB200_BACKEND builds only)
+    std::string backend = "generic";   // generic | b200 (FEATB200_BACKEND builds) | cuda (CUDA builds)
     bool b200_solver = false;          // FEATB200_BACKEND builds only
   };
 
@@ -546,10 +550,13 @@ namespace Oracle
       multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinEnergy);
     else if(opt.cgc == "defect")
       multigrid->set_adapt_cgc(Solver::MultiGridAdaptCGC::MinDefect);
-#ifdef FEATB200_BACKEND
-    // every LAFEM op from here on (smoother set-up, solve) goes to the CUDA backend = the library
-    if(opt.backend == "b200")
+#ifdef FEAT_HAVE_CUDA
+    // every LAFEM op from here on (smoother set-up, solve) goes to the CUDA backend: the library
+    // (FEATB200_BACKEND builds, "b200") or FEAT's own GPU kernels ("cuda")
+    if(opt.backend == "b200" || opt.backend == "cuda")
       Backend::set_preferred_backend(PreferredBackend::cuda);
+#endif
+#ifdef FEATB200_BACKEND
     std::shared_ptr<Solver::IterativeSolver<VectorType>> solver;
     if(opt.b200_solver)
       solver = std::make_shared<FEATB200::MultiGridPCG<MatrixType, FilterType, TransferType>>(hierarchy,
@@ -766,8 +773,10 @@ int main(int argc, char* argv[])
     else if(a == "--time") opt.time_reps = std::stoi(next());
     else if(a == "--smoother") opt.smoother = next();
     else if(a == "--sor-omega") opt.sor_omega = std::stod(next());
-#ifdef FEATB200_BACKEND
+#ifdef FEAT_HAVE_CUDA
     else if(a == "--backend") opt.backend = next();
+#endif
+#ifdef FEATB200_BACKEND
     else if(a == "--b200-solver") opt.b200_solver = true;
 #endif
     else

@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(REF_DIR, "libmgoracle.so")
 FEAT_BIN = os.path.join(REF_DIR, "feat_oracle")
 # the same driver built as a FEAT CUDA build on the library's FEAT binding
 FEAT_B200_BIN = os.path.join(REF_DIR, "feat_b200")
+FEAT_CUDA_BIN = os.path.join(REF_DIR, "feat_cuda")
 # the reference source tree the reference binary is compiled from (only where it exists)
 REF_SRC = os.environ.get("FEAT_REF", "/root/reference")
 
@@ -49,7 +50,9 @@ def build():
         # the FEAT build on the library's binding links the built library
         if os.path.exists(os.path.join(os.path.dirname(HERE), "feat3.doxytest_b200", "featb200", "libfeatb200.so")):
             targets.append("b200")
-    subprocess.run(["make", "-s", "-C", HERE, f"FEAT_REF={REF_SRC}"] + targets, check=True)
+        # FEAT on its own CUDA backend (a timing column beside the library)
+        targets.append("cuda")
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, f"FEAT_REF={REF_SRC}"] + targets, check=True)
 
 
 _lib = None
@@ -212,14 +215,19 @@ def feat_b200_available():
     return os.path.exists(FEAT_B200_BIN)
 
 
+def feat_cuda_available():
+    return os.path.exists(FEAT_CUDA_BIN)
+
+
 def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, omega=0.7, steps=2,
                tol=1e-8, iterates=0, vcycle=False, dump_levels=False, time_reps=0, dump=True,
                level_min=1, timeout=3600, cycle="v", cgc="fixed", b200=None, smoother="jacobi", sor_omega=1.0):
     """Run the reference's own solver through oracle/_ref/feat_oracle; returns its JSON summary.
     b200 = "ops" or "solver": the same program built as a FEAT CUDA build on the library's FEAT
     binding (oracle/_ref/feat_b200), with every LAFEM op on the library ("ops") or the whole solve
-    handed to the library's solver object ("solver")."""
-    exe = FEAT_BIN if b200 is None else FEAT_B200_BIN
+    handed to the library's solver object ("solver"); b200 = "cuda": the FEAT CUDA build on FEAT's
+    own GPU backend (oracle/_ref/feat_cuda), every LAFEM op on FEAT's cuSPARSE / cuBLAS kernels."""
+    exe = FEAT_BIN if b200 is None else (FEAT_CUDA_BIN if b200 == "cuda" else FEAT_B200_BIN)
     cmd = [exe, "solve", "--dim", str(dim), "--level", str(level), "--level-min", str(level_min),
            "--out", out_dir, "--rhs", rhs, "--omega", repr(omega), "--steps", str(steps), "--tol",
            repr(tol), "--iterates", str(iterates), "--time", str(time_reps), "--cycle", cycle, "--cgc", cgc]
@@ -239,6 +247,8 @@ def feat_solve(out_dir, dim=2, level=7, rhs="sine", params=None, kappa=None, ome
         cmd += ["--backend", "b200"]
     elif b200 == "solver":
         cmd.append("--b200-solver")
+    elif b200 == "cuda":
+        cmd += ["--backend", "cuda"]
     elif b200 is not None:
         raise ValueError(b200)
     os.makedirs(out_dir, exist_ok=True)

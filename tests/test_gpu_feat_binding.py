@@ -108,3 +108,21 @@ def test_feat_generic_on_managed_memory(featlib, cuda, tmp_path):
     assert summ["backend"] == "generic" and summ["solver"] == "feat"
     for f in ("vcycle.npy", "sol.npy"):
         assert np.array_equal(np.load(os.path.join(out_g, f)), np.load(os.path.join(out_r, f)))
+
+
+def test_feat_own_cuda_backend(featlib, cuda, tmp_path):
+    """FEAT built on its own CUDA backend (oracle/_ref/feat_cuda: cuSPARSE SpMV, cuBLAS vector ops) and
+    run with Backend::set_preferred_backend(cuda) solves the same problem as the generic build (its
+    sums are ordered differently, so to solver tolerance, not bitwise): the problem behind the
+    reference GPU timing column."""
+    import oracle as O
+    require_reference_binary()
+    if not O.feat_cuda_available():
+        if os.environ.get("FEATB200_REQUIRE_REF") == "1":
+            pytest.fail("oracle/_ref/feat_cuda not built (FEATB200_REQUIRE_REF=1)")
+        pytest.skip("oracle/_ref/feat_cuda not built")
+    ref = _run(tmp_path, "generic", dim=2, level=7)
+    cu = _run(tmp_path, "cuda", dim=2, level=7, b200="cuda")
+    assert cu["summ"]["backend"] == "cuda" and cu["summ"]["status"] == "success"
+    assert abs(cu["summ"]["iters"] - ref["summ"]["iters"]) <= 1
+    assert rel_err(cu["sol"], ref["sol"]) <= 1e-7
