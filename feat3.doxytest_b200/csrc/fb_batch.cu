@@ -29,7 +29,7 @@ namespace fb
 {
 namespace bt
 {
-  constexpr int BNT = 256;       // block size of the PCG-space kernels
+  constexpr int BNT = 256;       // block size of the PCG-space kernels (4 resident per SM: at most 64 registers)
   constexpr int BNT_MAX = 512;   // largest block size the autotuner may pick for the V-cycle passes
   constexpr int BW = BNT / 32;
   constexpr int MAXG = 16;
@@ -340,7 +340,7 @@ namespace bt
   }
 
   // r = F(rhs - A x), ||r|| -> def_init, status
-  __global__ void __launch_bounds__(BNT) kb_pcg_init(DCsr<double> A, const double* __restrict__ rhs,
+  __global__ void __launch_bounds__(BNT, 4) kb_pcg_init(DCsr<double> A, const double* __restrict__ rhs,
     const double* __restrict__ x, double* __restrict__ r, const uint8_t* __restrict__ dm, const int* __restrict__ sinst,
     BScal sc)
   {
@@ -380,7 +380,7 @@ namespace bt
   // the V-cycle input of every instance at its top level: b = S(r * scale_j), sol1 = F(D .* b);
   // ||b|| -> the top level's pre-smoother skip flag
   template<typename S>
-  __global__ void __launch_bounds__(BNT) kb_prep(const double* __restrict__ r, TopPtrs<S> tp,
+  __global__ void __launch_bounds__(BNT, 4) kb_prep(const double* __restrict__ r, TopPtrs<S> tp,
     const int* __restrict__ mg_base, const uint8_t* __restrict__ dm, const int* __restrict__ sinst, uint32_t n,
     int scale_mode, BScal sc)
   {
@@ -420,7 +420,7 @@ namespace bt
       });
   }
 
-  __global__ void __launch_bounds__(BNT) kb_pcg_p(double* __restrict__ p, const double* __restrict__ z,
+  __global__ void __launch_bounds__(BNT, 4) kb_pcg_p(double* __restrict__ p, const double* __restrict__ z,
     const int* __restrict__ sinst, uint32_t n, int first, BScal sc)
   {
     if(closed(sc))
@@ -434,7 +434,7 @@ namespace bt
     p[i] = first ? z[i] : add(mul(p[i], sc.beta[j]), z[i]);
   }
 
-  __global__ void __launch_bounds__(BNT) kb_pcg_q(DCsr<double> A, const double* __restrict__ p, double* __restrict__ q,
+  __global__ void __launch_bounds__(BNT, 4) kb_pcg_q(DCsr<double> A, const double* __restrict__ p, double* __restrict__ q,
     const uint8_t* __restrict__ dm, const int* __restrict__ sinst, BScal sc)
   {
     if(closed(sc))
@@ -469,7 +469,7 @@ namespace bt
 
   // x += alpha p, r -= alpha q, ||r||, stopping test, next V-cycle input at the top level
   template<typename S>
-  __global__ void __launch_bounds__(BNT) kb_pcg_x(double* __restrict__ x, double* __restrict__ r,
+  __global__ void __launch_bounds__(BNT, 4) kb_pcg_x(double* __restrict__ x, double* __restrict__ r,
     const double* __restrict__ p, const double* __restrict__ q, const uint8_t* __restrict__ dm, TopPtrs<S> tp,
     const int* __restrict__ mg_base, const int* __restrict__ sinst, uint32_t n, int scale_mode, BScal sc)
   {
@@ -857,8 +857,10 @@ namespace bt
         for(int r = 0; r < 7; ++r)
         {
           FB_CUDA(cudaEventRecord(s->ev0, st));
-          kb_defect<V, S><<<nblk(f.n, bs), bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)f.x, (S*)f.d, f.dm,
-            f.sinst, sc);
+          // a pass with the per-instance reduction (one arrival per block): it favours larger
+          // blocks than a pass without one
+          kb_post1<V, S><<<nblk(f.n, bs), bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)f.x, (S*)f.d,
+            (S*)f.c, (const S*)f.dinv, f.dm, f.sinst, sc.skip_post + size_t(G) * sc.J, sc);
           FB_CUDA(cudaEventRecord(s->ev1, st));
           FB_CUDA(cudaEventSynchronize(s->ev1));
           float ms = 0.f;
