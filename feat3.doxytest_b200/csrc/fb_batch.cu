@@ -17,9 +17,12 @@
 // are held in diagonal storage (values only), as in the single-system solver.
 #include "fb_common.cuh"
 #include "fb_rows.cuh"
+#include "fb_tma.cuh"
 #include "fb_setup.h"
 
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -302,6 +305,373 @@ namespace bt
       });
   }
 
+  // ---------------------------------------------------------------- staged passes
+  // Epilogues of the single-system staged pass (k_tma_pass, fb_tma.cuh) on a global level: the
+  // matrix rows stream through shared memory by bulk copies, and each epilogue applies the row body
+  // of the one-thread-per-row kernel above (the same arithmetic, so the same values) to the rows of
+  // instances in progress.  A row's instance is looked up per warp (instances are padded to whole
+  // warps).  Reducing epilogues add each warp's contributions to its instance's accumulator and
+  // finish in block_done: one arrival per block; warp 0 of the last block finalises every instance.
+
+  // every lane of a warp calls this for its row (inst < 0: the warp contributes nothing)
+  __device__ __forceinline__ void warp_add(double v, int inst, const BScal& sc)
+  {
+    const double t = warp_sum(v);
+    if((threadIdx.x & 31u) == 0 && inst >= 0)
+      atomicAdd(&sc.acc[inst], t);
+  }
+
+  template<class Fin>
+  __device__ __forceinline__ void blocks_done(const BScal& sc, Fin fin)
+  {
+    __shared__ unsigned int prev_b;
+    if((threadIdx.x & 31u) == 0)
+      __threadfence();   // this warp's accumulator atomics before the block's arrival
+    __syncthreads();
+    if(threadIdx.x == 0)
+      prev_b = atomicAdd(sc.arrive, 1u);
+    __syncthreads();
+    if(prev_b != gridDim.x - 1 || threadIdx.x >= 32)
+      return;
+    __threadfence();
+    finalize_all(sc, fin);
+  }
+
+  // x' = x + F(D F(b - A x)) (smooth_row); skipped -> 0
+  template<typename V, typename S>
+  struct BOpSmooth
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b, x, di; bool d, on, skip; };
+    static constexpr bool REDUCES = false;
+    const S* b; const S* x; S* xo; const S* dinv; const uint8_t* dm; const int* sinst; const int* skip; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      const int j = __ldg(sinst + (i >> 5));
+      p.on = active(sc, j);
+      if(p.on)
+      {
+        p.skip = skip[j] != 0;
+        p.d = __ldg(dm + i) != 0;
+        p.b = Ac(b[i]);
+        p.x = Ac(x[i]);
+        p.di = Ac(__ldg(dinv + i));
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      if(p.on)
+      {
+        S out = S(0);
+        if(!p.skip)
+        {
+          const Ac d1 = p.d ? Ac(0) : sub(p.b, sum);
+          const Ac c = p.d ? Ac(0) : mul(p.di, d1);
+          out = S(add(p.x, c));
+        }
+        xo[i] = out;
+      }
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
+  // d = F(b - A x) (defect_row)
+  template<typename V, typename S>
+  struct BOpDefect
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b; bool d, on; };
+    static constexpr bool REDUCES = false;
+    const S* b; S* dv; const uint8_t* dm; const int* sinst; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      p.on = active(sc, __ldg(sinst + (i >> 5)));
+      if(p.on)
+      {
+        p.d = __ldg(dm + i) != 0;
+        p.b = Ac(b[i]);
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      if(p.on)
+        dv[i] = p.d ? S(0) : S(sub(p.b, sum));
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
+  // x += F(P x_c) (prolong_row); the gathered vector is the coarse x
+  template<typename V, typename S>
+  struct BOpProlong
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac x; bool d, on; };
+    static constexpr bool REDUCES = false;
+    S* x; const uint8_t* dm; const int* sinst; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      p.on = active(sc, __ldg(sinst + (i >> 5)));
+      if(p.on)
+      {
+        p.d = __ldg(dm + i) != 0;
+        p.x = Ac(x[i]);
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      if(p.on)
+      {
+        const Ac c = p.d ? Ac(0) : add(sum, Ac(0));
+        x[i] = S(add(p.x, c));
+      }
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+  };
+
+  // d = F(b - A x), c = F(D d) (post1_calc); per-instance ||d|| -> the post-smoother's skip flag
+  template<typename V, typename S>
+  struct BOpPost1
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac b, di; bool d; int j; };
+    static constexpr bool REDUCES = false;
+    const S* b; S* dv; S* cv; const S* dinv; const uint8_t* dm; const int* sinst; int* skip; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      const int j = __ldg(sinst + (i >> 5));
+      p.j = active(sc, j) ? j : -1;
+      if(p.j >= 0)
+      {
+        p.d = __ldg(dm + i) != 0;
+        p.b = Ac(b[i]);
+        p.di = Ac(__ldg(dinv + i));
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      double sq = 0.0;
+      if(p.j >= 0)
+      {
+        const Ac d1 = p.d ? Ac(0) : sub(p.b, sum);
+        const Ac c1 = p.d ? Ac(0) : mul(p.di, d1);
+        dv[i] = S(d1);
+        cv[i] = S(add(Ac(0), c1));
+        sq = double(d1) * double(d1);
+      }
+      warp_add(sq, p.j, sc);
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+    __device__ void block_done() const
+    {
+      int* sk = skip;
+      blocks_done(sc, [&](int j, double tot) { sk[j] = skip_from_norm<S>(sqrt(tot)); });
+    }
+  };
+
+  // post-smoothing step k >= 2 (post2_row) with the gathered c; LAST: x = x + c' (instances whose
+  // top is g write z = x * inv_scale and add r.z -> gamma, beta), else c' to co
+  template<typename V, typename S, bool LAST>
+  struct BOpPost2
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac d, c, di, x; double r, inv; uint32_t pr; bool dd, skip, top; int j; };
+    static constexpr bool REDUCES = false;
+    const S* d; const S* c; S* co; S* x; double* z; const double* r; const int* pcg_base; const S* dinv;
+    const uint8_t* dm; const int* sinst; int g; const int* skip; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      const int j = __ldg(sinst + (i >> 5));
+      p.j = active(sc, j) ? j : -1;
+      if(p.j >= 0)
+      {
+        p.skip = skip[j] != 0;
+        p.dd = __ldg(dm + i) != 0;
+        p.d = Ac(d[i]);
+        p.c = Ac(c[i]);
+        p.di = Ac(__ldg(dinv + i));
+        if(LAST)
+        {
+          p.x = Ac(x[i]);
+          p.top = sc.top[j] == g;
+          if(p.top)
+          {
+            p.pr = uint32_t(__ldg(pcg_base + (i >> 5))) + (i & 31u);
+            p.r = r[p.pr];
+            p.inv = sc.inv_scale[j];
+          }
+        }
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      double rz = 0.0;
+      if(p.j >= 0)
+      {
+        Ac cn = Ac(0);
+        if(!p.skip)
+        {
+          const Ac dk = p.dd ? Ac(0) : sub(p.d, sum);
+          const Ac ck = p.dd ? Ac(0) : mul(p.di, dk);
+          cn = add(p.c, ck);
+        }
+        if(!LAST)
+          co[i] = S(cn);
+        else
+        {
+          const S xn = S(add(p.x, cn));
+          if(p.top)
+          {
+            const double zi = mul(double(xn), p.inv);
+            z[p.pr] = zi;
+            rz = mul(p.r, zi);
+          }
+          else
+            x[i] = xn;
+        }
+      }
+      if(LAST)
+        warp_add(rz, p.j >= 0 && p.top ? p.j : -1, sc);
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+    __device__ void block_done() const
+    {
+      if(!LAST)
+        return;
+      const BScal& s = sc;
+      const int gg = g;
+      blocks_done(sc, [&](int j, double tot)
+      {
+        if(active(s, j) && s.top[j] == gg)
+        {
+          s.gamma_prev[j] = s.gamma[j];
+          s.gamma[j] = tot;
+          s.beta[j] = tot / s.gamma_prev[j];
+        }
+      });
+    }
+  };
+
+  // b_c = F(R d), sol1_c = F(D_c b_c) (restrict_calc) on coarse rows of instances whose top is not
+  // the coarse level; per-instance ||b_c|| -> the coarse pre-smoother's skip flag (xc == null: the
+  // coarsest level, no sol1 and no flag)
+  template<typename V, typename S>
+  struct BOpRestrict
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    struct Pre { Ac di; bool dc; int j; };
+    static constexpr bool REDUCES = false;
+    S* bc; S* xc; const S* dinvc; const uint8_t* dmc; const int* sinstc; int gc; int* skipc; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre p{};
+      const int j = __ldg(sinstc + (i >> 5));
+      p.j = (active(sc, j) && sc.top[j] != gc) ? j : -1;
+      if(p.j >= 0)
+      {
+        p.dc = __ldg(dmc + i) != 0;
+        if(xc)
+          p.di = Ac(__ldg(dinvc + i));
+      }
+      return p;
+    }
+    __device__ double operator()(uint32_t i, Ac sum, const Pre& p) const
+    {
+      double sq = 0.0;
+      if(p.j >= 0)
+      {
+        const Ac v = p.dc ? Ac(0) : add(sum, Ac(0));
+        bc[i] = S(v);
+        if(xc)
+        {
+          const Ac c = p.dc ? Ac(0) : mul(p.di, v);
+          xc[i] = S(add(Ac(0), c));
+        }
+        sq = double(v) * double(v);
+      }
+      if(xc)
+        warp_add(sq, p.j, sc);
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+    __device__ void block_done() const
+    {
+      if(!xc)
+        return;
+      const BScal& s = sc;
+      const int g = gc;
+      int* sk = skipc;
+      blocks_done(sc, [&](int j, double tot)
+      {
+        if(active(s, j) && s.top[j] > g)
+          sk[j] = skip_from_norm<S>(sqrt(tot));
+      });
+    }
+  };
+
+  // q = F(A p), per-instance q.p -> alpha (FP64, the PCG space)
+  struct BOpPcgQ
+  {
+    struct Pre { double p; bool d; int j; };
+    static constexpr bool REDUCES = false;
+    double* q; const double* p; const uint8_t* dm; const int* sinst; BScal sc;
+    __device__ bool closed() const { return bt::closed(sc); }
+    __device__ Pre pre(uint32_t i) const
+    {
+      Pre r{};
+      const int j = __ldg(sinst + (i >> 5));
+      r.j = active(sc, j) ? j : -1;
+      if(r.j >= 0)
+      {
+        r.d = dm[i] != 0;
+        r.p = p[i];
+      }
+      return r;
+    }
+    __device__ double operator()(uint32_t i, double sum, const Pre& pr) const
+    {
+      double qp = 0.0;
+      if(pr.j >= 0)
+      {
+        const double qv = pr.d ? 0.0 : add(sum, 0.0);
+        q[i] = qv;
+        qp = mul(qv, pr.p);
+      }
+      warp_add(qp, pr.j, sc);
+      return 0.0;
+    }
+    __device__ void finish(double) const {}
+    __device__ void block_done() const
+    {
+      const BScal& s = sc;
+      blocks_done(sc, [&](int j, double tot)
+      {
+        if(active(s, j))
+          s.alpha[j] = s.gamma[j] / tot;
+      });
+    }
+  };
+
   // ---------------------------------------------------------------- PCG space
   __device__ __forceinline__ double pow2_inv(double v)
   {
@@ -551,7 +921,7 @@ struct fb_batch
 {
   struct Mat
   {
-    uint32_t rows = 0, cols = 0, kw = 0;
+    uint32_t rows = 0, cols = 0, kw = 0, kmax = 0;
     uint64_t nnz = 0, entries = 0;
     uint32_t* soff = nullptr;
     uint32_t* col = nullptr;
@@ -598,6 +968,8 @@ struct fb_batch
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int* err = nullptr;   // a bounded wait of a staged pass expired
+  int nsm = 148;
   uint64_t launches_init = 0, launches_body = 0;
   double bytes_init = 0, bytes_body = 0;
 };
@@ -652,6 +1024,9 @@ namespace bt
     d.rows = H.rows;
     d.cols = H.cols;
     d.kw = H.kw;
+    d.kmax = H.kw;
+    for(uint32_t sl = 0; sl + 1 < uint32_t(H.soff.size()); ++sl)
+      d.kmax = std::max(d.kmax, (H.soff[sl + 1] - H.soff[sl]) / 32u);
     d.nnz = H.nnz;
     d.entries = H.entries;
     const size_t vb = prec == FB_PREC_F64 ? 8 : (prec == FB_PREC_F32 ? 4 : 2);
@@ -685,6 +1060,52 @@ namespace bt
       BT_TRY(upload_vec(s, &p, h));
       d.val = p;
     }
+    return FB_OK;
+  }
+
+  constexpr uint32_t STAGED_ROWS = 1000;   // matrices of at least this many rows take the staged passes
+
+  // resident blocks per SM of a staged-pass kernel with `smem` bytes of dynamic shared memory
+  static uint32_t staged_resident(const void* kern, size_t smem)
+  {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, size_t>, uint32_t> cache;
+    std::lock_guard<std::mutex> g(mu);
+    const auto key = std::make_pair(kern, smem);
+    const auto it = cache.find(key);
+    if(it != cache.end())
+      return it->second;
+    int nb = 0;
+    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, TMA_NT, smem) != cudaSuccess || nb < 1)
+    {
+      (void)cudaGetLastError();
+      nb = 1;
+    }
+    cache[key] = uint32_t(nb);
+    return uint32_t(nb);
+  }
+
+  // dynamic shared memory above 48 KB for every staged-pass instance the batch may launch
+  template<typename V, typename S, class Op>
+  static fb_status staged_attr()
+  {
+    const int mx = int(TMA_SMEM_MAX) + 8 * 1024;
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, Op, 9, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, Op, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    FB_CUDA(cudaFuncSetAttribute(k_tma_pass<V, S, Op, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    return FB_OK;
+  }
+  template<typename V, typename S>
+  static fb_status staged_attrs()
+  {
+    BT_TRY((staged_attr<V, S, BOpSmooth<V, S>>()));
+    BT_TRY((staged_attr<V, S, BOpDefect<V, S>>()));
+    BT_TRY((staged_attr<V, S, BOpProlong<V, S>>()));
+    BT_TRY((staged_attr<V, S, BOpPost1<V, S>>()));
+    BT_TRY((staged_attr<V, S, BOpPost2<V, S, true>>()));
+    BT_TRY((staged_attr<V, S, BOpPost2<V, S, false>>()));
+    BT_TRY((staged_attr<V, S, BOpRestrict<V, S>>()));
+    BT_TRY((staged_attr<double, double, BOpPcgQ>()));
     return FB_OK;
   }
 
@@ -723,6 +1144,65 @@ namespace bt
       return t;
     }
 
+    // the staged pass serves matrices of at least STAGED_ROWS rows whose stages fit
+    static bool use_tma(const fb_batch::Mat& m)
+    {
+      if(m.rows < STAGED_ROWS || !m.kmax || (m.doff && m.kw != 9))
+        return false;
+      const uint32_t cb = m.doff ? 0u : (m.dcol ? 2u : 4u);
+      return uint64_t(tma_stages<V>()) * tma_stage_bytes<V>(m.kmax, cb) <= TMA_SMEM_MAX;
+    }
+
+    // one staged pass (k_tma_pass) over m with gathered vector x and epilogue op: a persistent grid
+    // of one wave
+    // query_only: look the kernel's residency up (filling the cache outside graph capture), no launch
+    template<typename VV, typename XS, class Op>
+    void tma(const fb_batch::Mat& m, const void* x, const Op& op, bool query_only = false)
+    {
+      const uint32_t cb = m.doff ? 0u : (m.dcol ? 2u : 4u);
+      const uint32_t nch = (m.rows + TMA_NT - 1) / TMA_NT;
+      auto launch = [&](auto kern, size_t sm)
+      {
+        const uint32_t grid = std::max(1u, std::min(nch, uint32_t(s->nsm) * staged_resident((const void*)kern, sm)));
+        if(query_only)
+          return;
+        kern<<<grid, TMA_NT, sm, st>>>(bview<VV>(m), static_cast<const XS*>(x), m.rows, m.kmax, nullptr, 0u, 0u, 0,
+          op, RedSlot{nullptr, nullptr}, s->err);
+      };
+      if(m.doff)
+        launch(k_tma_pass<VV, XS, Op, 9, true>, size_t(tma_stages_dg<VV, true>()) * tma_stage_bytes<VV>(m.kmax, 0u));
+      else if(m.kw == 9)
+        launch(k_tma_pass<VV, XS, Op, 9>, size_t(tma_stages<VV>()) * tma_stage_bytes<VV>(m.kmax, cb));
+      else
+        launch(k_tma_pass<VV, XS, Op, 0>, size_t(tma_stages<VV>()) * tma_stage_bytes<VV>(m.kmax, cb));
+    }
+
+    // every staged pass the solve launches, looked up once before its launches are captured
+    void prime()
+    {
+      for(int G = 1; G < s->NG; ++G)
+      {
+        const fb_batch::GLevel& f = s->g[size_t(G)];
+        if(use_tma(f.A))
+        {
+          tma<V, S>(f.A, nullptr, BOpSmooth<V, S>{}, true);
+          tma<V, S>(f.A, nullptr, BOpDefect<V, S>{}, true);
+          tma<V, S>(f.A, nullptr, BOpPost1<V, S>{}, true);
+          tma<V, S>(f.A, nullptr, BOpPost2<V, S, true>{}, true);
+          tma<V, S>(f.A, nullptr, BOpPost2<V, S, false>{}, true);
+        }
+        if(use_tma(f.R))
+          tma<V, S>(f.R, nullptr, BOpRestrict<V, S>{}, true);
+        if(use_tma(f.P))
+          tma<V, S>(f.P, nullptr, BOpProlong<V, S>{}, true);
+      }
+      if(BLaunch<double, double>::use_tma(s->Atop))
+      {
+        BLaunch<double, double> d64{s, st, false};
+        d64.template tma<double, double>(s->Atop, nullptr, BOpPcgQ{}, true);
+      }
+    }
+
     void vcycle()
     {
       const int NG = s->NG;
@@ -738,7 +1218,12 @@ namespace bt
         void* xb = f.x2;
         for(int k = 1; k < steps; ++k)
         {
-          if(!dry)
+          if(dry)
+            ;
+          else if(use_tma(f.A))
+            tma<V, S>(f.A, xa, BOpSmooth<V, S>{(const S*)f.b, (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.sinst,
+              skp, sc});
+          else
             kb_smooth<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
               (const S*)f.dinv, f.dm, f.sinst, skp, sc);
           ++launches;
@@ -746,11 +1231,20 @@ namespace bt
           std::swap(xa, xb);
         }
         xcur[size_t(G)] = xa;
-        if(!dry)
+        if(dry)
+          ;
+        else if(use_tma(f.A))
+          tma<V, S>(f.A, xa, BOpDefect<V, S>{(const S*)f.b, (S*)f.d, f.dm, f.sinst, sc});
+        else
           kb_defect<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm,
             f.sinst, sc);
         const bool coarsest = (G - 1 == 0);
-        if(!dry)
+        if(dry)
+          ;
+        else if(use_tma(f.R))
+          tma<V, S>(f.R, f.d, BOpRestrict<V, S>{(S*)c.b, coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm,
+            c.sinst, G - 1, sc.skip_pre + size_t(G - 1) * sc.J, sc});
+        else
           kb_restrict<V, S><<<nblk(c.n, c.bs), c.bs, 0, st>>>(bview<V>(f.R), (const S*)f.d, (S*)c.b,
             coarsest ? (S*)nullptr : (S*)c.x, (const S*)c.dinv, c.dm, c.sinst, G - 1,
             sc.skip_pre + size_t(G - 1) * sc.J, sc);
@@ -771,12 +1265,21 @@ namespace bt
         fb_batch::GLevel& f = s->g[size_t(G)];
         void* xf = xcur[size_t(G)];
         int* skq = sc.skip_post + size_t(G) * sc.J;
-        if(!dry)
+        if(dry)
+          ;
+        else
         {
-          kb_prolong<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.P), (const S*)xcur[size_t(G - 1)], (S*)xf, f.dm,
-            f.sinst, sc);
-          kb_post1<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
-            (const S*)f.dinv, f.dm, f.sinst, skq, sc);
+          if(use_tma(f.P))
+            tma<V, S>(f.P, xcur[size_t(G - 1)], BOpProlong<V, S>{(S*)xf, f.dm, f.sinst, sc});
+          else
+            kb_prolong<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.P), (const S*)xcur[size_t(G - 1)], (S*)xf,
+              f.dm, f.sinst, sc);
+          if(use_tma(f.A))
+            tma<V, S>(f.A, xf, BOpPost1<V, S>{(const S*)f.b, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.sinst, skq,
+              sc});
+          else
+            kb_post1<V, S><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d,
+              (S*)f.c, (const S*)f.dinv, f.dm, f.sinst, skq, sc);
         }
         launches += 2;
         bytes += cb(f.P, 1, 1) + cb(f.A, 2, 2);
@@ -787,6 +1290,12 @@ namespace bt
           const bool last = (k == steps);
           if(dry)
             ;
+          else if(use_tma(f.A) && last)
+            tma<V, S>(f.A, ca, BOpPost2<V, S, true>{(const S*)f.d, (const S*)ca, (S*)cbuf, (S*)xf, s->z, s->r,
+              f.pcg_base, (const S*)f.dinv, f.dm, f.sinst, G, skq, sc});
+          else if(use_tma(f.A))
+            tma<V, S>(f.A, ca, BOpPost2<V, S, false>{(const S*)f.d, (const S*)ca, (S*)cbuf, (S*)xf, s->z, s->r,
+              f.pcg_base, (const S*)f.dinv, f.dm, f.sinst, G, skq, sc});
           else if(last)
             kb_post2<V, S, true><<<nblk(f.n, f.bs), f.bs, 0, st>>>(bview<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cbuf,
               (S*)xf, s->z, s->r, f.pcg_base, (const S*)f.dinv, f.dm, f.sinst, G, skq, sc);
@@ -823,7 +1332,13 @@ namespace bt
       if(!dry)
       {
         kb_pcg_p<<<nblk(s->np), BNT, 0, st>>>(s->p, s->z, s->sinst_top, s->np, first ? 1 : 0, sc);
-        kb_pcg_q<<<nblk(s->np), BNT, 0, st>>>(bview<double>(s->Atop), s->p, s->q, s->dm_top, s->sinst_top, sc);
+        if(BLaunch<double, double>::use_tma(s->Atop))
+        {
+          BLaunch<double, double> d64{s, st, false};
+          d64.template tma<double, double>(s->Atop, s->p, BOpPcgQ{s->q, s->p, s->dm_top, s->sinst_top, sc});
+        }
+        else
+          kb_pcg_q<<<nblk(s->np), BNT, 0, st>>>(bview<double>(s->Atop), s->p, s->q, s->dm_top, s->sinst_top, sc);
         kb_pcg_x<S><<<nblk(s->np), BNT, 0, st>>>(s->x, s->r, s->p, s->q, s->dm_top, tops(), s->mg_base_top,
           s->sinst_top, s->np, f64 ? 0 : 1, sc);
         kb_count<<<1, 256, 0, st>>>(sc, cond);
@@ -887,6 +1402,7 @@ namespace bt
   static fb_status build(fb_batch* s)
   {
     cudaStream_t st = s->stream;
+    BT_TRY((staged_attrs<V, S>()));
     if(s->cfg.rows_per_block > 0)
       for(auto& g : s->g)
         g.bs = std::max(32, std::min(BNT_MAX, (s->cfg.rows_per_block + 31) / 32 * 32));
@@ -898,6 +1414,7 @@ namespace bt
     }
     {
       BLaunch<V, S> a{s, st, true};
+      a.prime();
       a.init();
       a.vcycle();
       a.tail(true, 0);
@@ -1386,6 +1903,10 @@ fb_status fb_batch_create(fb_batch** out, int num, fb_hierarchy* const* hs, cons
     BT_TRY(bt::bmalloc(s.get(), (void**)&sc.skip_post, 4 * size_t(bt::MAXG) * J));
     BT_TRY(bt::bmalloc(s.get(), (void**)&sc.arrive, 64));
     BT_TRY(bt::bmalloc(s.get(), (void**)&sc.progress, 64));
+    BT_TRY(bt::bmalloc(s.get(), (void**)&s->err, 64));
+    int dev = 0;
+    FB_CUDA(cudaGetDevice(&dev));
+    FB_CUDA(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, dev));
     sc.tol_rel = cfg.tol_rel;
     sc.tol_abs = cfg.tol_abs;
     sc.div_rel = 1.0 / EPS64;
@@ -1424,7 +1945,15 @@ static fb_status batch_common(fb_batch* s, fb_solve_info* info)
   FB_CUDA(cudaMemcpyAsync(status.data(), s->sc.status, 4 * size_t(J), cudaMemcpyDeviceToHost, st));
   FB_CUDA(cudaMemcpyAsync(d0.data(), s->sc.def_init, 8 * size_t(J), cudaMemcpyDeviceToHost, st));
   FB_CUDA(cudaMemcpyAsync(d1.data(), s->sc.def_cur, 8 * size_t(J), cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  FB_CUDA(cudaMemcpyAsync(&err, s->err, sizeof(int), cudaMemcpyDeviceToHost, st));
   FB_CUDA(cudaStreamSynchronize(st));
+  if(err)
+  {
+    FB_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
+    set_error("batch_solve: a bounded wait for staged matrix data expired (results invalid)");
+    return FB_ERR_CUDA;
+  }
   float ms = 0.f;
   FB_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
   int maxit = 0;

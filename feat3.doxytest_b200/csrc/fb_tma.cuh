@@ -11,8 +11,17 @@
 
 #include "fb_rows.cuh"
 
+#include <type_traits>
+#include <utility>
+
 namespace fb
 {
+  // Op::block_done() exists: the epilogue finishes each block itself (instead of the grid reduction)
+  template<class T, class = void>
+  struct HasBlockDone : std::false_type {};
+  template<class T>
+  struct HasBlockDone<T, std::void_t<decltype(std::declval<const T&>().block_done())>> : std::true_type {};
+
   constexpr int TMA_NT = 256;          // threads = rows per chunk
   constexpr int TMA_STAGES = 3;   // pipeline depth, at most
   // Stages of a pass over values of type V: FP64 rows are wide, and two stages leave room for
@@ -350,6 +359,13 @@ namespace fb
         }
       }
       __syncthreads();
+    }
+    // an epilogue with its own end of block (the batched solver's per-instance reductions): every
+    // thread of every block that ran the loop calls it once
+    if constexpr(HasBlockDone<Op>::value)
+    {
+      op.block_done();
+      return;
     }
     if(!Op::REDUCES)
       return;
