@@ -50,9 +50,14 @@ def build():
         # the FEAT build on the library's binding links the built library
         if os.path.exists(os.path.join(os.path.dirname(HERE), "feat3.doxytest_b200", "featb200", "libfeatb200.so")):
             targets.append("b200")
-        # FEAT on its own CUDA backend (a timing column beside the library)
-        targets.append("cuda")
     subprocess.run(["make", "-s", "-j8", "-C", HERE, f"FEAT_REF={REF_SRC}"] + targets, check=True)
+    if os.path.isdir(REF_SRC):
+        # FEAT on its own CUDA backend: only a timing column beside the library, so a failure to
+        # build it (e.g. without the toolkit's cuSPARSE) leaves the checkers usable
+        r = subprocess.run(["make", "-s", "-j8", "-C", HERE, f"FEAT_REF={REF_SRC}", "cuda"], capture_output=True,
+                           text=True)
+        if r.returncode != 0:
+            print("oracle: FEAT's CUDA-backend build (feat_cuda) skipped:", (r.stderr or r.stdout).strip()[-300:])
 
 
 _lib = None
