@@ -464,7 +464,7 @@ def reference_sample(args):
 def run_reference_gpu(args):
     """The reference's own GPU backend (FEAT built with its CUDA sources: cuSPARSE SpMV, cuBLAS
     vector ops, managed memory, one synchronised launch per LAFEM op) on the default workload, FP64:
-    a timing column beside the library, not the driver's reference arm."""
+    a timing column beside the library, not the default reference arm (the generic CPU path)."""
     dim, level, rhs_kind, precision, desc = WORKLOADS[args.workload]
     from featb200 import assembly as AS
     if rhs_kind not in ("sine", "gauss"):

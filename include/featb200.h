@@ -35,7 +35,7 @@ typedef int fb_status;
 #define FB_ERR_CUDA 2         /* a CUDA runtime call failed */
 #define FB_ERR_STATE 3        /* object not initialised / wrong order of calls */
 #define FB_ERR_NOMEM 4        /* device allocation failed */
-#define FB_ERR_UNSUPPORTED 5  /* option not available in this build */
+#define FB_ERR_UNSUPPORTED 5  /* option not supported for this configuration */
 
 /* Solver status codes: the reference's Solver::Status (kernel/solver/base.hpp:48-64). */
 #define FB_SOLVER_UNDEFINED 0
