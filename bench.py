@@ -472,7 +472,14 @@ def run_reference_gpu(args):
                           "unavailable": "timed for the single-system workloads only"}))
         return 0
     gauss = AS.gauss_params(1, dim) if rhs_kind == "gauss" else None
-    res = cpu_reference_times(dim, level, rhs_kind, gauss, max(1, min(args.warmup + args.steps, 20)), backend="cuda")
+    try:
+        res = cpu_reference_times(dim, level, rhs_kind, gauss, max(1, min(args.warmup + args.steps, 20)),
+                                  backend="cuda")
+    except (subprocess.CalledProcessError, subprocess.TimeoutExpired) as e:
+        print(json.dumps({"impl": "reference", "reference_backend": "cuda",
+                          "unavailable": f"the reference's CUDA build did not run here ({type(e).__name__}; "
+                                         "it needs a GPU)"}))
+        return 0
     if res is None:
         print(json.dumps({"impl": "reference", "reference_backend": "cuda",
                           "unavailable": "oracle/_ref/feat_cuda is missing; build it with `make -C oracle cuda`"}))
