@@ -20,10 +20,24 @@ type-0 matrix with a type-1 vector, then `sync_0`.  `global_pcg` is `Solver::PCG
 types with the global Jacobi preconditioner (the type-1 diagonal from `sync_0` of the patch-local
 diagonals, `Solver::JacobiPrecond` with a global matrix).
 
+The multigrid on these types: `GlobalTransfer` is `Global::Transfer` (kernel/global/transfer.hpp:
+252-336): the patch-local restriction followed by `sync_0` of the coarse vector, the patch-local
+prolongation followed by `sync_0` of the fine vector, which is exact because the patch-local
+prolongation's rows are scaled by the inverse of the globally summed assembly weights
+(`prolongation_row_scaling`, control/scalar_basic.hpp:308-324).  `Muxer` is `Global::Muxer`
+(kernel/global/muxer.hpp:344-530): the coarse levels below a chosen level live on one parent rank,
+`join` gathers the children's type-0 vectors into the parent's merged vector, `split` hands the
+type-1 result back.  A rank that is a child but not the parent holds a ghost transfer: it sends its
+restriction (`rest_send`) and waits for the prolongation (`prol_recv`) while the parent runs the
+coarse levels (kernel/solver/multigrid.hpp:1783-1790, 1871-1877).  `GlobalMultiGrid` is the V-cycle
+with the Richardson-Jacobi smoother and an exact coarse solve on these global levels, in the
+operation order of the single-system solve, and `global_pcg` takes it as its preconditioner.
+
 Vectors are torch tensors: on CUDA devices with the NCCL backend the exchange runs over NVLink,
 on the CPU with gloo (the tests).  The exchange is point-to-point (`isend` / `irecv` of the gathered
-buffers) because only neighbours share DOFs.  The local matrix product is a callable, so that the
-product path can use the library's device SpMV and the tests a host CSR product.
+buffers) because only neighbours share DOFs; the muxer's join and split are a gather to and a
+scatter from the parent.  The local matrix, prolongation and restriction products are callables, so
+that the product path can use the library's device SpMV and the tests a host CSR product.
 """
 from __future__ import annotations
 
@@ -172,28 +186,279 @@ class GlobalUnitFilter:
         return v
 
 
+def prolongation_row_scaling(weight: torch.Tensor, gate: Gate) -> torch.Tensor:
+    """The row scaling of a patch-local prolongation (control/scalar_basic.hpp:308-324).  The patch
+    assembles its prolongation summed over its own coarse cells together with a weight vector that
+    counts, per fine DOF, the cells that contributed; the global weight is the `sync_0` of the patch
+    weights, and the patch's rows are scaled by its inverse.  A shared fine DOF then receives a part
+    of the global row on every sharing rank, and `sync_0` of the patch products is the global
+    prolongation.  Returns the scaling vector (type 1)."""
+    w = gate.sync_0(weight.clone())
+    return 1.0 / w
+
+
+class Muxer:
+    """Global::Muxer (kernel/global/muxer.hpp:69-533) with the whole process group as the sibling
+    communicator: every rank is a child, and rank `parent` holds the merged coarse levels.
+
+    Every rank sends the entries its parent mirror lists (`push_parent`; the patch's coarse DOFs);
+    the parent knows, per rank, where those entries sit in its merged vector (`push_child`, in rank
+    order).  `join` sums the children's type-0 vectors into the merged vector (gather, then
+    scatter-add in rank order: muxer.hpp:380-432), `split` hands each child its entries of the merged
+    type-1 vector (gather per child, scatter: muxer.hpp:481-530).  Buffers have the length of the
+    largest parent mirror over the ranks."""
+
+    def __init__(self, dist=None, parent=0):
+        self.dist, self.parent = dist, int(parent)
+        self.parent_mirror: torch.Tensor | None = None
+        self.child_mirrors: list[torch.Tensor] = []
+        self.bufsize = 0
+
+    def _size(self):
+        return 1 if self.dist is None else self.dist.get_world_size()
+
+    def _rank(self):
+        return 0 if self.dist is None else self.dist.get_rank()
+
+    def is_child(self) -> bool:
+        return self._size() > 1
+
+    def is_parent(self) -> bool:
+        return self._rank() == self.parent
+
+    def is_ghost(self) -> bool:
+        """A child that is not the parent holds no coarser level (muxer.hpp:249-252)."""
+        return self.is_child() and not self.is_parent()
+
+    def push_parent(self, mirror):
+        self.parent_mirror = torch.as_tensor(mirror, dtype=torch.long)
+
+    def push_child(self, mirror):
+        self.child_mirrors.append(torch.as_tensor(mirror, dtype=torch.long))
+
+    def compile(self, device="cpu"):
+        if self.parent_mirror is None:
+            raise ValueError("Muxer.compile: push_parent first")
+        if self.is_child() and self.is_parent() and len(self.child_mirrors) != self._size():
+            raise ValueError("Muxer.compile: the parent needs one child mirror per rank")
+        self.parent_mirror = self.parent_mirror.to(device)
+        self.child_mirrors = [m.to(device) for m in self.child_mirrors]
+        n = torch.tensor([self.parent_mirror.numel()], dtype=torch.int64, device=device)
+        if self.is_child():
+            self.dist.all_reduce(n, op=self.dist.ReduceOp.MAX)
+        self.bufsize = int(n.item())
+        self.device = device
+        return self
+
+    def _own_buffer(self, v: torch.Tensor) -> torch.Tensor:
+        buf = torch.zeros(self.bufsize, dtype=v.dtype, device=v.device)
+        buf[: self.parent_mirror.numel()] = v.index_select(0, self.parent_mirror)
+        return buf
+
+    def _from_buffer(self, buf: torch.Tensor, n_local: int) -> torch.Tensor:
+        v = torch.zeros(n_local, dtype=buf.dtype, device=buf.device)
+        return v.index_add_(0, self.parent_mirror, buf[: self.parent_mirror.numel()])
+
+    def join_send(self, v: torch.Tensor):
+        self.dist.gather(self._own_buffer(v), None, dst=self.parent)
+
+    def join(self, v: torch.Tensor, n_trg: int) -> torch.Tensor:
+        if not self.is_child():
+            return v.clone()
+        bufs = [torch.empty(self.bufsize, dtype=v.dtype, device=v.device) for _ in range(self._size())]
+        self.dist.gather(self._own_buffer(v), bufs, dst=self.parent)
+        trg = torch.zeros(n_trg, dtype=v.dtype, device=v.device)
+        for m, b in zip(self.child_mirrors, bufs):
+            trg.index_add_(0, m, b[: m.numel()])
+        return trg
+
+    def split_recv(self, n_local: int, dtype=torch.float64) -> torch.Tensor:
+        buf = torch.empty(self.bufsize, dtype=dtype, device=self.device)
+        self.dist.scatter(buf, None, src=self.parent)
+        return self._from_buffer(buf, n_local)
+
+    def split(self, v: torch.Tensor, n_local: int) -> torch.Tensor:
+        if not self.is_child():
+            return v.clone()
+        bufs = []
+        for m in self.child_mirrors:
+            b = torch.zeros(self.bufsize, dtype=v.dtype, device=v.device)
+            b[: m.numel()] = v.index_select(0, m)
+            bufs.append(b)
+        buf = torch.empty(self.bufsize, dtype=v.dtype, device=v.device)
+        self.dist.scatter(buf, bufs, src=self.parent)
+        return self._from_buffer(buf, n_local)
+
+
+class GlobalTransfer:
+    """Global::Transfer (kernel/global/transfer.hpp:252-336) between a fine level and the next
+    coarser one.
+
+    prol / rest: the patch-local products (callables returning new tensors): the row-scaled
+    prolongation (patch coarse -> patch fine) and its transpose.  gate_fine: the fine level's gate;
+    gate_coarse: the coarse level's gate (on the parent, the merged level's; unused on a ghost).
+    With a muxer the coarse level is merged on its parent: coarse_local_size is this rank's patch-local
+    coarse size, coarse_size the merged level's size on the parent."""
+
+    def __init__(self, prol, rest, gate_fine: Gate, gate_coarse: Gate | None = None, muxer: Muxer | None = None,
+                 coarse_local_size: int | None = None, coarse_size: int | None = None):
+        self._prol, self._rest = prol, rest
+        self.gate_fine, self.gate_coarse, self.muxer = gate_fine, gate_coarse, muxer
+        self.coarse_local_size, self.coarse_size = coarse_local_size, coarse_size
+        if muxer is not None and muxer.is_child() and coarse_local_size is None:
+            raise ValueError("GlobalTransfer: a muxed transfer needs coarse_local_size")
+
+    def _muxed(self) -> bool:
+        return self.muxer is not None and self.muxer.is_child()
+
+    def is_ghost(self) -> bool:
+        return self.muxer is not None and self.muxer.is_ghost()
+
+    def rest(self, vec_fine: torch.Tensor) -> torch.Tensor:
+        """Type-1 fine defect -> type-1 coarse defect."""
+        tmp = self._rest(vec_fine)
+        vec_coarse = self.muxer.join(tmp, self.coarse_size) if self._muxed() else tmp
+        if self.gate_coarse is not None:
+            self.gate_coarse.sync_0(vec_coarse)
+        return vec_coarse
+
+    def rest_send(self, vec_fine: torch.Tensor):
+        self.muxer.join_send(self._rest(vec_fine))
+
+    def prol(self, vec_coarse: torch.Tensor) -> torch.Tensor:
+        """Type-1 coarse vector -> type-1 fine vector."""
+        tmp = self.muxer.split(vec_coarse, self.coarse_local_size) if self._muxed() else vec_coarse
+        return self.gate_fine.sync_0(self._prol(tmp))
+
+    def prol_recv(self, dtype=torch.float64) -> torch.Tensor:
+        return self.gate_fine.sync_0(self._prol(self.muxer.split_recv(self.coarse_local_size, dtype)))
+
+
+def coarse_inverse(A: torch.Tensor, filter_idx):
+    """The exact coarse solve: the inverse of the dense coarse matrix restricted to its free
+    (unfiltered) DOFs; the solution is zero on the filtered DOFs."""
+    n = A.shape[0]
+    free = torch.ones(n, dtype=torch.bool, device=A.device)
+    free[torch.as_tensor(filter_idx, dtype=torch.long, device=A.device)] = False
+    inv = torch.linalg.inv(A[free][:, free])
+
+    def solve(b: torch.Tensor) -> torch.Tensor:
+        x = torch.zeros_like(b)
+        x[free] = inv @ b[free]
+        return x
+    return solve
+
+
+class GlobalMultiGrid:
+    """Solver::MultiGrid's V-cycle (kernel/solver/multigrid.hpp:1335-1350 with _apply_rest :1713-1838
+    and _apply_prol :1845-2000, fixed coarse-grid correction) on global levels, with `steps`
+    Richardson steps preconditioned by Jacobi omega / diag(A) (the global diagonal) as pre- and
+    post-smoother (kernel/solver/richardson.hpp:160-228) and an exact coarse solve.
+
+    levels: finest first, dicts with "matrix" (GlobalMatrix), "filter" (GlobalUnitFilter) and, on
+    every level but the coarsest, "transfer" (GlobalTransfer).  On a ghost rank the list ends with
+    the level whose transfer is a ghost; there `coarse_solve` is unused.  The coarse solve runs on
+    the coarsest level: the parent's merged one, or every rank's without a muxer."""
+
+    EPS = 2.220446049250313e-16
+
+    def __init__(self, levels, coarse_solve=None, omega=0.7, steps=2):
+        self.levels, self.coarse_solve, self.steps = levels, coarse_solve, int(steps)
+        last = levels[-1]
+        self.ghost = "transfer" in last and last["transfer"].is_ghost()
+        if not self.ghost and "transfer" in last:
+            raise ValueError("GlobalMultiGrid: the coarsest level has a transfer that is not a ghost")
+        if not self.ghost and coarse_solve is None:
+            raise ValueError("GlobalMultiGrid: the coarsest level needs a coarse solve")
+        self.dinv = []
+        for lv in levels:
+            if "transfer" in lv:
+                self.dinv.append(omega / lv["matrix"].diagonal())
+            else:
+                self.dinv.append(None)
+
+    def _smooth(self, k: int, rhs: torch.Tensor) -> torch.Tensor:
+        """Richardson from a zero start with the initial-defect test (iterative.hpp:492-507):
+        nothing to do for a non-finite or vanishing defect; min_iter = max_iter = steps."""
+        A, filt = self.levels[k]["matrix"], self.levels[k]["filter"]
+        out = torch.zeros_like(rhs)
+        d = rhs.clone()
+        def_init = A.gate.norm2(d)
+        if not math.isfinite(def_init) or def_init <= self.EPS * self.EPS:
+            return out
+        for _ in range(self.steps):
+            z = self.dinv[k] * d
+            filt.filter_cor(z)
+            out.add_(z)
+            A.apply_axpy(d, out, rhs, -1.0)
+            filt.filter_def(d)
+            if def_init > 1.0 / (self.EPS * self.EPS):
+                break                                # Status::diverged
+        return out
+
+    def vcycle(self, d: torch.Tensor) -> torch.Tensor:
+        """The correction for the type-1 defect d on the finest level."""
+        L = self.levels
+        n = len(L)
+        rhs, sol, dfc = [None] * n, [None] * n, [None] * n
+        rhs[0] = d.clone()
+        top = n - 2
+        for i in range(n - 1 if not self.ghost else n):
+            A, filt, T = L[i]["matrix"], L[i]["filter"], L[i]["transfer"]
+            sol[i] = self._smooth(i, rhs[i])
+            dfc[i] = torch.empty_like(rhs[i])
+            A.apply_axpy(dfc[i], sol[i], rhs[i], -1.0)
+            filt.filter_def(dfc[i])
+            if T.is_ghost():
+                T.rest_send(dfc[i])
+                top = i
+                break
+            rhs[i + 1] = T.rest(dfc[i])
+            L[i + 1]["filter"].filter_def(rhs[i + 1])
+        if not self.ghost:
+            sol[n - 1] = self.coarse_solve(rhs[n - 1])
+        for i in range(top, -1, -1):
+            A, filt, T = L[i]["matrix"], L[i]["filter"], L[i]["transfer"]
+            cor = T.prol_recv(d.dtype) if T.is_ghost() else T.prol(sol[i + 1])
+            filt.filter_def(cor)
+            sol[i].add_(cor)
+            A.apply_axpy(dfc[i], sol[i], rhs[i], -1.0)
+            filt.filter_def(dfc[i])
+            sol[i].add_(self._smooth(i, dfc[i]))
+        return sol[0]
+
+    __call__ = vcycle
+
+
 def global_pcg(A: GlobalMatrix, filt: GlobalUnitFilter, rhs: torch.Tensor, x: torch.Tensor, omega=1.0,
-               tol_rel=1e-8, max_iter=1000):
-    """Solver::PCG (kernel/solver/pcg.hpp:188-286) on global vectors with the global Jacobi
-    preconditioner omega / diag(A) (kernel/solver/jacobi_precond.hpp:136-165).  rhs and x are type 1;
-    x holds the initial guess and receives the solution.  Returns (iterations, def_init, def_final,
+               tol_rel=1e-8, max_iter=1000, precond=None):
+    """Solver::PCG (kernel/solver/pcg.hpp:188-286) on global vectors.  The preconditioner is
+    `precond` (a callable on a type-1 defect, e.g. a `GlobalMultiGrid`) or, when None, the global
+    Jacobi omega / diag(A) (kernel/solver/jacobi_precond.hpp:136-165).  rhs and x are type 1; x holds
+    the initial guess and receives the solution.  Returns (iterations, def_init, def_final,
     converged)."""
     gate = A.gate
-    dinv = omega / A.diagonal()
-    filt.filter_cor(dinv)                       # the filtered rows never contribute
+    if precond is None:
+        dinv = omega / A.diagonal()
+        filt.filter_cor(dinv)                   # the filtered rows never contribute
+
+        def precond(v):
+            return dinv * v
     r = torch.empty_like(x)
     A.apply_axpy(r, x, rhs, -1.0)
     filt.filter_def(r)
-    z = dinv * r
+    d0 = gate.norm2(r)
+    dc = d0
+    if not math.isfinite(d0):
+        return 0, d0, dc, False                 # Status::aborted
+    if d0 <= GlobalMultiGrid.EPS * GlobalMultiGrid.EPS:
+        return 0, d0, dc, True
+    z = precond(r)
     filt.filter_cor(z)
     p = z.clone()
     gamma = gate.dot(r, z)
-    d0 = gate.norm2(r)
-    dc = d0
     q = torch.empty_like(x)
     it = 0
-    if d0 <= 0.0:
-        return 0, d0, dc, True
     while it < max_iter:
         A.apply(q, p)
         filt.filter_def(q)
@@ -204,7 +469,7 @@ def global_pcg(A: GlobalMatrix, filt: GlobalUnitFilter, rhs: torch.Tensor, x: to
         dc = gate.norm2(r)
         if dc <= tol_rel * d0:
             return it, d0, dc, True
-        z = dinv * r
+        z = precond(r)
         filt.filter_cor(z)
         gamma_new = gate.dot(r, z)
         p = z + (gamma_new / gamma) * p

@@ -176,3 +176,248 @@ def test_global_pcg_on_device_one_rank(featlib, cuda):
     xr, itr = _pcg_reference(Ag, bg, bnd)
     assert ok and it == itr
     assert float(np.abs(x.cpu().numpy() - xr).max() / np.abs(xr).max()) <= 1e-12
+
+
+# --- the global multigrid: Global::Transfer, Global::Muxer and the V-cycle on global levels ---
+
+def _patch_vertices(level, rank):
+    N = 2 ** level
+    vx = np.arange((N + 1) ** 2) % (N + 1)
+    return np.nonzero(vx <= N // 2)[0] if rank == 0 else np.nonzero(vx >= N // 2)[0]
+
+
+def _prolongation_cells(level_f, csel):
+    """Assembly::GridTransfer::assemble_prolongation over the selected coarse cells of level_f - 1:
+    every coarse cell adds the bilinear interpolation weights of the 3x3 fine vertices it covers, and
+    1 to the weight of each of them.  Returns the summed matrix and the weight vector."""
+    Nf = 2 ** level_f
+    Nc = Nf // 2
+    _, idx = AS._cells(level_f - 1, 2)
+    cx, cy = idx[0][csel], idx[1][csel]
+    rows, cols, vals, wrows = [], [], [], []
+    for a in range(3):
+        for b in range(3):
+            fine = (2 * cy + b) * (Nf + 1) + 2 * cx + a
+            wrows.append(fine)
+            for p in range(2):
+                for q in range(2):
+                    v = (a / 2.0 if p else 1.0 - a / 2.0) * (b / 2.0 if q else 1.0 - b / 2.0)
+                    if v != 0.0:
+                        rows.append(fine)
+                        cols.append((cy + q) * (Nc + 1) + cx + p)
+                        vals.append(np.full(fine.size, v))
+    P = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=((Nf + 1) ** 2, (Nc + 1) ** 2)).tocsr()
+    P.sum_duplicates()
+    P.sort_indices()
+    w = np.bincount(np.concatenate(wrows), minlength=(Nf + 1) ** 2).astype(np.float64)
+    return P, w
+
+
+def _mg_levels(rank, merge, dist):
+    """Rank's global levels, finest first: levels LEVEL..merge+1 split into the two patches, levels
+    merge..1 merged on rank 0 (the muxer's parent) and absent on rank 1 (a ghost below merge + 1)."""
+    import torch
+    from featb200.global_layer import (Gate, GlobalMatrix, GlobalTransfer, GlobalUnitFilter, Muxer,
+                                       coarse_inverse, prolongation_row_scaling)
+
+    def csr_op(M):
+        return lambda v: torch.tensor(M @ v.numpy())
+
+    levels = []
+    for lv in range(LEVEL, merge, -1):
+        mine, Al, _, shared, bnd = _patch(lv, rank)
+        gate = Gate(dist)
+        gate.push(1 - rank, shared)
+        gate.compile(len(mine))
+        levels.append({"matrix": GlobalMatrix(csr_op(Al), gate, torch.tensor(Al.diagonal())),
+                       "filter": GlobalUnitFilter(bnd), "mine": mine})
+    parent = rank == 0
+    if parent:
+        for lv in range(merge, 0, -1):
+            A, _, bnd = _global_problem(lv)
+            levels.append({"matrix": GlobalMatrix(csr_op(A), Gate(None).compile(A.shape[0]),
+                                                  torch.tensor(A.diagonal())),
+                           "filter": GlobalUnitFilter(bnd)})
+    # transfers: patch -> patch, the muxed patch -> merged one, merged -> merged
+    for k in range(len(levels) - (0 if not parent else 1)):
+        lv = LEVEL - k
+        fine = levels[k]
+        if lv > merge:
+            mine_f = fine["mine"]
+            Nc = 2 ** (lv - 1)
+            _, cidx = AS._cells(lv - 1, 2)
+            csel = (cidx[0] < Nc // 2) if rank == 0 else (cidx[0] >= Nc // 2)
+            Psum, w = _prolongation_cells(lv, csel)
+            mine_c = _patch_vertices(lv - 1, rank)
+            Ploc = Psum[mine_f][:, mine_c]
+            s = prolongation_row_scaling(torch.tensor(w[mine_f]), fine["matrix"].gate).numpy()
+            Ploc = sp.diags(s) @ Ploc
+            Rloc = Ploc.T.tocsr()
+            if lv - 1 > merge:
+                T = GlobalTransfer(csr_op(Ploc), csr_op(Rloc), fine["matrix"].gate, levels[k + 1]["matrix"].gate)
+            else:
+                mux = Muxer(dist, parent=0)
+                mux.push_parent(np.arange(mine_c.size))
+                if parent:
+                    for r in range(2):
+                        mux.push_child(_patch_vertices(lv - 1, r))
+                mux.compile()
+                T = GlobalTransfer(csr_op(Ploc), csr_op(Rloc), fine["matrix"].gate,
+                                   levels[k + 1]["matrix"].gate if parent else None, mux,
+                                   coarse_local_size=mine_c.size, coarse_size=(Nc + 1) ** 2)
+        else:
+            P = AS.prolongation(lv)
+            T = GlobalTransfer(csr_op(P), csr_op(P.T.tocsr()), fine["matrix"].gate, levels[k + 1]["matrix"].gate)
+        fine["transfer"] = T
+    coarse = None
+    if parent:
+        A1, _, bnd1 = _global_problem(1)
+        coarse = coarse_inverse(torch.tensor(A1.toarray()), bnd1)
+    return levels, coarse
+
+
+def _mg_worker(rank, world, port, q, merges):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from featb200.global_layer import GlobalMultiGrid, global_pcg
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        out = {}
+        for merge in merges:
+            levels, coarse = _mg_levels(rank, merge, dist)
+            mg = GlobalMultiGrid(levels, coarse, omega=0.7, steps=2)
+            top = levels[0]
+            mine = top["mine"]
+            # one V-cycle on a fixed (filtered, type-1) defect
+            Ag, bg, bndg = _global_problem(LEVEL)
+            dg = np.sin(np.arange(bg.size) * 0.61)
+            dg[bndg] = 0.0
+            z = mg.vcycle(torch.tensor(dg[mine]))
+            # PCG preconditioned by the global multigrid, from the patch load vectors
+            _, _, bl, _, _ = _patch(LEVEL, rank)
+            b = top["matrix"].gate.sync_0(torch.tensor(bl))
+            top["filter"].filter_def(b)
+            x = torch.zeros(len(mine), dtype=torch.float64)
+            it, d0, dc, ok = global_pcg(top["matrix"], top["filter"], b, x, tol_rel=1e-8, max_iter=100,
+                                        precond=mg)
+            out[merge] = (mine, z.numpy(), x.numpy(), it, ok, mg.ghost)
+        q.put((rank, out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_prolongation_assembly_weights_give_the_interpolation():
+    """The summed cell contributions divided by the weights are the Q1 interpolation, on the whole
+    mesh and, after prolongation_row_scaling's global weights, as the sum of the two patches."""
+    import torch
+    from featb200.global_layer import Gate, prolongation_row_scaling
+    for lv in (2, 5):
+        Nc = 2 ** (lv - 1)
+        _, cidx = AS._cells(lv - 1, 2)
+        Psum, w = _prolongation_cells(lv, np.ones(Nc * Nc, dtype=bool))
+        P = AS.prolongation(lv)
+        assert abs(sp.diags(1.0 / w) @ Psum - P).max() == 0.0
+        parts = [_prolongation_cells(lv, (cidx[0] < Nc // 2) if r == 0 else (cidx[0] >= Nc // 2)) for r in range(2)]
+        wsum = parts[0][1] + parts[1][1]        # what sync_0 forms on the shared DOFs
+        Pg = sp.diags(1.0 / wsum) @ (parts[0][0] + parts[1][0])
+        assert abs(Pg - P).max() == 0.0
+    g = Gate(None).compile(3)
+    s = prolongation_row_scaling(torch.tensor([2.0, 4.0, 1.0], dtype=torch.float64), g)
+    assert torch.equal(s, torch.tensor([0.5, 0.25, 1.0], dtype=torch.float64))
+
+
+def test_global_multigrid_two_patches_gloo(oracle_lib):
+    """Two gloo ranks, each holding one half of the 2D Q1 hierarchy (levels 5..merge+1) with the
+    levels merge..1 muxed onto rank 0 (merge 4: only the finest level is split): one global V-cycle and the multigrid-preconditioned global PCG
+    against the oracle's single-system V-cycle and PCG on the whole hierarchy (same operation
+    order; only the split sums of the shared rows differ in rounding)."""
+    from helpers import rel_err
+    merges = (1, 3, 4)
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mg_worker, args=(r, world, port, q, merges)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    O = oracle_lib
+    lv_ref = []
+    for lv in range(LEVEL, 0, -1):
+        A, _, bnd = _global_problem(lv)
+        d = {"A": O.Csr.of(A.indptr, A.indices, A.data, A.shape), "filter_idx": bnd.astype(np.uint64)}
+        if lv > 1:
+            P = AS.prolongation(lv)
+            R = P.T.tocsr()
+            d["P"] = O.Csr.of(P.indptr, P.indices, P.data, P.shape)
+            d["R"] = O.Csr.of(R.indptr, R.indices, R.data, R.shape)
+        lv_ref.append(d)
+    mg = O.MultigridPCG(lv_ref, 0.7, 2)
+    Ag, bg, bndg = _global_problem(LEVEL)
+    dg = np.sin(np.arange(bg.size) * 0.61)
+    dg[bndg] = 0.0
+    z_ref = mg.vcycle(dg)
+    b = bg.copy()
+    b[bndg] = 0.0
+    x_ref, info = mg.solve(b, tol_rel=1e-8, max_iter=100)
+    assert info["status"] == "success"
+    for merge in merges:
+        for rank in range(world):
+            mine, z, x, it, ok, ghost = res[rank][merge]
+            assert ghost == (rank == 1)
+            assert rel_err(z, z_ref[mine]) <= 1e-13, (merge, rank, rel_err(z, z_ref[mine]))
+            assert ok and it == info["iters"], (merge, rank, it, info["iters"])
+            assert rel_err(x, x_ref[mine]) <= 1e-12, (merge, rank, rel_err(x, x_ref[mine]))
+
+
+@pytest.mark.gpu
+def test_global_multigrid_on_device_one_rank(featlib, cuda, oracle_lib):
+    """The device form of the global multigrid with one rank: every patch product (matrix,
+    prolongation, restriction) through the library's CSR kernel on CUDA tensors; same iterations as
+    the oracle's PCG-multigrid and the same solution to rounding."""
+    torch = cuda
+    O = oracle_lib
+    from featb200.global_layer import (Gate, GlobalMatrix, GlobalMultiGrid, GlobalTransfer, GlobalUnitFilter,
+                                       coarse_inverse, device_csr_apply, global_pcg)
+    from featb200.lafem import SparseMatrixCSR
+    from helpers import rel_err
+    levels, lv_ref = [], []
+    for lv in range(LEVEL, 0, -1):
+        A, _, bnd = _global_problem(lv)
+        gate = Gate(None).compile(A.shape[0], device="cuda")
+        levels.append({"matrix": GlobalMatrix(device_csr_apply(SparseMatrixCSR.from_scipy(A)), gate,
+                                              torch.tensor(A.diagonal(), device="cuda")),
+                       "filter": GlobalUnitFilter(bnd).to("cuda")})
+        d = {"A": O.Csr.of(A.indptr, A.indices, A.data, A.shape), "filter_idx": bnd.astype(np.uint64)}
+        if lv > 1:
+            P = AS.prolongation(lv)
+            R = P.T.tocsr()
+            levels[-1]["P"] = (P, R)
+            d["P"] = O.Csr.of(P.indptr, P.indices, P.data, P.shape)
+            d["R"] = O.Csr.of(R.indptr, R.indices, R.data, R.shape)
+        lv_ref.append(d)
+    for k in range(len(levels) - 1):
+        P, R = levels[k].pop("P")
+        levels[k]["transfer"] = GlobalTransfer(device_csr_apply(SparseMatrixCSR.from_scipy(P)),
+                                               device_csr_apply(SparseMatrixCSR.from_scipy(R)),
+                                               levels[k]["matrix"].gate, levels[k + 1]["matrix"].gate)
+    A1, _, bnd1 = _global_problem(1)
+    mg = GlobalMultiGrid(levels, coarse_inverse(torch.tensor(A1.toarray(), device="cuda"), bnd1), 0.7, 2)
+    Ag, bg, bndg = _global_problem(LEVEL)
+    b = bg.copy()
+    b[bndg] = 0.0
+    x = torch.zeros(bg.size, dtype=torch.float64, device="cuda")
+    it, d0, dc, ok = global_pcg(levels[0]["matrix"], levels[0]["filter"], torch.tensor(b, device="cuda"), x,
+                                tol_rel=1e-8, max_iter=100, precond=mg)
+    ref = O.MultigridPCG(lv_ref, 0.7, 2)
+    x_ref, info = ref.solve(b, tol_rel=1e-8, max_iter=100)
+    assert ok and it == info["iters"]
+    assert rel_err(x.cpu().numpy(), x_ref) <= 1e-12
