@@ -264,6 +264,35 @@ def batch_instance(level, k):
     return poisson_hierarchy(level, 2, rhs="gauss", gauss=g, field=f)
 
 
+def gauss_load_vector(level, params, dim=2):
+    """load_vector of the Gaussian sum `params` (gauss_params rows), formed by direction: each
+    Gaussian, the Gauss rule and the Q1 basis factor into one factor per coordinate, so
+    b = sum_k a_k (B_k,z (x) B_k,y (x) B_k,x) with B_k,d[i] the 1D load vector of the k-th Gaussian's
+    factor in direction d.  The same integral as load_vector with gauss_eval, to rounding, in
+    O(count x vertices) instead of O(count x cells x 3^dim)."""
+    N = 2 ** level
+    h = 1.0 / N
+    e = np.arange(N)
+    xq = (e[:, None] + (1.0 + GL3_X[None, :]) / 2.0) * h                # [cells, q], 1D
+    phi = np.stack([(1.0 - GL3_X) / 2.0, (1.0 + GL3_X) / 2.0])          # [local vertex, q]
+    b = np.zeros((N + 1,) * dim)
+    for row in params:
+        w, a = row[dim], row[dim + 1]
+        term = None
+        for d in range(dim):
+            g = np.exp(-((xq - row[d]) ** 2) / (2.0 * w * w))            # [cells, q]
+            loc = (h / 2.0) * np.einsum("cq,q,vq->cv", g, GL3_W, phi)
+            B = np.zeros(N + 1)
+            B[:-1] += loc[:, 0]
+            B[1:] += loc[:, 1]
+            # x fastest: direction d is axis dim-1-d of the vertex array
+            shape = [1] * dim
+            shape[dim - 1 - d] = N + 1
+            term = B.reshape(shape) if term is None else term * B.reshape(shape)
+        b += a * term
+    return b.ravel()
+
+
 def rhs64_params(j, dim=3):
     """Gaussian right-hand side j (0..63) of the many-right-hand-side 3D set (seeds 100..163)."""
     return gauss_params(100 + j, dim, width=(0.03, 0.12) if dim == 3 else (0.02, 0.1))
@@ -276,8 +305,7 @@ def rhs64_family(level=6, dim=3, k=64):
     fidx = levels[0]["filter"].indices.astype(np.int64)
     B = np.zeros((levels[0]["matrix"].rows(), k))
     for j in range(k):
-        g = rhs64_params(j, dim)
-        b = load_vector(level, lambda *xs: gauss_eval(g, *xs), dim)
+        b = gauss_load_vector(level, rhs64_params(j, dim), dim)
         b[fidx] = 0.0
         B[:, j] = b
     return levels, B

@@ -56,3 +56,15 @@ def test_field_statistics():
     vals = np.concatenate([AS.field_eval_grid(AS.field_params(s), xs, xs).ravel() for s in range(40)])
     assert abs(vals.mean()) < 0.1
     assert abs(vals.std() - 1.0) < 0.1
+
+
+@pytest.mark.parametrize("dim,level", [(2, 5), (2, 7), (3, 3), (3, 5)])
+def test_gauss_load_vector_by_direction(dim, level):
+    """The Gaussian load vector formed by direction equals the cell-wise Gauss-rule assembly to
+    rounding (the same integral, factored per coordinate)."""
+    from featb200 import assembly as AS
+    for seed in (0, 17, 63):
+        g = AS.rhs64_params(seed, dim) if dim == 3 else AS.gauss_params(seed, 2)
+        ref = AS.load_vector(level, lambda *xs: AS.gauss_eval(g, *xs), dim)
+        b = AS.gauss_load_vector(level, g, dim)
+        assert np.abs(b - ref).max() <= 1e-14 * np.abs(ref).max()
