@@ -28,6 +28,11 @@ namespace mr
   constexpr int MW = MNT / 32;            // warps (rows in flight) per block
   constexpr int KMAX = 64;
 
+  // A matrix in CSR form and, for a system matrix whose stored rows all share one pattern of 9 or
+  // 27 column offsets made of triplets (o-1, o, o+1) -- the Q1 stencil of a lexicographically
+  // numbered grid -- also in stencil form: dval[k * dn + row] is entry k of the row (zeros for rows
+  // stored empty and for the padding up to dn, a multiple of 8), goff[g] the centre offset of
+  // triplet g.  nd = 0: CSR only.
   template<typename V>
   struct MCsr
   {
@@ -35,7 +40,15 @@ namespace mr
     const uint32_t* col;
     const V* val;
     uint32_t rows;
+    const V* dval;
+    uint32_t dn;
+    int nd;
+    int goff[9];
   };
+
+  // rows per warp in the stencil form: the strip's rows share their x gathers (M + 2 row loads per
+  // triplet for M rows instead of 3 M); 4 for FP64 values to bound the registers
+  template<typename V> struct StripRows { static constexpr int value = sizeof(V) == 8 ? 4 : 8; };
 
   struct MScal
   {
@@ -132,6 +145,114 @@ namespace mr
     }
   }
 
+  // the strip's M values of one diagonal (uniform loads: every lane reads the same 16 bytes)
+  template<int M>
+  __device__ __forceinline__ void ldg_diag(const float* p, float (&v)[M])
+  {
+    #pragma unroll
+    for(int i = 0; i < M; i += 4)
+    {
+      const float4 t = __ldg(reinterpret_cast<const float4*>(p + i));
+      v[i] = t.x;
+      v[i + 1] = t.y;
+      v[i + 2] = t.z;
+      v[i + 3] = t.w;
+    }
+  }
+  template<int M>
+  __device__ __forceinline__ void ldg_diag(const double* p, double (&v)[M])
+  {
+    #pragma unroll
+    for(int i = 0; i < M; i += 2)
+    {
+      const double2 t = __ldg(reinterpret_cast<const double2*>(p + i));
+      v[i] = t.x;
+      v[i + 1] = t.y;
+    }
+  }
+
+  // Stencil form, G triplets per row: one warp takes M consecutive rows r0..r0+M-1.  For triplet g
+  // the rows need the x rows r0-1+goff[g] .. r0+M+goff[g]; each is loaded once and added to the (up
+  // to three) rows whose entry it is.  Row m receives its entries in ascending column order
+  // (triplets in order, then o-1, o, o+1), which is the stored CSR order, so every row sum equals
+  // mrow's bit for bit.  x rows outside [0, rows) are read only by rows stored empty (their values
+  // are zero); they are not loaded.  epi(row, sum) runs for every row < rows.
+  template<typename V, typename S, int R, int G, class Epi>
+  __device__ __forceinline__ void strip_rows(const MCsr<V>& A, const S* __restrict__ x, Epi& epi)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    constexpr int M = StripRows<V>::value;
+    constexpr int K = 32 * R;
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = A.rows;
+    const uint32_t nstrips = (n + M - 1) / M;
+    for(uint32_t st = blockIdx.x * MW + (threadIdx.x >> 5); st < nstrips; st += gridDim.x * MW)
+    {
+      const uint32_t r0 = st * M;
+      Ac sum[M][R];
+      #pragma unroll
+      for(int m = 0; m < M; ++m)
+        #pragma unroll
+        for(int r = 0; r < R; ++r)
+          sum[m][r] = Ac(0);
+      #pragma unroll
+      for(int g = 0; g < G; ++g)
+      {
+        V v[3][M];
+        #pragma unroll
+        for(int dx = 0; dx < 3; ++dx)
+          ldg_diag<M>(A.dval + size_t(3 * g + dx) * A.dn + r0, v[dx]);
+        const int64_t base = int64_t(r0) - 1 + A.goff[g];
+        #pragma unroll
+        for(int t = 0; t < M + 2; ++t)
+        {
+          const int64_t xr = base + t;
+          S xv[R];
+          if(xr >= 0 && xr < int64_t(n))
+            ldg_row<S, R>(x + size_t(xr) * K + lane * R, xv);
+          else
+          {
+            #pragma unroll
+            for(int r = 0; r < R; ++r)
+              xv[r] = S(0);
+          }
+          #pragma unroll
+          for(int m = t - 2; m <= t; ++m)
+          {
+            if(m < 0 || m >= M)
+              continue;
+            const Ac vk = Ac(v[t - m][m]);
+            #pragma unroll
+            for(int r = 0; r < R; ++r)
+              sum[m][r] = add(sum[m][r], mul(vk, Ac(xv[r])));
+          }
+        }
+      }
+      #pragma unroll
+      for(int m = 0; m < M; ++m)
+        if(r0 + uint32_t(m) < n)
+          epi(r0 + uint32_t(m), sum[m]);
+    }
+  }
+
+  // epi(row, sum) for every row of A with sum = (A x)[row], in the stencil form where A has one
+  template<typename V, typename S, int R, class Epi>
+  __device__ __forceinline__ void for_rows(const MCsr<V>& A, const S* __restrict__ x, Epi epi)
+  {
+    typedef typename ValueTraits<V>::acc Ac;
+    if(A.nd == 27)
+      strip_rows<V, S, R, 9>(A, x, epi);
+    else if(A.nd == 9)
+      strip_rows<V, S, R, 3>(A, x, epi);
+    else
+      for(uint32_t row = blockIdx.x * MW + (threadIdx.x >> 5); row < A.rows; row += gridDim.x * MW)
+      {
+        Ac sum[R];
+        mrow<V, S, R>(A, row, x, sum);
+        epi(row, sum);
+      }
+  }
+
   // block partials per right-hand side (smem), atomically added to sc->acc; the last block calls
   // fin(j, total) for every j < K and clears the accumulators.  Returns true in the last block.
   template<int R, class Fin>
@@ -184,10 +305,8 @@ namespace mr
     if(closed(sc))
       return;
     const int lane = threadIdx.x & 31;
-    MR_ROWS(A.rows)
+    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
-      Ac sum[R];
-      mrow<V, S, R>(A, row, x, sum);
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
       #pragma unroll
@@ -203,7 +322,7 @@ namespace mr
         }
         xo[e] = out;
       }
-    }
+    });
   }
 
   template<typename V, typename S, int R>
@@ -215,10 +334,8 @@ namespace mr
     if(closed(sc))
       return;
     const int lane = threadIdx.x & 31;
-    MR_ROWS(A.rows)
+    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
-      Ac sum[R];
-      mrow<V, S, R>(A, row, x, sum);
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
       for(int r = 0; r < R; ++r)
@@ -226,7 +343,7 @@ namespace mr
         const size_t e = size_t(row) * K + lane * R + r;
         dv[e] = d ? S(0) : S(sub(Ac(b[e]), sum[r]));
       }
-    }
+    });
   }
 
   template<typename V, typename S, int R>
@@ -325,10 +442,8 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    MR_ROWS(A.rows)
+    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
-      Ac sum[R];
-      mrow<V, S, R>(A, row, x, sum);
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
       #pragma unroll
@@ -341,7 +456,7 @@ namespace mr
         cv[e] = S(add(Ac(0), c));
         part[r] += double(dd) * double(dd);
       }
-    }
+    });
     reduce_per_rhs<R>(part, sc, [&](int j, double tot) { skip[j] = skip_of<S>(sqrt(tot)); });
   }
 
@@ -359,10 +474,8 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    MR_ROWS(A.rows)
+    for_rows<V, S, R>(A, cv, [&](uint32_t row, const Ac (&sum)[R])
     {
-      Ac sum[R];
-      mrow<V, S, R>(A, row, cv, sum);
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
       #pragma unroll
@@ -392,7 +505,7 @@ namespace mr
             x[e] = xn;
         }
       }
-    }
+    });
     if(!(LAST && TOP))
       return;
     reduce_per_rhs<R>(part, sc, [&](int j, double tot)
@@ -424,10 +537,8 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    MR_ROWS(A.rows)
+    for_rows<double, double, R>(A, x, [&](uint32_t row, const double (&sum)[R])
     {
-      double sum[R];
-      mrow<double, double, R>(A, row, x, sum);
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
       for(int r = 0; r < R; ++r)
@@ -442,7 +553,7 @@ namespace mr
         }
         part[r] += mul(rv, rv);
       }
-    }
+    });
     reduce_per_rhs<R>(part, sc, [&](int j, double tot)
     {
       const double d0 = sqrt(tot);
@@ -533,10 +644,8 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    MR_ROWS(A.rows)
+    for_rows<double, double, R>(A, p, [&](uint32_t row, const double (&sum)[R])
     {
-      double sum[R];
-      mrow<double, double, R>(A, row, p, sum);
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
       for(int r = 0; r < R; ++r)
@@ -546,7 +655,7 @@ namespace mr
         q[e] = qv;
         part[r] += mul(qv, p[e]);
       }
-    }
+    });
     reduce_per_rhs<R>(part, sc, [&](int j, double tot) { sc->alpha[j] = sc->gamma[j] / tot; });
   }
 
@@ -675,6 +784,10 @@ struct fb_msolver
     uint32_t rows = 0, cols = 0, nnz = 0;
     uint32_t *rp = nullptr, *col = nullptr;
     void* val = nullptr;
+    void* dval = nullptr;                  // stencil form (nd = 9 or 27), see mr::MCsr
+    uint32_t dn = 0;
+    int nd = 0;
+    int goff[9] = {};
   };
   struct Level
   {
@@ -728,8 +841,11 @@ namespace mr
     if(t_ != FB_OK) return t_;        \
   } while(0)
 
+  static fb_status upload_stencil(fb_msolver* s, fb_msolver::Mat& d, const std::vector<uint32_t>& rp,
+    const std::vector<uint32_t>& col, const std::vector<double>& val, int prec, bool use);
+
   static fb_status upload(fb_msolver* s, fb_msolver::Mat& d, const HostCsr& M, int prec,
-    const std::vector<uint8_t>* empty)
+    const std::vector<uint8_t>* empty, bool stencil = false)
   {
     std::vector<uint32_t> rp(size_t(M.rows) + 1, 0), col;
     std::vector<double> val;
@@ -763,12 +879,77 @@ namespace mr
         FB_CUDA(cudaMemcpy(d.val, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
       }
     }
+    return upload_stencil(s, d, rp, col, val, prec, stencil);
+  }
+
+  // The stencil form of a system matrix (see MCsr): every stored row has the same column offsets,
+  // 9 or 27 of them in triplets (o-1, o, o+1) with increasing centres.  Leaves d.nd = 0 when the
+  // pattern does not hold (another numbering, another element) or use is 0.
+  static fb_status upload_stencil(fb_msolver* s, fb_msolver::Mat& d, const std::vector<uint32_t>& rp,
+    const std::vector<uint32_t>& col, const std::vector<double>& val, int prec, bool use)
+  {
+    d.nd = 0;
+    if(!use)
+      return FB_OK;
+    std::vector<int64_t> off;
+    for(uint32_t r = 0; r < d.rows; ++r)
+    {
+      const uint32_t len = rp[r + 1] - rp[r];
+      if(len == 0)
+        continue;
+      if(off.empty())
+      {
+        if(len != 9 && len != 27)
+          return FB_OK;
+        for(uint32_t j = rp[r]; j < rp[r + 1]; ++j)
+          off.push_back(int64_t(col[j]) - int64_t(r));
+        for(size_t g = 0; g < off.size() / 3; ++g)
+        {
+          if(off[3 * g] + 1 != off[3 * g + 1] || off[3 * g + 1] + 1 != off[3 * g + 2])
+            return FB_OK;
+          if(g > 0 && off[3 * g] <= off[3 * g - 1])
+            return FB_OK;
+          if(off[3 * g + 1] > INT32_MAX || off[3 * g + 1] < -INT32_MAX)
+            return FB_OK;
+        }
+        continue;
+      }
+      if(len != off.size())
+        return FB_OK;
+      for(uint32_t j = rp[r], k = 0; j < rp[r + 1]; ++j, ++k)
+        if(int64_t(col[j]) - int64_t(r) != off[k])
+          return FB_OK;
+    }
+    if(off.empty())
+      return FB_OK;
+    const int nd = int(off.size());
+    const uint32_t dn = (d.rows + 7u) & ~7u;
+    std::vector<double> dv(size_t(nd) * dn, 0.0);
+    for(uint32_t r = 0; r < d.rows; ++r)
+      for(uint32_t j = rp[r], k = 0; j < rp[r + 1]; ++j, ++k)
+        dv[size_t(k) * dn + r] = val[j];
+    const size_t vb = prec == FB_PREC_F64 ? 8 : 4;
+    MR_TRY(malloc0(s, &d.dval, vb * dv.size()));
+    if(prec == FB_PREC_F64)
+      FB_CUDA(cudaMemcpy(d.dval, dv.data(), 8 * dv.size(), cudaMemcpyHostToDevice));
+    else
+    {
+      std::vector<float> f(dv.begin(), dv.end());
+      FB_CUDA(cudaMemcpy(d.dval, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
+    }
+    d.dn = dn;
+    d.nd = nd;
+    for(int g = 0; g < nd / 3; ++g)
+      d.goff[g] = int(off[size_t(3 * g + 1)]);
     return FB_OK;
   }
 
   template<typename V> MCsr<V> mv(const fb_msolver::Mat& m)
   {
-    return MCsr<V>{m.rp, m.col, static_cast<const V*>(m.val), m.rows};
+    MCsr<V> c{m.rp, m.col, static_cast<const V*>(m.val), m.rows, static_cast<const V*>(m.dval), m.dn, m.nd, {}};
+    for(int g = 0; g < 9; ++g)
+      c.goff[g] = m.goff[g];
+    return c;
   }
 
   template<typename V, typename S, int R>
@@ -785,10 +966,20 @@ namespace mr
     {
       return std::max(1u, std::min(s->grid, (rows + MW - 1) / MW));
     }
-    double mb(const fb_msolver::Mat& m) const
+    // blocks of a pass over a system matrix: one warp per row, or per strip in the stencil form
+    template<typename W> unsigned int ga(const fb_msolver::Mat& m) const
     {
-      return double(m.nnz) * (sizeof(V) + 4.0) + double(m.rows + 1) * 4.0;
+      constexpr uint32_t M = StripRows<W>::value;
+      return g(m.nd ? (m.rows + M - 1) / M : m.rows);
     }
+    // matrix bytes read by one pass, as stored
+    static double mbytes(const fb_msolver::Mat& m, double vsize)
+    {
+      if(m.nd)
+        return double(m.nd) * m.dn * vsize;
+      return double(m.nnz) * (vsize + 4.0) + double(m.rows + 1) * 4.0;
+    }
+    double mb(const fb_msolver::Mat& m) const { return mbytes(m, sizeof(V)); }
     double vb(uint32_t n, double count) const { return double(n) * K * sizeof(S) * count; }
 
     void vcycle(bool top_pcg)
@@ -804,7 +995,7 @@ namespace mr
         for(int k = 1; k < s->cfg.smooth_steps; ++k)
         {
           if(!dry)
-            km_smooth<V, S, R><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
+            km_smooth<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
               (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
           ++launches;
           bytes += mb(f.A) + vb(f.n, 4);
@@ -812,7 +1003,7 @@ namespace mr
         }
         xcur[size_t(l)] = xa;
         if(!dry)
-          km_defect<V, S, R><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
+          km_defect<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
         ++launches;
         bytes += mb(f.A) + vb(f.n, 3);
         const bool coarsest = (l + 2 == nl);
@@ -837,7 +1028,7 @@ namespace mr
         if(!dry)
           km_prolong<V, S, R><<<g(f.n), MNT, 0, st>>>(mv<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
         if(!dry)
-          km_post1<V, S, R><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
+          km_post1<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
             (const S*)f.dinv, f.dm, f.skip_post, s->sc);
         launches += 2;
         bytes += mb(f.P) + vb(f.n, 2) + vb(s->lv[size_t(l + 1)].n, 1) + mb(f.A) + vb(f.n, 4);
@@ -850,13 +1041,13 @@ namespace mr
           if(dry)
             ;
           else if(!last)
-            km_post2<V, S, R, false, false><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
+            km_post2<V, S, R, false, false><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
               (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
           else if(top)
-            km_post2<V, S, R, true, true><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
+            km_post2<V, S, R, true, true><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
               (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
           else
-            km_post2<V, S, R, true, false><<<g(f.n), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
+            km_post2<V, S, R, true, false><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
               (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
           ++launches;
           bytes += mb(f.A) + vb(f.n, 4) + (top && last ? double(f.n) * K * 16.0 : 0.0);
@@ -874,12 +1065,12 @@ namespace mr
       if(!dry)
         km_open<<<1, 32, 0, st>>>(s->sc, K);
       if(!dry)
-        km_pcg_init<S, R><<<g(t.n), MNT, 0, st>>>(mv<double>(A64()), s->rhs, s->x, s->r, t.dm,
+        km_pcg_init<S, R><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->rhs, s->x, s->r, t.dm,
           f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->sc);
       if(!dry)
         km_count_progress<<<1, 64, 0, st>>>(s->sc, K, 0);
       launches += 3;
-      bytes += double(A64().nnz) * 12.0 + double(t.n) * K * 8.0 * 3;
+      bytes += mbytes(A64(), 8.0) + double(t.n) * K * 8.0 * 3;
       if(!f64)
       {
         if(!dry)
@@ -896,7 +1087,7 @@ namespace mr
       if(!dry)
       {
         km_pcg_p<R><<<g(t.n), MNT, 0, st>>>(s->p, s->z, t.n, first ? 1 : 0, s->sc);
-        km_pcg_q<R><<<g(t.n), MNT, 0, st>>>(mv<double>(A64()), s->p, s->q, t.dm, s->sc);
+        km_pcg_q<R><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->p, s->q, t.dm, s->sc);
         if(f64)
           km_pcg_x<S, R, false><<<g(t.n), MNT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
             (const S*)t.dinv, t.skip_pre, s->hist, t.n, K, s->sc);
@@ -906,7 +1097,7 @@ namespace mr
         km_count_progress<<<1, 64, 0, st>>>(s->sc, K, cond);
       }
       launches += 4;
-      bytes += double(t.n) * K * 8.0 * 3 + double(A64().nnz) * 12.0 + double(t.n) * K * 8.0 * 3 +
+      bytes += double(t.n) * K * 8.0 * 3 + mbytes(A64(), 8.0) + double(t.n) * K * 8.0 * 3 +
                double(t.n) * K * (8.0 * 6 + 2 * sizeof(S));
     }
   };
@@ -1092,9 +1283,9 @@ fb_status fb_msolver_create(fb_msolver** out, fb_hierarchy* h, const fb_solver_c
     const std::vector<uint32_t> inv_f = pf.empty() ? std::vector<uint32_t>() : inverse_perm(pf);
     D.n = H.A.rows;
     HostCsr A = permute(H.A, pf, inv_f);
-    MR_TRY(mr::upload(s.get(), D.A, A, prec, &dms[size_t(l)]));
+    MR_TRY(mr::upload(s.get(), D.A, A, prec, &dms[size_t(l)], cfg.diagonal != 0));
     if(l == 0 && prec != FB_PREC_F64)
-      MR_TRY(mr::upload(s.get(), D.A64, A, FB_PREC_F64, &dms[size_t(l)]));
+      MR_TRY(mr::upload(s.get(), D.A64, A, FB_PREC_F64, &dms[size_t(l)], cfg.diagonal != 0));
     if(l + 1 < s->nlev)
     {
       const std::vector<uint32_t>& pc = perms[size_t(l + 1)];
