@@ -537,9 +537,10 @@ STREAM_PASSES = ("mg_sdown", "mg_sup")
 
 
 def pass_table(solver, levels, precision, reps=20):
-    """Each finest-level pass of a solve timed alone (cold L2) with its CSR-algorithmic bytes (the
-    survey's definition: nnz * (value + 4 B index) + (rows + 1) * 4 B + the vectors it reads and
-    writes) and the bytes it moves as stored on the device (solver's count)."""
+    """Each finest-level pass of a solve timed alone (cold L2) with its CSR-algorithmic bytes
+    (nnz * (value + 4 B index) + (rows + 1) * 4 B + the vectors it reads and writes: the bytes a CSR
+    pass over the reference's containers must move) and the bytes it moves as stored on the device
+    (solver's count)."""
     sv = {"f64": 8, "f32": 4, "f32_bf16": 2}[precision]
     sx = 8 if precision == "f64" else 4
     A = levels[0]["matrix"]

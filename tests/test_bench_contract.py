@@ -25,7 +25,7 @@ def test_reference_arm_json_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "ms" and d["higher_is_better"] is False
     assert d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1 and d["value"] > 0
-    assert d["config"]["iterations"] == 5   # the reference's own count at L7 (survey probe: 5)
+    assert d["config"]["iterations"] == 5   # the reference's own iteration count at L7
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"]
     e = d["e2e"]
