@@ -39,19 +39,44 @@ def _assemble_cells(level, cells_sel):
     return A, b
 
 
-def _patch(level, rank):
-    """Cells with x-index in the rank's half; the rank's vertices in global order; the mirror of the
-    shared column; the Dirichlet DOFs; patch matrix and load vector in local numbering."""
-    N = 2 ** level
+def _strip_bounds(level, world, base):
+    """x-index bounds of the ranks' vertical strips at `level`: floor(r 2^base / world) cell columns
+    on level `base`, refined by 2 per level, so that every patch is the refinement of its patch on
+    the coarser levels down to `base`."""
+    nb = 2 ** base
+    f = 2 ** (level - base)
+    return [(r * nb // world) * f for r in range(world + 1)]
+
+
+def _strip_vertices(level, rank, world=2, base=None):
+    b = _strip_bounds(level, world, level if base is None else base)
+    vx = np.arange((2 ** level + 1) ** 2) % (2 ** level + 1)
+    return np.nonzero((vx >= b[rank]) & (vx <= b[rank + 1]))[0]
+
+
+def _strip_cells(level, rank, world=2, base=None):
+    b = _strip_bounds(level, world, level if base is None else base)
     _, idx = AS._cells(level, 2)
-    sel = (idx[0] < N // 2) if rank == 0 else (idx[0] >= N // 2)
-    A, b = _assemble_cells(level, sel)
+    return (idx[0] >= b[rank]) & (idx[0] < b[rank + 1])
+
+
+def _patch(level, rank, world=2, base=None):
+    """The rank's vertical strip of cells: its vertices in global order, the patch matrix and load
+    vector in local numbering (type 0), the mirrors [(neighbour rank, local indices of the shared
+    column in ascending global order)] and the Dirichlet DOFs."""
+    N = 2 ** level
+    b = _strip_bounds(level, world, level if base is None else base)
+    A, bv = _assemble_cells(level, _strip_cells(level, rank, world, base))
     vx = np.arange((N + 1) ** 2) % (N + 1)
-    mine = np.nonzero(vx <= N // 2)[0] if rank == 0 else np.nonzero(vx >= N // 2)[0]
+    mine = _strip_vertices(level, rank, world, base)
     Al = A[mine][:, mine].tocsr()
-    shared = np.nonzero(vx[mine] == N // 2)[0]
+    nbrs = []
+    if rank > 0:
+        nbrs.append((rank - 1, np.nonzero(vx[mine] == b[rank])[0]))
+    if rank < world - 1:
+        nbrs.append((rank + 1, np.nonzero(vx[mine] == b[rank + 1])[0]))
     bnd = np.isin(mine, AS.boundary_dofs(level).astype(np.int64))
-    return mine, Al, b[mine], shared, np.nonzero(bnd)[0]
+    return mine, Al, bv[mine], nbrs, np.nonzero(bnd)[0]
 
 
 def _global_problem(level):
@@ -101,9 +126,10 @@ def _worker(rank, world, port, q):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        mine, Al, bl, shared, bnd = _patch(LEVEL, rank)
+        mine, Al, bl, nbrs, bnd = _patch(LEVEL, rank)
         gate = Gate(dist)
-        gate.push(1 - rank, shared)
+        for nb, shared in nbrs:
+            gate.push(nb, shared)
         gate.compile(len(mine))
         Ag, bg, bndg = _global_problem(LEVEL)
         # sync_0 turns the patch load vectors into the global one; dot is the global dot product
@@ -180,12 +206,6 @@ def test_global_pcg_on_device_one_rank(featlib, cuda):
 
 # --- the global multigrid: Global::Transfer, Global::Muxer and the V-cycle on global levels ---
 
-def _patch_vertices(level, rank):
-    N = 2 ** level
-    vx = np.arange((N + 1) ** 2) % (N + 1)
-    return np.nonzero(vx <= N // 2)[0] if rank == 0 else np.nonzero(vx >= N // 2)[0]
-
-
 def _prolongation_cells(level_f, csel):
     """Assembly::GridTransfer::assemble_prolongation over the selected coarse cells of level_f - 1:
     every coarse cell adds the bilinear interpolation weights of the 3x3 fine vertices it covers, and
@@ -214,9 +234,11 @@ def _prolongation_cells(level_f, csel):
     return P, w
 
 
-def _mg_levels(rank, merge, dist):
-    """Rank's global levels, finest first: levels LEVEL..merge+1 split into the two patches, levels
-    merge..1 merged on rank 0 (the muxer's parent) and absent on rank 1 (a ghost below merge + 1)."""
+def _mg_levels(rank, merge, dist, world):
+    """Rank's global levels, finest first: levels LEVEL..merge+1 split into `world` vertical strips
+    (bounds fixed on level `merge`, so every patch refines a set of the merged level's cells), levels
+    merge..1 merged on rank 0 (the muxer's parent) and absent on the other ranks (ghosts below
+    merge + 1)."""
     import torch
     from featb200.global_layer import (Gate, GlobalMatrix, GlobalTransfer, GlobalUnitFilter, Muxer,
                                        coarse_inverse, prolongation_row_scaling)
@@ -226,9 +248,10 @@ def _mg_levels(rank, merge, dist):
 
     levels = []
     for lv in range(LEVEL, merge, -1):
-        mine, Al, _, shared, bnd = _patch(lv, rank)
+        mine, Al, _, nbrs, bnd = _patch(lv, rank, world, merge)
         gate = Gate(dist)
-        gate.push(1 - rank, shared)
+        for nb, shared in nbrs:
+            gate.push(nb, shared)
         gate.compile(len(mine))
         levels.append({"matrix": GlobalMatrix(csr_op(Al), gate, torch.tensor(Al.diagonal())),
                        "filter": GlobalUnitFilter(bnd), "mine": mine})
@@ -246,10 +269,8 @@ def _mg_levels(rank, merge, dist):
         if lv > merge:
             mine_f = fine["mine"]
             Nc = 2 ** (lv - 1)
-            _, cidx = AS._cells(lv - 1, 2)
-            csel = (cidx[0] < Nc // 2) if rank == 0 else (cidx[0] >= Nc // 2)
-            Psum, w = _prolongation_cells(lv, csel)
-            mine_c = _patch_vertices(lv - 1, rank)
+            Psum, w = _prolongation_cells(lv, _strip_cells(lv - 1, rank, world, merge))
+            mine_c = _strip_vertices(lv - 1, rank, world, merge)
             Ploc = Psum[mine_f][:, mine_c]
             s = prolongation_row_scaling(torch.tensor(w[mine_f]), fine["matrix"].gate).numpy()
             Ploc = sp.diags(s) @ Ploc
@@ -260,8 +281,8 @@ def _mg_levels(rank, merge, dist):
                 mux = Muxer(dist, parent=0)
                 mux.push_parent(np.arange(mine_c.size))
                 if parent:
-                    for r in range(2):
-                        mux.push_child(_patch_vertices(lv - 1, r))
+                    for r in range(world):
+                        mux.push_child(_strip_vertices(lv - 1, r, world, merge))
                 mux.compile()
                 T = GlobalTransfer(csr_op(Ploc), csr_op(Rloc), fine["matrix"].gate,
                                    levels[k + 1]["matrix"].gate if parent else None, mux,
@@ -289,7 +310,7 @@ def _mg_worker(rank, world, port, q, merges):
     try:
         out = {}
         for merge in merges:
-            levels, coarse = _mg_levels(rank, merge, dist)
+            levels, coarse = _mg_levels(rank, merge, dist, world)
             mg = GlobalMultiGrid(levels, coarse, omega=0.7, steps=2)
             top = levels[0]
             mine = top["mine"]
@@ -299,7 +320,7 @@ def _mg_worker(rank, world, port, q, merges):
             dg[bndg] = 0.0
             z = mg.vcycle(torch.tensor(dg[mine]))
             # PCG preconditioned by the global multigrid, from the patch load vectors
-            _, _, bl, _, _ = _patch(LEVEL, rank)
+            _, _, bl, _, _ = _patch(LEVEL, rank, world, merge)
             b = top["matrix"].gate.sync_0(torch.tensor(bl))
             top["filter"].filter_def(b)
             x = torch.zeros(len(mine), dtype=torch.float64)
@@ -318,11 +339,10 @@ def test_prolongation_assembly_weights_give_the_interpolation():
     from featb200.global_layer import Gate, prolongation_row_scaling
     for lv in (2, 5):
         Nc = 2 ** (lv - 1)
-        _, cidx = AS._cells(lv - 1, 2)
         Psum, w = _prolongation_cells(lv, np.ones(Nc * Nc, dtype=bool))
         P = AS.prolongation(lv)
         assert abs(sp.diags(1.0 / w) @ Psum - P).max() == 0.0
-        parts = [_prolongation_cells(lv, (cidx[0] < Nc // 2) if r == 0 else (cidx[0] >= Nc // 2)) for r in range(2)]
+        parts = [_prolongation_cells(lv, _strip_cells(lv - 1, r)) for r in range(2)]
         wsum = parts[0][1] + parts[1][1]        # what sync_0 forms on the shared DOFs
         Pg = sp.diags(1.0 / wsum) @ (parts[0][0] + parts[1][0])
         assert abs(Pg - P).max() == 0.0
@@ -331,25 +351,8 @@ def test_prolongation_assembly_weights_give_the_interpolation():
     assert torch.equal(s, torch.tensor([0.5, 0.25, 1.0], dtype=torch.float64))
 
 
-def test_global_multigrid_two_patches_gloo(oracle_lib):
-    """Two gloo ranks, each holding one half of the 2D Q1 hierarchy (levels 5..merge+1) with the
-    levels merge..1 muxed onto rank 0 (merge 4: only the finest level is split): one global V-cycle and the multigrid-preconditioned global PCG
-    against the oracle's single-system V-cycle and PCG on the whole hierarchy (same operation
-    order; only the split sums of the shared rows differ in rounding)."""
-    from helpers import rel_err
-    merges = (1, 3, 4)
-    world = 2
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_mg_worker, args=(r, world, port, q, merges)) for r in range(world)]
-    for p in procs:
-        p.start()
-    res = dict(q.get(timeout=180) for _ in range(world))
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
-    O = oracle_lib
+def _oracle_mg_reference(O):
+    """The oracle's single-system V-cycle of the fixed defect and PCG-multigrid solution."""
     lv_ref = []
     for lv in range(LEVEL, 0, -1):
         A, _, bnd = _global_problem(lv)
@@ -369,13 +372,39 @@ def test_global_multigrid_two_patches_gloo(oracle_lib):
     b[bndg] = 0.0
     x_ref, info = mg.solve(b, tol_rel=1e-8, max_iter=100)
     assert info["status"] == "success"
+    return z_ref, x_ref, info["iters"]
+
+
+@pytest.mark.parametrize("world,merges", [(2, (1, 3, 4)), (3, (2, 3)), (4, (2,))])
+def test_global_multigrid_strips_gloo(oracle_lib, world, merges):
+    """`world` gloo ranks, each holding one vertical strip of the 2D Q1 hierarchy on levels
+    5..merge+1 (uneven strips for three ranks; the middle ranks have two neighbours), the levels
+    merge..1 muxed onto rank 0 (merge 4: only the finest level is split): one global V-cycle and the
+    multigrid-preconditioned global PCG against the oracle's single-system V-cycle and PCG on the
+    whole hierarchy (same operation order; only the split sums of the shared rows differ in
+    rounding)."""
+    from helpers import rel_err
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mg_worker, args=(r, world, port, q, merges)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=240) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    z_ref, x_ref, iters = _oracle_mg_reference(oracle_lib)
     for merge in merges:
+        covered = np.zeros(z_ref.size, dtype=bool)
         for rank in range(world):
             mine, z, x, it, ok, ghost = res[rank][merge]
-            assert ghost == (rank == 1)
+            covered[mine] = True
+            assert ghost == (rank != 0)
             assert rel_err(z, z_ref[mine]) <= 1e-13, (merge, rank, rel_err(z, z_ref[mine]))
-            assert ok and it == info["iters"], (merge, rank, it, info["iters"])
+            assert ok and it == iters, (merge, rank, it, iters)
             assert rel_err(x, x_ref[mine]) <= 1e-12, (merge, rank, rel_err(x, x_ref[mine]))
+        assert covered.all()
 
 
 @pytest.mark.gpu
