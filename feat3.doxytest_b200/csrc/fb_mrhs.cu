@@ -8,8 +8,10 @@
 // (K/32 per lane): the row's entries are read once, coalesced, and broadcast by shuffles, and every
 // gather of x[col][0..K) is one coalesced K*sizeof(S) access -- the matrix traffic is shared by all
 // right-hand sides (the reference's multi-vector CSR kernel, apply.cu:109-135, covers K <= 3).
-// Rows are summed in stored entry order without FMA, per right-hand side, as in the single-RHS
-// kernels.  Dot products and norms are reduced per block and then with FP64 atomics (their
+// System matrices of lexicographically numbered Q1 grids run in a stencil form instead: values by
+// diagonal, one warp per strip of consecutive rows, each x row gathered once for all the strip's
+// rows it enters (strip_rows).  Rows are summed in stored entry order without FMA, per right-hand
+// side, as in the single-RHS kernels, in both forms.  Dot products and norms are reduced per block and then with FP64 atomics (their
 // summation order is not fixed; results agree with the single-RHS path to rounding).
 #include "fb_common.cuh"
 #include "fb_setup.h"
