@@ -185,6 +185,29 @@ def test_gate_single_rank_is_local():
     assert torch.equal(g.sync_0(y), x) and torch.equal(g.sync_1(y), x)
 
 
+
+def test_muxer_and_transfer_single_rank():
+    """Without siblings the muxer is no child: join and split copy, the transfer is the patch-local
+    one, and a muxer without a parent mirror refuses to compile."""
+    import torch
+    from featb200.global_layer import Gate, GlobalTransfer, Muxer
+    with pytest.raises(ValueError):
+        Muxer(None).compile()
+    m = Muxer(None)
+    m.push_parent([0, 1, 2])
+    m.push_child([0, 1, 2])
+    m.compile()
+    assert not m.is_child() and m.is_parent() and not m.is_ghost() and m.bufsize == 3
+    v = torch.tensor([1.0, 2.0, 3.0], dtype=torch.float64)
+    assert torch.equal(m.join(v, 3), v) and torch.equal(m.split(v, 3), v)
+    P = torch.tensor([[1.0, 0.0], [0.5, 0.5], [0.0, 1.0]], dtype=torch.float64)
+    T = GlobalTransfer(lambda c: P @ c, lambda f: P.T @ f, Gate(None).compile(3), Gate(None).compile(2), m,
+                       coarse_local_size=2, coarse_size=2)
+    assert not T.is_ghost()
+    assert torch.equal(T.rest(v), P.T @ v)
+    c = torch.tensor([4.0, 6.0], dtype=torch.float64)
+    assert torch.equal(T.prol(c), P @ c)
+
 @pytest.mark.gpu
 def test_global_pcg_on_device_one_rank(featlib, cuda):
     """The device form of the global layer with one rank: the patch product through the library's
