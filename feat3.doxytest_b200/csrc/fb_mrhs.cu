@@ -8,9 +8,9 @@
 // (K/32 per lane): the row's entries are read once, coalesced, and broadcast by shuffles, and every
 // gather of x[col][0..K) is one coalesced K*sizeof(S) access -- the matrix traffic is shared by all
 // right-hand sides (the reference's multi-vector CSR kernel, apply.cu:109-135, covers K <= 3).
-// System matrices of lexicographically numbered Q1 grids run in a stencil form instead: values by
-// diagonal, one warp per strip of consecutive rows, each x row gathered once for all the strip's
-// rows it enters (strip_rows).  Rows are summed in stored entry order without FMA, per right-hand
+// With the configuration's `diagonal` set, system matrices of lexicographically numbered Q1 grids
+// run in a stencil form instead: values by diagonal, one warp per strip of consecutive rows, each x
+// row gathered once for all the strip's rows it enters (strip_rows).  Rows are summed in stored entry order without FMA, per right-hand
 // side, as in the single-RHS kernels, in both forms.  Dot products and norms are reduced per block and then with FP64 atomics (their
 // summation order is not fixed; results agree with the single-RHS path to rounding).
 #include "fb_common.cuh"
@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 namespace fb
@@ -237,15 +238,15 @@ namespace mr
     }
   }
 
-  // epi(row, sum) for every row of A with sum = (A x)[row], in the stencil form where A has one
-  template<typename V, typename S, int R, class Epi>
+  // epi(row, sum) for every row of A with sum = (A x)[row]: in the stencil form with G = 9 or 3
+  // triplets per row, in the CSR form for G = 0.  The form is a template parameter of every matrix
+  // pass, so the CSR instances keep the registers (and the resident warps) of the row kernel.
+  template<typename V, typename S, int R, int G, class Epi>
   __device__ __forceinline__ void for_rows(const MCsr<V>& A, const S* __restrict__ x, Epi epi)
   {
     typedef typename ValueTraits<V>::acc Ac;
-    if(A.nd == 27)
-      strip_rows<V, S, R, 9>(A, x, epi);
-    else if(A.nd == 9)
-      strip_rows<V, S, R, 3>(A, x, epi);
+    if constexpr(G > 0)
+      strip_rows<V, S, R, G>(A, x, epi);
     else
       for(uint32_t row = blockIdx.x * MW + (threadIdx.x >> 5); row < A.rows; row += gridDim.x * MW)
       {
@@ -297,7 +298,7 @@ namespace mr
 #define MR_ROWS(n) \
   for(uint32_t row = blockIdx.x * MW + (threadIdx.x >> 5); row < (n); row += gridDim.x * MW)
 
-  template<typename V, typename S, int R>
+  template<typename V, typename S, int R, int G>
   __global__ void __launch_bounds__(MNT) km_smooth(MCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ xo, const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip,
     const MScal* __restrict__ sc)
@@ -307,7 +308,7 @@ namespace mr
     if(closed(sc))
       return;
     const int lane = threadIdx.x & 31;
-    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
+    for_rows<V, S, R, G>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
@@ -327,7 +328,7 @@ namespace mr
     });
   }
 
-  template<typename V, typename S, int R>
+  template<typename V, typename S, int R, int G>
   __global__ void __launch_bounds__(MNT) km_defect(MCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ dv, const uint8_t* __restrict__ dm, const MScal* __restrict__ sc)
   {
@@ -336,7 +337,7 @@ namespace mr
     if(closed(sc))
       return;
     const int lane = threadIdx.x & 31;
-    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
+    for_rows<V, S, R, G>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
@@ -430,7 +431,7 @@ namespace mr
     }
   }
 
-  template<typename V, typename S, int R>
+  template<typename V, typename S, int R, int G>
   __global__ void __launch_bounds__(MNT) km_post1(MCsr<V> A, const S* __restrict__ b, const S* __restrict__ x,
     S* __restrict__ dv, S* __restrict__ cv, const S* __restrict__ dinv, const uint8_t* __restrict__ dm,
     int* __restrict__ skip, MScal* __restrict__ sc)
@@ -444,7 +445,7 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    for_rows<V, S, R>(A, x, [&](uint32_t row, const Ac (&sum)[R])
+    for_rows<V, S, R, G>(A, x, [&](uint32_t row, const Ac (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
@@ -462,7 +463,7 @@ namespace mr
     reduce_per_rhs<R>(part, sc, [&](int j, double tot) { skip[j] = skip_of<S>(sqrt(tot)); });
   }
 
-  template<typename V, typename S, int R, bool LAST, bool TOP>
+  template<typename V, typename S, int R, bool LAST, bool TOP, int G>
   __global__ void __launch_bounds__(MNT) km_post2(MCsr<V> A, const S* __restrict__ dv, const S* __restrict__ cv,
     S* __restrict__ co, S* __restrict__ x, double* __restrict__ z, const double* __restrict__ rr,
     const S* __restrict__ dinv, const uint8_t* __restrict__ dm, const int* __restrict__ skip, MScal* __restrict__ sc)
@@ -476,7 +477,7 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    for_rows<V, S, R>(A, cv, [&](uint32_t row, const Ac (&sum)[R])
+    for_rows<V, S, R, G>(A, cv, [&](uint32_t row, const Ac (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       const Ac di = Ac(__ldg(dinv + row));
@@ -528,7 +529,7 @@ namespace mr
   }
 
   // r = F(rhs - A x), norms -> def_init, status; FP64 mode: sol1 = F(D .* r)
-  template<typename S, int R>
+  template<typename S, int R, int G>
   __global__ void __launch_bounds__(MNT) km_pcg_init(MCsr<double> A, const double* __restrict__ rhs,
     const double* __restrict__ x, double* __restrict__ rr, const uint8_t* __restrict__ dm, S* __restrict__ x1,
     const S* __restrict__ dinv, int* __restrict__ skip_top, MScal* __restrict__ sc)
@@ -539,7 +540,7 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    for_rows<double, double, R>(A, x, [&](uint32_t row, const double (&sum)[R])
+    for_rows<double, double, R, G>(A, x, [&](uint32_t row, const double (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
@@ -634,7 +635,7 @@ namespace mr
   }
 
   // q = F(A p), q.p -> alpha
-  template<int R>
+  template<int R, int G>
   __global__ void __launch_bounds__(MNT) km_pcg_q(MCsr<double> A, const double* __restrict__ p, double* __restrict__ q,
     const uint8_t* __restrict__ dm, MScal* __restrict__ sc)
   {
@@ -646,7 +647,7 @@ namespace mr
     #pragma unroll
     for(int r = 0; r < R; ++r)
       part[r] = 0.0;
-    for_rows<double, double, R>(A, p, [&](uint32_t row, const double (&sum)[R])
+    for_rows<double, double, R, G>(A, p, [&](uint32_t row, const double (&sum)[R])
     {
       const bool d = __ldg(dm + row) != 0;
       #pragma unroll
@@ -982,6 +983,16 @@ namespace mr
       return double(m.nnz) * (vsize + 4.0) + double(m.rows + 1) * 4.0;
     }
     double mb(const fb_msolver::Mat& m) const { return mbytes(m, sizeof(V)); }
+    // f(std::integral_constant<int, G>) with G the stored form of m: 9 or 3 stencil triplets, 0 = CSR
+    template<class F> static void by_form(const fb_msolver::Mat& m, F&& f)
+    {
+      if(m.nd == 27)
+        f(std::integral_constant<int, 9>());
+      else if(m.nd == 9)
+        f(std::integral_constant<int, 3>());
+      else
+        f(std::integral_constant<int, 0>());
+    }
     double vb(uint32_t n, double count) const { return double(n) * K * sizeof(S) * count; }
 
     void vcycle(bool top_pcg)
@@ -997,15 +1008,20 @@ namespace mr
         for(int k = 1; k < s->cfg.smooth_steps; ++k)
         {
           if(!dry)
-            km_smooth<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)xb,
-              (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
+            by_form(f.A, [&](auto gc) {
+              km_smooth<V, S, R, decltype(gc)::value><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b,
+                (const S*)xa, (S*)xb, (const S*)f.dinv, f.dm, f.skip_pre, s->sc);
+            });
           ++launches;
           bytes += mb(f.A) + vb(f.n, 4);
           std::swap(xa, xb);
         }
         xcur[size_t(l)] = xa;
         if(!dry)
-          km_defect<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xa, (S*)f.d, f.dm, s->sc);
+          by_form(f.A, [&](auto gc) {
+            km_defect<V, S, R, decltype(gc)::value><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b,
+              (const S*)xa, (S*)f.d, f.dm, s->sc);
+          });
         ++launches;
         bytes += mb(f.A) + vb(f.n, 3);
         const bool coarsest = (l + 2 == nl);
@@ -1030,8 +1046,10 @@ namespace mr
         if(!dry)
           km_prolong<V, S, R><<<g(f.n), MNT, 0, st>>>(mv<V>(f.P), (const S*)xcur[size_t(l + 1)], (S*)xf, f.dm, s->sc);
         if(!dry)
-          km_post1<V, S, R><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b, (const S*)xf, (S*)f.d, (S*)f.c,
-            (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+          by_form(f.A, [&](auto gc) {
+            km_post1<V, S, R, decltype(gc)::value><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.b,
+              (const S*)xf, (S*)f.d, (S*)f.c, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+          });
         launches += 2;
         bytes += mb(f.P) + vb(f.n, 2) + vb(s->lv[size_t(l + 1)].n, 1) + mb(f.A) + vb(f.n, 4);
         void* ca = f.c;
@@ -1040,17 +1058,19 @@ namespace mr
         for(int k = 2; k <= s->cfg.smooth_steps; ++k)
         {
           const bool last = (k == s->cfg.smooth_steps);
-          if(dry)
-            ;
-          else if(!last)
-            km_post2<V, S, R, false, false><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
-              (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
-          else if(top)
-            km_post2<V, S, R, true, true><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
-              (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
-          else
-            km_post2<V, S, R, true, false><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d, (const S*)ca, (S*)cb,
-              (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+          if(!dry)
+            by_form(f.A, [&](auto gc) {
+              constexpr int G = decltype(gc)::value;
+              if(!last)
+                km_post2<V, S, R, false, false, G><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d,
+                  (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+              else if(top)
+                km_post2<V, S, R, true, true, G><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d,
+                  (const S*)ca, (S*)cb, (S*)xf, s->z, s->r, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+              else
+                km_post2<V, S, R, true, false, G><<<ga<V>(f.A), MNT, 0, st>>>(mv<V>(f.A), (const S*)f.d,
+                  (const S*)ca, (S*)cb, (S*)xf, nullptr, nullptr, (const S*)f.dinv, f.dm, f.skip_post, s->sc);
+            });
           ++launches;
           bytes += mb(f.A) + vb(f.n, 4) + (top && last ? double(f.n) * K * 16.0 : 0.0);
           std::swap(ca, cb);
@@ -1067,8 +1087,10 @@ namespace mr
       if(!dry)
         km_open<<<1, 32, 0, st>>>(s->sc, K);
       if(!dry)
-        km_pcg_init<S, R><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->rhs, s->x, s->r, t.dm,
-          f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->sc);
+        by_form(A64(), [&](auto gc) {
+          km_pcg_init<S, R, decltype(gc)::value><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->rhs,
+            s->x, s->r, t.dm, f64 ? (S*)t.x : (S*)nullptr, (const S*)t.dinv, t.skip_pre, s->sc);
+        });
       if(!dry)
         km_count_progress<<<1, 64, 0, st>>>(s->sc, K, 0);
       launches += 3;
@@ -1089,7 +1111,10 @@ namespace mr
       if(!dry)
       {
         km_pcg_p<R><<<g(t.n), MNT, 0, st>>>(s->p, s->z, t.n, first ? 1 : 0, s->sc);
-        km_pcg_q<R><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->p, s->q, t.dm, s->sc);
+        by_form(A64(), [&](auto gc) {
+          km_pcg_q<R, decltype(gc)::value><<<ga<double>(A64()), MNT, 0, st>>>(mv<double>(A64()), s->p, s->q, t.dm,
+            s->sc);
+        });
         if(f64)
           km_pcg_x<S, R, false><<<g(t.n), MNT, 0, st>>>(s->x, s->r, s->p, s->q, t.dm, (S*)nullptr, (S*)t.x,
             (const S*)t.dinv, t.skip_pre, s->hist, t.n, K, s->sc);

@@ -239,9 +239,9 @@ typedef struct
                            every row (structured grids numbered lexicographically), is stored as
                            its diagonals without column indices (row sums keep the stored order;
                            missing diagonals hold zeros); 0 = always sliced ELL.  The multi-RHS
-                           solver (fb_msolver_*) uses the stencil form for system matrices whose
-                           stored rows all have the same 9 or 27 column offsets in triplets
-                           (o-1, o, o+1); 0 = always CSR */
+                           solver (fb_msolver_*) uses, for diagonal != 0, a stencil form for system
+                           matrices whose stored rows all have the same 9 or 27 column offsets in
+                           triplets (o-1, o, o+1); 0 = always CSR (measured as fast there) */
   int pdl;              /* 1 (default): the solve's kernels are launched with programmatic stream
                            serialisation, so each one's launch and its matrix prologue overlap the
                            end of its predecessor; 0 = plain stream order */

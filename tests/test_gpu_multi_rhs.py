@@ -87,7 +87,7 @@ def test_multi_rhs_stencil_form(featlib, cuda, dim, level, precision):
     h = fb.build_hierarchy(levels)
     out = {}
     for diag in (False, True):
-        ms = fb.MultiRhsPCG(h, 64, precision=precision, ordering="native", diagonal=diag)
+        ms = fb.MultiRhsPCG(h, 64, precision=precision, ordering="native", stencil=diag)
         X = ms.solve(np.zeros_like(B), B)
         assert all(s == fb.Status.success for s in ms.statuses())
         out[diag] = (X, ms.iterations())
