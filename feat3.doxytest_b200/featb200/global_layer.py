@@ -350,26 +350,34 @@ def coarse_inverse(A: torch.Tensor, filter_idx):
 
 
 class GlobalMultiGrid:
-    """Solver::MultiGrid's V-cycle (kernel/solver/multigrid.hpp:1335-1350 with _apply_rest :1713-1838
-    and _apply_prol :1845-2000, fixed coarse-grid correction) on global levels, with `steps`
-    Richardson steps preconditioned by Jacobi omega / diag(A) (the global diagonal) as pre- and
-    post-smoother (kernel/solver/richardson.hpp:160-228) and an exact coarse solve.
+    """Solver::MultiGrid (kernel/solver/multigrid.hpp:1270-2000) on global levels: the V, F or W
+    cycle (_apply_cycle_v / _f / _w, :1335-1510) with the fixed or an adaptive coarse-grid
+    correction (MultiGridAdaptCGC MinEnergy / MinDefect, :1880-1960), `steps` Richardson steps
+    preconditioned by Jacobi omega / diag(A) (the global diagonal) as pre-, post- and peak smoother
+    (kernel/solver/richardson.hpp:160-228) and an exact coarse solve.
 
     levels: finest first, dicts with "matrix" (GlobalMatrix), "filter" (GlobalUnitFilter) and, on
     every level but the coarsest, "transfer" (GlobalTransfer).  On a ghost rank the list ends with
     the level whose transfer is a ghost; there `coarse_solve` is unused.  The coarse solve runs on
-    the coarsest level: the parent's merged one, or every rank's without a muxer."""
+    the coarsest level: the parent's merged one, or every rank's without a muxer.  Every rank runs
+    the cycle over its own levels, its last level being the coarse level or, on a ghost rank, one
+    past its ghost level (multigrid.hpp:1386, 1445); the F and W cycles then cross the muxed transfer
+    in the same order on every rank, as rest_send / prol_recv on the ghosts."""
 
     EPS = 2.220446049250313e-16
 
-    def __init__(self, levels, coarse_solve=None, omega=0.7, steps=2):
+    def __init__(self, levels, coarse_solve=None, omega=0.7, steps=2, cycle="V", cgc="fixed"):
         self.levels, self.coarse_solve, self.steps = levels, coarse_solve, int(steps)
+        if cycle not in ("V", "F", "W") or cgc not in ("fixed", "energy", "defect"):
+            raise ValueError("GlobalMultiGrid: cycle is V, F or W and cgc fixed, energy or defect")
+        self.cycle, self.cgc = cycle, cgc
         last = levels[-1]
         self.ghost = "transfer" in last and last["transfer"].is_ghost()
         if not self.ghost and "transfer" in last:
             raise ValueError("GlobalMultiGrid: the coarsest level has a transfer that is not a ghost")
         if not self.ghost and coarse_solve is None:
             raise ValueError("GlobalMultiGrid: the coarsest level needs a coarse solve")
+        self.last = len(levels) if self.ghost else len(levels) - 1
         self.dinv = []
         for lv in levels:
             if "transfer" in lv:
@@ -396,36 +404,100 @@ class GlobalMultiGrid:
                 break                                # Status::diverged
         return out
 
-    def vcycle(self, d: torch.Tensor) -> torch.Tensor:
-        """The correction for the type-1 defect d on the finest level."""
+    def _rest(self, cur: int, smooth: bool):
+        """_apply_rest (multigrid.hpp:1713-1838): pre-smoothing and defect on every level from cur
+        (not on cur itself unless smooth), restriction to the next level; a ghost sends it."""
         L = self.levels
-        n = len(L)
-        rhs, sol, dfc = [None] * n, [None] * n, [None] * n
-        rhs[0] = d.clone()
-        top = n - 2
-        for i in range(n - 1 if not self.ghost else n):
+        for i in range(cur, self.last):
             A, filt, T = L[i]["matrix"], L[i]["filter"], L[i]["transfer"]
-            sol[i] = self._smooth(i, rhs[i])
-            dfc[i] = torch.empty_like(rhs[i])
-            A.apply_axpy(dfc[i], sol[i], rhs[i], -1.0)
-            filt.filter_def(dfc[i])
+            if smooth or i > cur:
+                self.sol[i] = self._smooth(i, self.rhs[i])
+                if self.dfc[i] is None:
+                    self.dfc[i] = torch.empty_like(self.rhs[i])
+                A.apply_axpy(self.dfc[i], self.sol[i], self.rhs[i], -1.0)
+            filt.filter_def(self.dfc[i])
             if T.is_ghost():
-                T.rest_send(dfc[i])
-                top = i
-                break
-            rhs[i + 1] = T.rest(dfc[i])
-            L[i + 1]["filter"].filter_def(rhs[i + 1])
+                T.rest_send(self.dfc[i])
+                return
+            self.rhs[i + 1] = T.rest(self.dfc[i])
+            L[i + 1]["filter"].filter_def(self.rhs[i + 1])
+
+    def _coarse(self):
+        """_apply_coarse: nothing on a rank without the coarse level."""
         if not self.ghost:
-            sol[n - 1] = self.coarse_solve(rhs[n - 1])
-        for i in range(top, -1, -1):
+            c = len(self.levels) - 1
+            self.sol[c] = self.coarse_solve(self.rhs[c])
+
+    def _prol(self, cur: int, smooth: bool):
+        """_apply_prol (multigrid.hpp:1845-2000): prolongation (a ghost receives it), coarse-grid
+        correction, post-smoothing on every level down to cur (not on cur itself unless smooth)."""
+        L = self.levels
+        for i in range(self.last - 1, cur - 1, -1):
             A, filt, T = L[i]["matrix"], L[i]["filter"], L[i]["transfer"]
-            cor = T.prol_recv(d.dtype) if T.is_ghost() else T.prol(sol[i + 1])
+            cor = T.prol_recv(self.dtype) if T.is_ghost() else T.prol(self.sol[i + 1])
             filt.filter_def(cor)
-            sol[i].add_(cor)
-            A.apply_axpy(dfc[i], sol[i], rhs[i], -1.0)
-            filt.filter_def(dfc[i])
-            sol[i].add_(self._smooth(i, dfc[i]))
-        return sol[0]
+            w = 1.0
+            if self.cgc != "fixed":
+                tmp = torch.empty_like(cor)
+                A.apply(tmp, cor)
+                filt.filter_def(tmp)
+                if self.cgc == "energy":
+                    w = A.gate.dot(self.dfc[i], cor) / A.gate.dot(tmp, cor)
+                else:
+                    w = A.gate.dot(self.dfc[i], tmp) / A.gate.dot(tmp, tmp)
+            self.sol[i].add_(cor, alpha=w)
+            if smooth or i > cur:
+                if self.cgc != "fixed":
+                    self.dfc[i].add_(tmp, alpha=-w)
+                else:
+                    A.apply_axpy(self.dfc[i], self.sol[i], self.rhs[i], -1.0)
+                    filt.filter_def(self.dfc[i])
+                self.sol[i].add_(self._smooth(i, self.dfc[i]))
+
+    def _peak(self, k: int):
+        """_apply_smooth_peak + _apply_smooth_def (multigrid.hpp:1591-1700)."""
+        A, filt = self.levels[k]["matrix"], self.levels[k]["filter"]
+        A.apply_axpy(self.dfc[k], self.sol[k], self.rhs[k], -1.0)
+        filt.filter_def(self.dfc[k])
+        cor = self._smooth(k, self.dfc[k])
+        filt.filter_def(cor)
+        self.sol[k].add_(cor)
+        A.apply_axpy(self.dfc[k], self.sol[k], self.rhs[k], -1.0)
+        filt.filter_def(self.dfc[k])
+
+    def vcycle(self, d: torch.Tensor) -> torch.Tensor:
+        """One cycle: the correction for the type-1 defect d on the finest level."""
+        n = len(self.levels)
+        self.dtype = d.dtype
+        self.rhs, self.sol, self.dfc = [None] * n, [None] * n, [None] * n
+        self.rhs[0] = d.clone()
+        self._rest(0, True)
+        if self.cycle == "F":
+            for pk in range(self.last - 1, 0, -1):
+                self._coarse()
+                self._prol(pk, False)
+                self._peak(pk)
+                self._rest(pk, False)
+        elif self.cycle == "W":
+            self._coarse()
+            counters = [0] * (self.last + 1)
+            for _ in range(1, 1 << self.last):
+                pk = self.last
+                while pk > 0:
+                    pk -= 1
+                    if counters[pk] == 0:
+                        break
+                for i in range(self.last - 1, pk, -1):
+                    counters[i] = 0
+                counters[pk] += 1
+                self._prol(pk, False)
+                self._peak(pk)
+                self._rest(pk, False)
+                self._coarse()
+        if self.cycle != "W":
+            self._coarse()
+        self._prol(0, True)
+        return self.sol[0]
 
     __call__ = vcycle
 

@@ -321,7 +321,7 @@ def _mg_levels(rank, merge, dist, world):
     return levels, coarse
 
 
-def _mg_worker(rank, world, port, q, merges):
+def _mg_worker(rank, world, port, q, configs):
     import datetime
 
     import torch
@@ -332,9 +332,9 @@ def _mg_worker(rank, world, port, q, merges):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         out = {}
-        for merge in merges:
+        for merge, cycle, cgc in configs:
             levels, coarse = _mg_levels(rank, merge, dist, world)
-            mg = GlobalMultiGrid(levels, coarse, omega=0.7, steps=2)
+            mg = GlobalMultiGrid(levels, coarse, omega=0.7, steps=2, cycle=cycle, cgc=cgc)
             top = levels[0]
             mine = top["mine"]
             # one V-cycle on a fixed (filtered, type-1) defect
@@ -349,7 +349,7 @@ def _mg_worker(rank, world, port, q, merges):
             x = torch.zeros(len(mine), dtype=torch.float64)
             it, d0, dc, ok = global_pcg(top["matrix"], top["filter"], b, x, tol_rel=1e-8, max_iter=100,
                                         precond=mg)
-            out[merge] = (mine, z.numpy(), x.numpy(), it, ok, mg.ghost)
+            out[(merge, cycle, cgc)] = (mine, z.numpy(), x.numpy(), it, ok, mg.ghost)
         q.put((rank, out))
     finally:
         dist.destroy_process_group()
@@ -374,8 +374,8 @@ def test_prolongation_assembly_weights_give_the_interpolation():
     assert torch.equal(s, torch.tensor([0.5, 0.25, 1.0], dtype=torch.float64))
 
 
-def _oracle_mg_reference(O):
-    """The oracle's single-system V-cycle of the fixed defect and PCG-multigrid solution."""
+def _oracle_mg_reference(O, cycle="V", cgc="fixed"):
+    """The oracle's single-system cycle of the fixed defect and PCG-multigrid solution."""
     lv_ref = []
     for lv in range(LEVEL, 0, -1):
         A, _, bnd = _global_problem(lv)
@@ -386,7 +386,7 @@ def _oracle_mg_reference(O):
             d["P"] = O.Csr.of(P.indptr, P.indices, P.data, P.shape)
             d["R"] = O.Csr.of(R.indptr, R.indices, R.data, R.shape)
         lv_ref.append(d)
-    mg = O.MultigridPCG(lv_ref, 0.7, 2)
+    mg = O.MultigridPCG(lv_ref, 0.7, 2, cycle=cycle, cgc=cgc)
     Ag, bg, bndg = _global_problem(LEVEL)
     dg = np.sin(np.arange(bg.size) * 0.61)
     dg[bndg] = 0.0
@@ -398,6 +398,35 @@ def _oracle_mg_reference(O):
     return z_ref, x_ref, info["iters"]
 
 
+def _run_strips(oracle_lib, world, configs, tol_z, tol_x):
+    from helpers import rel_err
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_mg_worker, args=(r, world, port, q, configs)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    refs = {}
+    for cfg in configs:
+        key = cfg[1:]
+        if key not in refs:
+            refs[key] = _oracle_mg_reference(oracle_lib, *key)
+        z_ref, x_ref, iters = refs[key]
+        covered = np.zeros(z_ref.size, dtype=bool)
+        for rank in range(world):
+            mine, z, x, it, ok, ghost = res[rank][cfg]
+            covered[mine] = True
+            assert ghost == (rank != 0)
+            assert rel_err(z, z_ref[mine]) <= tol_z, (cfg, rank, rel_err(z, z_ref[mine]))
+            assert ok and it == iters, (cfg, rank, it, iters)
+            assert rel_err(x, x_ref[mine]) <= tol_x, (cfg, rank, rel_err(x, x_ref[mine]))
+        assert covered.all()
+
+
 @pytest.mark.parametrize("world,merges", [(2, (1, 3, 4)), (3, (2, 3)), (4, (2,))])
 def test_global_multigrid_strips_gloo(oracle_lib, world, merges):
     """`world` gloo ranks, each holding one vertical strip of the 2D Q1 hierarchy on levels
@@ -406,28 +435,19 @@ def test_global_multigrid_strips_gloo(oracle_lib, world, merges):
     multigrid-preconditioned global PCG against the oracle's single-system V-cycle and PCG on the
     whole hierarchy (same operation order; only the split sums of the shared rows differ in
     rounding)."""
-    from helpers import rel_err
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    port = _free_port()
-    procs = [ctx.Process(target=_mg_worker, args=(r, world, port, q, merges)) for r in range(world)]
-    for p in procs:
-        p.start()
-    res = dict(q.get(timeout=240) for _ in range(world))
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
-    z_ref, x_ref, iters = _oracle_mg_reference(oracle_lib)
-    for merge in merges:
-        covered = np.zeros(z_ref.size, dtype=bool)
-        for rank in range(world):
-            mine, z, x, it, ok, ghost = res[rank][merge]
-            covered[mine] = True
-            assert ghost == (rank != 0)
-            assert rel_err(z, z_ref[mine]) <= 1e-13, (merge, rank, rel_err(z, z_ref[mine]))
-            assert ok and it == iters, (merge, rank, it, iters)
-            assert rel_err(x, x_ref[mine]) <= 1e-12, (merge, rank, rel_err(x, x_ref[mine]))
-        assert covered.all()
+    _run_strips(oracle_lib, world, [(m, "V", "fixed") for m in merges], 1e-13, 1e-12)
+
+
+@pytest.mark.parametrize("world,merge", [(2, 1), (3, 2)])
+def test_global_multigrid_fw_cycles_gloo(oracle_lib, world, merge):
+    """F and W cycles and the adaptive coarse-grid corrections on the strips, with the coarse
+    levels muxed onto rank 0: the ghost ranks cross the muxed transfer in the parent's order (the
+    test would hang or fail otherwise); cycle and solution against the oracle run with the same
+    cycle and correction (the adaptive step lengths come from global dot products, summed in
+    another order than the oracle's)."""
+    configs = [(merge, "F", "fixed"), (merge, "W", "fixed"), (merge, "V", "energy"), (merge, "F", "defect"),
+               (merge, "W", "energy")]
+    _run_strips(oracle_lib, world, configs, 1e-12, 1e-12)
 
 
 @pytest.mark.gpu
