@@ -101,22 +101,20 @@ class Gate:
             self.sync_0(v)
         return v
 
-    def _sum(self, x: float) -> float:
+    def _sum(self, local: torch.Tensor) -> float:
+        """The sum over the ranks of a one-element tensor, all-reduced on its own device (no host
+        copy before the reduction; one synchronisation to read the result)."""
         if self._world() == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64)
-        if self.freqs is not None and self.freqs.is_cuda:
-            t = t.cuda()
+            return float(local)
+        t = local.reshape(1).clone()
         self.dist.all_reduce(t)
         return float(t.item())
 
     def dot(self, x: torch.Tensor, y: torch.Tensor) -> float:
         """Global dot product of two type-1 vectors (gate.hpp:476-492)."""
-        if self._world() == 1:
-            return float(torch.dot(x, y))
-        if not self.ranks:
-            return self._sum(float(torch.dot(x, y)))
-        return self._sum(float(torch.sum(self.freqs * x * y)))
+        if self._world() == 1 or not self.ranks:
+            return self._sum(torch.dot(x, y))
+        return self._sum(torch.sum(self.freqs * x * y))
 
     def norm2(self, x: torch.Tensor) -> float:
         return math.sqrt(self.dot(x, x))
